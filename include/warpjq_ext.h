@@ -1,0 +1,106 @@
+/* warpjq device backend -- extension entry points.
+ *
+ * These sit beside the drop-in ABI of warpjq_kernels.h and leave its structs
+ * untouched.  They have no counterpart in the reference project: they serve
+ * callers whose input is already resident in device memory (the
+ * device-resident scan the benchmark measures), and they report aggregates
+ * with exact 128-bit integer sums, which the reference's f64-only
+ * warpjq_agg_partial cannot carry.
+ *
+ * Usage: warpjq_launch_device() enqueues the whole scan on a CUDA stream and
+ * returns without synchronising; warpjq_collect_device() waits for it and
+ * fills a warpjq_device_result.  Device buffers named in the result belong to
+ * the context and stay valid until the next launch on it.
+ */
+#ifndef WARPJQ_EXT_H
+#define WARPJQ_EXT_H
+
+#include "warpjq_kernels.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One group of a device-resident run. */
+typedef struct {
+  uint64_t key_off;   /* byte offset of the key in the input (string: body) */
+  uint32_t key_len;
+  uint32_t key_kind;  /* JSON kind code 0..6 */
+  uint64_t count;     /* lines that reached the aggregate */
+  uint64_t numeric;   /* lines that contributed a number */
+  uint64_t isum_lo;   /* exact sum of integer-literal values, two's complement */
+  uint64_t isum_hi;
+  uint64_t n_int;     /* how many values went into the exact sum */
+  double fsum;        /* fixed-order FP64 sum of the other numbers */
+  double min;
+  double max;
+  double sum;         /* isum + fsum rounded once to FP64 */
+} warpjq_group_ext;
+
+/* Aggregate and counters of a device-resident run. */
+typedef struct {
+  uint64_t n_lines;
+  uint64_t n_blank;
+  uint64_t n_invalid;
+  uint64_t n_type_error;
+  uint64_t n_selected;
+  uint64_t first_invalid;    /* lowest invalid line index, or UINT64_MAX */
+  uint64_t first_type_error; /* lowest line index with a type error, or UINT64_MAX */
+
+  /* Rows (non-aggregate queries) stay in device memory. */
+  const uint8_t *d_out_bytes;
+  uint64_t out_len;
+  const uint64_t *d_out_line_idx; /* n_selected entries */
+  const uint64_t *d_out_row_off;  /* n_selected + 1 entries */
+
+  /* Ungrouped aggregate. */
+  uint64_t count;
+  uint64_t numeric;
+  uint64_t isum_lo;
+  uint64_t isum_hi;
+  uint64_t n_int;
+  double fsum;
+  double min;
+  double max;
+  double sum; /* isum + fsum rounded once */
+  uint32_t saw_non_numeric;
+
+  /* Grouped aggregate: host copy, valid until the next launch. */
+  const warpjq_group_ext *groups;
+  uint32_t n_groups;
+
+  /* Device kernels launched by the last run (for launch accounting). */
+  uint32_t kernels_launched;
+} warpjq_device_result;
+
+/* Enqueues the context's query over `n_bytes` of input at device address
+ * `d_data` on `stream` (a cudaStream_t, or NULL for the default stream).
+ * The input must stay unchanged until warpjq_collect_device returns.  Any
+ * scratch that must grow is allocated here, synchronously, before enqueueing;
+ * a later launch of the same or smaller size allocates nothing. */
+warpjq_status warpjq_launch_device(warpjq_ctx *ctx, const uint8_t *d_data, uint64_t n_bytes,
+                                   void *stream, char *err, size_t err_len);
+
+/* Waits for the last launch and fills `out`.  If a device buffer proved too
+ * small (an unusually selective projection, a very high group cardinality),
+ * the buffers are grown and the run is repeated before returning, so the
+ * result is always complete. */
+warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, char *err,
+                                    size_t err_len);
+
+/* Lowest line index (within the chunk last waited on) that was malformed,
+ * and that hit a type error; UINT64_MAX for none.  warpjq_chunk_result
+ * carries only the first; the second lets a host stop at the first bad
+ * line of either kind, as --strict does on the CPU (exec/cpu.rs:394-407). */
+warpjq_status warpjq_slot_first_errors(warpjq_ctx *ctx, uint32_t slot, uint64_t *first_invalid,
+                                       uint64_t *first_type_error);
+
+/* Device-resident scan tunables: bytes per tile and the halo staged after it.
+ * 0 keeps the current value.  Both must be multiples of 1024. */
+warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t halo_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARPJQ_EXT_H */

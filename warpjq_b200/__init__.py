@@ -1,0 +1,268 @@
+"""warpjq_b200: a B200-native (sm_100a) backend for warpjq's NDJSON scan path.
+
+The product is native code behind a C ABI:
+  * libwarpjq_kernels.so -- the device backend with the reference's
+    warpjq_kernels.h ABI (include/warpjq_kernels.h) plus the device-resident
+    extension (include/warpjq_ext.h);
+  * libwarpjq_host.so -- the host driver (include/warpjq_host.h) that parses
+    a jq-subset query, streams input through the ABI and formats the output
+    as warpjq does.
+
+This module is the Python mirror of that interface, through ctypes.  It
+never evaluates a line itself: if the native libraries are missing it raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(_HERE, "_lib")
+KERNELS_SO = os.path.join(LIB_DIR, "libwarpjq_kernels.so")
+HOST_SO = os.path.join(LIB_DIR, "libwarpjq_host.so")
+
+FORMATS = {"ndjson": 0, "csv": 1, "count": 2}
+ON_INVALID = {"warn": 0, "skip": 1, "abort": 2}
+
+# Every symbol include/*.h declares, by library.
+ABI_SYMBOLS = [
+    "warpjq_probe", "warpjq_abi_check", "warpjq_ctx_create", "warpjq_ctx_destroy",
+    "warpjq_slot_buffer", "warpjq_slot_capacity", "warpjq_max_lines", "warpjq_submit",
+    "warpjq_wait", "warpjq_device_name",
+]
+EXT_SYMBOLS = [
+    "warpjq_launch_device", "warpjq_collect_device", "warpjq_slot_first_errors",
+    "warpjq_set_tiling",
+]
+HOST_SYMBOLS = [
+    "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
+    "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
+    "warpjq_gen_nginx", "warpjq_gen_nginx_block",
+]
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+_kern = None
+_host = None
+
+
+def _load():
+    global _kern, _host
+    if _host is not None:
+        return _kern, _host
+    for p in (KERNELS_SO, HOST_SO):
+        if not os.path.exists(p):
+            raise NativeLibraryMissing(
+                f"{p} is not built; run `python -m warpjq_b200.build` (no CPU fallback exists)")
+    k = ctypes.CDLL(KERNELS_SO, mode=ctypes.RTLD_GLOBAL)
+    h = ctypes.CDLL(HOST_SO)
+    vp, sz, u64, u32, cp = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_char_p
+    k.warpjq_probe.argtypes = [cp, sz]
+    k.warpjq_probe.restype = ctypes.c_int
+    k.warpjq_abi_check.argtypes = [ctypes.POINTER(u64), sz]
+    k.warpjq_abi_check.restype = ctypes.c_int
+    k.warpjq_device_name.argtypes = [cp, sz]
+    k.warpjq_device_name.restype = ctypes.c_int
+    k.warpjq_launch_device.argtypes = [vp, vp, u64, vp, cp, sz]
+    k.warpjq_launch_device.restype = ctypes.c_int
+    k.warpjq_collect_device.argtypes = [vp, vp, cp, sz]
+    k.warpjq_collect_device.restype = ctypes.c_int
+    k.warpjq_set_tiling.argtypes = [vp, u32, u32]
+    k.warpjq_set_tiling.restype = ctypes.c_int
+    h.warpjq_query_open.argtypes = [cp, u32, u64, ctypes.POINTER(vp), cp, sz]
+    h.warpjq_query_open.restype = ctypes.c_int
+    h.warpjq_query_close.argtypes = [vp]
+    h.warpjq_query_ctx.argtypes = [vp]
+    h.warpjq_query_ctx.restype = vp
+    h.warpjq_query_is_aggregate.argtypes = [vp]
+    h.warpjq_query_is_aggregate.restype = ctypes.c_int
+    h.warpjq_query_run.argtypes = [vp, cp, sz, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
+                                   ctypes.POINTER(u64), cp, sz]
+    h.warpjq_query_run.restype = ctypes.c_int
+    h.warpjq_run_bytes.argtypes = [cp, cp, sz, u32, u32, u64, u64, ctypes.POINTER(vp),
+                                   ctypes.POINTER(sz), ctypes.POINTER(u64), cp, sz]
+    h.warpjq_run_bytes.restype = ctypes.c_int
+    h.warpjq_query_render_device.argtypes = [vp, vp, cp, ctypes.POINTER(vp), ctypes.POINTER(sz)]
+    h.warpjq_query_render_device.restype = ctypes.c_int
+    h.warpjq_host_free.argtypes = [vp]
+    h.warpjq_gen_nginx.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
+    h.warpjq_gen_nginx.restype = u64
+    _kern, _host = k, h
+    return k, h
+
+
+def libraries():
+    """(kernels, host) ctypes handles; raises NativeLibraryMissing."""
+    return _load()
+
+
+@dataclass
+class RunResult:
+    rc: int
+    out: bytes
+    stats: dict
+    err: str
+
+
+def _take(ptr, n) -> bytes:
+    if not ptr.value:
+        return b""
+    b = ctypes.string_at(ptr.value, n.value)
+    _load()[1].warpjq_host_free(ptr)
+    return b
+
+
+def _stats(arr):
+    return dict(zip(["bytes_in", "lines_in", "lines_out", "malformed", "type_errors"], list(arr)))
+
+
+def run_bytes(query: str, data: bytes, fmt: str = "ndjson", on_invalid: str = "skip",
+              chunk_bytes: int = 0, max_line_bytes: int = 0) -> RunResult:
+    """Runs `query` over `data` on the GPU, like warpjq's run_bytes."""
+    _, h = _load()
+    out = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    st = (ctypes.c_uint64 * 5)()
+    err = ctypes.create_string_buffer(4096)
+    rc = h.warpjq_run_bytes(query.encode(), data, len(data), FORMATS[fmt], ON_INVALID[on_invalid],
+                            chunk_bytes, max_line_bytes, ctypes.byref(out), ctypes.byref(n), st,
+                            err, len(err))
+    return RunResult(rc, _take(out, n), _stats(st), err.value.decode(errors="replace"))
+
+
+class _GroupExt(ctypes.Structure):
+    _fields_ = [("key_off", ctypes.c_uint64), ("key_len", ctypes.c_uint32),
+                ("key_kind", ctypes.c_uint32), ("count", ctypes.c_uint64),
+                ("numeric", ctypes.c_uint64), ("isum_lo", ctypes.c_uint64),
+                ("isum_hi", ctypes.c_uint64), ("n_int", ctypes.c_uint64),
+                ("fsum", ctypes.c_double), ("min", ctypes.c_double), ("max", ctypes.c_double),
+                ("sum", ctypes.c_double)]
+
+
+class DeviceResult(ctypes.Structure):
+    """Mirror of warpjq_device_result (include/warpjq_ext.h)."""
+    _fields_ = [("n_lines", ctypes.c_uint64), ("n_blank", ctypes.c_uint64),
+                ("n_invalid", ctypes.c_uint64), ("n_type_error", ctypes.c_uint64),
+                ("n_selected", ctypes.c_uint64), ("first_invalid", ctypes.c_uint64),
+                ("first_type_error", ctypes.c_uint64),
+                ("d_out_bytes", ctypes.c_void_p), ("out_len", ctypes.c_uint64),
+                ("d_out_line_idx", ctypes.c_void_p), ("d_out_row_off", ctypes.c_void_p),
+                ("count", ctypes.c_uint64), ("numeric", ctypes.c_uint64),
+                ("isum_lo", ctypes.c_uint64), ("isum_hi", ctypes.c_uint64),
+                ("n_int", ctypes.c_uint64), ("fsum", ctypes.c_double), ("min", ctypes.c_double),
+                ("max", ctypes.c_double), ("sum", ctypes.c_double),
+                ("saw_non_numeric", ctypes.c_uint32), ("groups", ctypes.POINTER(_GroupExt)),
+                ("n_groups", ctypes.c_uint32), ("kernels_launched", ctypes.c_uint32)]
+
+    def isum(self) -> int:
+        v = (self.isum_hi << 64) | self.isum_lo
+        return v - (1 << 128) if self.isum_hi >> 63 else v
+
+
+class Query:
+    """A compiled query with its device context (warpjq_query_open)."""
+
+    def __init__(self, query: str, fmt: str = "ndjson", chunk_bytes: int = 0):
+        _, h = _load()
+        self._h = h
+        self._q = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(4096)
+        rc = h.warpjq_query_open(query.encode(), FORMATS[fmt], chunk_bytes, ctypes.byref(self._q),
+                                 err, len(err))
+        if rc:
+            raise ValueError(err.value.decode(errors="replace")) if rc == 2 else \
+                RuntimeError(err.value.decode(errors="replace"))
+        self.query = query
+        self.fmt = fmt
+
+    def close(self):
+        if self._q:
+            self._h.warpjq_query_close(self._q)
+            self._q = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ctx(self):
+        return self._h.warpjq_query_ctx(self._q)
+
+    @property
+    def is_aggregate(self) -> bool:
+        return bool(self._h.warpjq_query_is_aggregate(self._q))
+
+    def run(self, data: bytes, on_invalid: str = "skip", max_line_bytes: int = 0) -> RunResult:
+        out = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        st = (ctypes.c_uint64 * 5)()
+        err = ctypes.create_string_buffer(4096)
+        rc = self._h.warpjq_query_run(self._q, data, len(data), ON_INVALID[on_invalid],
+                                      max_line_bytes, ctypes.byref(out), ctypes.byref(n), st, err,
+                                      len(err))
+        return RunResult(rc, _take(out, n), _stats(st), err.value.decode(errors="replace"))
+
+    def set_tiling(self, tile_bytes: int = 0, halo_bytes: int = 0):
+        k, _ = _load()
+        if k.warpjq_set_tiling(self.ctx, tile_bytes, halo_bytes) != 0:
+            raise ValueError("bad tiling")
+
+    def launch_device(self, d_ptr: int, n: int, stream: int = 0):
+        """Enqueues a device-resident run (no host synchronisation)."""
+        k, _ = _load()
+        err = ctypes.create_string_buffer(1024)
+        rc = k.warpjq_launch_device(self.ctx, ctypes.c_void_p(d_ptr), n, ctypes.c_void_p(stream),
+                                    err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+
+    def collect_device(self) -> DeviceResult:
+        k, _ = _load()
+        r = DeviceResult()
+        err = ctypes.create_string_buffer(1024)
+        rc = k.warpjq_collect_device(self.ctx, ctypes.byref(r), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+        return r
+
+    def render_device(self, r: DeviceResult, host_data: bytes) -> bytes:
+        out = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        self._h.warpjq_query_render_device(self._q, ctypes.byref(r), host_data, ctypes.byref(out),
+                                           ctypes.byref(n))
+        return _take(out, n)
+
+
+def probe() -> str:
+    """'' when a usable sm_100 device is present, else the reason."""
+    k, _ = _load()
+    err = ctypes.create_string_buffer(512)
+    rc = k.warpjq_probe(err, len(err))
+    return "" if rc == 0 else err.value.decode(errors="replace")
+
+
+def device_name() -> str:
+    k, _ = _load()
+    buf = ctypes.create_string_buffer(256)
+    k.warpjq_device_name(buf, len(buf))
+    return buf.value.decode()
+
+
+def gen_nginx(n_bytes: int, seed: int = 1, threads: int = 0, into=None):
+    """About n_bytes of the benchmark's nginx-style NDJSON (whole lines).
+
+    Returns (buffer, used_bytes, n_lines).  `into` may be a writable numpy
+    uint8 array of at least n_bytes (e.g. pinned host memory)."""
+    import numpy as np
+    _, h = _load()
+    buf = into if into is not None else np.empty(n_bytes, dtype=np.uint8)
+    lines = ctypes.c_uint64()
+    used = h.warpjq_gen_nginx(seed, buf.ctypes.data, n_bytes, 1 << 20, threads, ctypes.byref(lines))
+    return buf, int(used), int(lines.value)

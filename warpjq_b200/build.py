@@ -1,0 +1,73 @@
+"""Builds the native parts of warpjq_b200 in-tree.
+
+  warpjq_b200/_lib/libwarpjq_kernels.so  -- the sm_100a device backend (C ABI)
+  warpjq_b200/_lib/libwarpjq_kernels.a   -- the same, as the static library the
+                                            reference's Rust crate links
+  warpjq_b200/_lib/libwarpjq_host.so     -- the C++ host driver (query front-end,
+                                            pipeline, formatting)
+  warpjq_b200/_lib/warpjq                -- the command-line tool
+
+Run: python -m warpjq_b200.build   (nvcc cross-compiles; no GPU needed)
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "_lib")
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
+
+KERNEL_SRCS = [os.path.join(CSRC, "backend.cu")]
+KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "plan.h")]
+HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc")]
+CLI_SRCS = [os.path.join(CSRC, "host", "cli.cc")]
+HEADERS = [os.path.join(ROOT, "include", f) for f in ("warpjq_kernels.h", "warpjq_ext.h", "warpjq_host.h")]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> None:
+    os.makedirs(LIB, exist_ok=True)
+    so = os.path.join(LIB, "libwarpjq_kernels.so")
+    deps = KERNEL_SRCS + KERNEL_DEPS + HEADERS
+    if force or _stale(so, deps):
+        extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+        _run([NVCC, *NVFLAGS, *extra, "-shared", "-o", so, *KERNEL_SRCS])
+    static = os.path.join(LIB, "libwarpjq_kernels.a")
+    if force or _stale(static, deps):
+        obj = os.path.join(LIB, "backend.o")
+        _run([NVCC, *NVFLAGS, "-c", "-o", obj, *KERNEL_SRCS])
+        if os.path.exists(static):
+            os.remove(static)
+        _run(["ar", "rcs", static, obj])
+        os.remove(obj)
+    host = os.path.join(LIB, "libwarpjq_host.so")
+    hdeps = HOST_SRCS + [os.path.join(CSRC, "host", "query.h")] + HEADERS + [so]
+    if force or _stale(host, hdeps):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", host, *HOST_SRCS,
+              "-L" + LIB, "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+    cli = os.path.join(LIB, "warpjq")
+    if all(os.path.exists(s) for s in CLI_SRCS) and (force or _stale(cli, CLI_SRCS + [host])):
+        _run(["g++", "-O2", "-std=c++17", "-o", cli, *CLI_SRCS, "-L" + LIB, "-lwarpjq_host",
+              "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv)

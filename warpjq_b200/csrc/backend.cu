@@ -1,0 +1,1026 @@
+// The warpjq device backend for sm_100a: the C ABI of warpjq_kernels.h
+// (reference crates/warpjq-core/cuda/warpjq_kernels.h:238-274) and the
+// device-resident extension of warpjq_ext.h.
+//
+// Per run the backend launches four kernels on one stream -- reset, scan,
+// tile reduction, finalize -- with no host synchronisation in between.
+// Device buffers that depend on the data (row records, output bytes, the
+// group table, the deep-nesting stack) start at a size that fits ordinary
+// input and are grown when the scan reports that one was too small; the run
+// is then repeated on the device, so every line is always decided there.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/warpjq_ext.h"
+#include "../../include/warpjq_kernels.h"
+#include "kernels.cuh"
+#include "plan.h"
+
+using namespace wjq;
+
+namespace {
+
+void set_err(char *err, size_t n, const char *fmt, ...) {
+  if (!err || !n) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(err, n, fmt, ap);
+  va_end(ap);
+}
+
+#define CK(call, what)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      set_err(err, err_len, "%s: %s", what, cudaGetErrorString(e_));                      \
+      return e_ == cudaErrorMemoryAllocation ? WARPJQ_ERR_OOM : WARPJQ_ERR_CUDA;          \
+    }                                                                                     \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Plan compilation: flat tables -> DevPlan with a preorder-numbered trie.
+// ---------------------------------------------------------------------------
+
+struct TmpNode {
+  bool is_index = false;
+  uint32_t index = 0;
+  uint32_t key_off = 0, key_len = 0;
+  std::vector<int> kids;
+  int parent = -1;
+};
+
+warpjq_status build_plan(const warpjq_program *p, DevPlan &P, char *err, size_t err_len) {
+  std::memset(&P, 0, sizeof(P));
+  if (!p) {
+    set_err(err, err_len, "program is null");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  if (p->n_needed > (uint32_t)kMaxSlots) {
+    set_err(err, err_len, "query needs %u field paths; this backend resolves at most %d",
+            p->n_needed, kMaxSlots);
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  if (p->n_blob > (uint32_t)kMaxBlob || p->n_cmps > (uint32_t)kMaxCmps ||
+      p->n_cond > (uint32_t)kMaxCond || p->n_fields > (uint32_t)kMaxFields) {
+    set_err(err, err_len, "query is too large for the device plan");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  if (p->n_blob) std::memcpy(P.blob, p->blob, p->n_blob);
+  auto slot_of = [&](uint32_t path) -> int {
+    if (path >= p->n_paths) return -1;
+    uint32_t s = p->slot_of_path[path];
+    return s == 0xFFFFFFFFu ? -1 : (int)s;
+  };
+
+  // Trie over the needed paths.
+  std::vector<TmpNode> tn(1);
+  std::vector<int> slot_tmp(p->n_needed, 0);
+  for (uint32_t s = 0; s < p->n_needed; s++) {
+    uint32_t path = p->needed_paths[s];
+    if (path >= p->n_paths) {
+      set_err(err, err_len, "needed path %u out of range", path);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+    const warpjq_path &wp = p->paths[path];
+    if (wp.step_count == 0 || wp.step_count > (uint32_t)kMaxDepthFast - 2) {
+      set_err(err, err_len, "path %u has %u steps; the device supports 1..%d", path, wp.step_count,
+              kMaxDepthFast - 2);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+    int cur = 0;
+    for (uint32_t k = 0; k < wp.step_count; k++) {
+      const warpjq_step &st = p->steps[wp.step_off + k];
+      bool is_index = st.kind == WARPJQ_STEP_INDEX;
+      if (!is_index && (st.key_off + st.key_len > p->n_blob)) {
+        set_err(err, err_len, "step key out of the blob");
+        return WARPJQ_ERR_INVALID_ARG;
+      }
+      int found = -1;
+      for (int c : tn[cur].kids) {
+        const TmpNode &x = tn[c];
+        if (x.is_index != is_index) continue;
+        if (is_index ? x.index == st.index
+                     : (x.key_len == st.key_len &&
+                        std::memcmp(p->blob + x.key_off, p->blob + st.key_off, st.key_len) == 0)) {
+          found = c;
+          break;
+        }
+      }
+      if (found < 0) {
+        TmpNode nn;
+        nn.is_index = is_index;
+        nn.index = st.index;
+        nn.key_off = st.key_off;
+        nn.key_len = st.key_len;
+        nn.parent = cur;
+        tn.push_back(nn);
+        found = (int)tn.size() - 1;
+        tn[cur].kids.push_back(found);
+      }
+      cur = found;
+    }
+    slot_tmp[s] = cur;
+  }
+  if (tn.size() > (size_t)kMaxNodes) {
+    set_err(err, err_len, "query paths need %zu trie nodes; at most %d", tn.size(), kMaxNodes);
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  // Preorder numbering.
+  std::vector<int> order, newid(tn.size());
+  std::vector<int> stack{0};
+  while (!stack.empty()) {
+    int x = stack.back();
+    stack.pop_back();
+    newid[x] = (int)order.size();
+    order.push_back(x);
+    for (auto it = tn[x].kids.rbegin(); it != tn[x].kids.rend(); ++it) stack.push_back(*it);
+  }
+  std::vector<int> subtree_end(tn.size());
+  for (int i = (int)order.size() - 1; i >= 0; i--) {
+    int x = order[i];
+    int e = i + 1;
+    for (int c : tn[x].kids) e = std::max(e, subtree_end[c]);
+    subtree_end[x] = e;
+  }
+  P.n_nodes = p->n_needed ? (uint32_t)tn.size() : 0;
+  for (size_t i = 0; i < order.size() && P.n_nodes; i++) {
+    const TmpNode &x = tn[order[i]];
+    PlanNode &d = P.nodes[i];
+    d.index = x.index;
+    d.key_off = (uint16_t)x.key_off;
+    d.key_len = (uint16_t)x.key_len;
+    d.parent = x.parent < 0 ? kNoNode : (uint8_t)newid[x.parent];
+    d.is_index = x.is_index;
+    d.first_child = x.kids.empty() ? kNoNode : (uint8_t)newid[x.kids[0]];
+    d.next_sibling = kNoNode;
+    d.subtree_end = (uint8_t)subtree_end[order[i]];
+    d.key_first = (!x.is_index && x.key_len) ? p->blob[x.key_off] : 0;
+    for (size_t k = 0; k < x.kids.size(); k++) {
+      const TmpNode &c = tn[x.kids[k]];
+      if (c.is_index) d.has_index_children = 1;
+      else d.has_key_children = 1;
+    }
+    for (size_t k = 0; k + 1 < x.kids.size(); k++)
+      P.nodes[newid[x.kids[k]]].next_sibling = (uint8_t)newid[x.kids[k + 1]];
+  }
+  P.n_slots = p->n_needed;
+  for (uint32_t s = 0; s < p->n_needed; s++) P.slot_node[s] = (uint8_t)newid[slot_tmp[s]];
+
+  // Condition.
+  P.n_cmps = p->n_cmps;
+  for (uint32_t i = 0; i < p->n_cmps; i++) {
+    const warpjq_cmp &c = p->cmps[i];
+    int s = slot_of(c.path);
+    if (s < 0 || c.op > 5 || c.lit_kind > 4 || c.lit_off + c.lit_len > p->n_blob) {
+      set_err(err, err_len, "comparison %u is malformed", i);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+    PlanCmp &d = P.cmps[i];
+    d.lit_num = c.lit_num;
+    d.lit_off = (uint16_t)c.lit_off;
+    d.lit_len = (uint16_t)c.lit_len;
+    d.slot = (uint8_t)s;
+    d.op = (uint8_t)c.op;
+    d.lit_kind = (uint8_t)c.lit_kind;
+    d.lit_rank = (uint8_t)c.lit_kind;  // null 0, false 1, true 2, num 3, str 4 (ir.rs:100-108)
+    P.filter_slot_mask |= 1u << s;
+  }
+  P.n_cond = p->n_cond;
+  int depth = 0, max_depth = 0;
+  for (uint32_t i = 0; i < p->n_cond; i++) {
+    const warpjq_cond_op &o = p->cond_rpn[i];
+    PlanCond &d = P.cond[i];
+    d.op = (uint8_t)o.op;
+    if (o.op == WARPJQ_COND_CMP) {
+      if (o.arg >= p->n_cmps) {
+        set_err(err, err_len, "condition references comparison %u", o.arg);
+        return WARPJQ_ERR_INVALID_ARG;
+      }
+      d.arg = (uint8_t)o.arg;
+      depth++;
+    } else if (o.op == WARPJQ_COND_TRUTHY) {
+      int s = slot_of(o.arg);
+      if (s < 0) {
+        set_err(err, err_len, "condition references an unresolved path");
+        return WARPJQ_ERR_INVALID_ARG;
+      }
+      d.arg = (uint8_t)s;
+      P.filter_slot_mask |= 1u << s;
+      depth++;
+    } else if (o.op == WARPJQ_COND_AND || o.op == WARPJQ_COND_OR) {
+      depth--;
+    } else if (o.op != WARPJQ_COND_NOT) {
+      set_err(err, err_len, "unknown condition op %u", o.op);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+    max_depth = std::max(max_depth, depth);
+    if (depth < 1) {
+      set_err(err, err_len, "condition stack underflows");
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+  }
+  if (max_depth > 63) {
+    set_err(err, err_len, "condition nests deeper than the device evaluator supports");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  P.has_filter = p->has_filter && p->n_cond > 0;
+
+  // Output.
+  P.output_kind = p->output_kind;
+  P.agg_kind = p->agg_kind;
+  P.csv_mode = p->csv_mode;
+  P.out_slot = -1;
+  P.agg_slot = -1;
+  P.group_slot = -1;
+  if (p->output_kind == WARPJQ_OUT_PATH) {
+    P.out_slot = slot_of(p->output_path);
+    if (P.out_slot < 0) {
+      set_err(err, err_len, "output path has no slot");
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+  } else if (p->output_kind == WARPJQ_OUT_PROJECT) {
+    P.n_fields = p->n_fields;
+    for (uint32_t f = 0; f < p->n_fields; f++) {
+      int s = slot_of(p->field_paths[f]);
+      if (s < 0 || p->prefix_off[f] + p->prefix_len[f] > p->n_blob) {
+        set_err(err, err_len, "projection field %u is malformed", f);
+        return WARPJQ_ERR_INVALID_ARG;
+      }
+      P.field_slot[f] = (int8_t)s;
+      P.prefix_off[f] = (uint16_t)p->prefix_off[f];
+      P.prefix_len[f] = (uint16_t)p->prefix_len[f];
+    }
+    P.suffix_off = p->suffix_off;
+    P.suffix_len = p->suffix_len;
+  } else if (p->output_kind == WARPJQ_OUT_AGG) {
+    if (p->agg_path != 0xFFFFFFFFu) P.agg_slot = slot_of(p->agg_path);
+    if (p->group_path != 0xFFFFFFFFu) P.group_slot = slot_of(p->group_path);
+    if ((p->agg_path != 0xFFFFFFFFu && P.agg_slot < 0) ||
+        (p->group_path != 0xFFFFFFFFu && P.group_slot < 0)) {
+      set_err(err, err_len, "aggregate path has no slot");
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+  } else if (p->output_kind != WARPJQ_OUT_PASSTHROUGH) {
+    set_err(err, err_len, "unknown output kind %u", p->output_kind);
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  P.needs_rows = p->output_kind != WARPJQ_OUT_AGG;
+  uint32_t nf = p->output_kind == WARPJQ_OUT_PROJECT ? p->n_fields
+                : p->output_kind == WARPJQ_OUT_PATH  ? 1
+                                                     : 0;
+  P.rec_stride = (uint32_t)sizeof(RowRec) + 8 * nf;
+  return WARPJQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device buffers of one run, sized for an input length.
+// ---------------------------------------------------------------------------
+
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc((void **)&p, std::max<size_t>(want, 1) * sizeof(T));
+    if (e == cudaSuccess) n = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct RunBufs {
+  DevBuf<RunCounters> ctr;
+  DevBuf<TileDesc> tiles;
+  DevBuf<unsigned int> lb_flag;
+  DevBuf<unsigned long long> lb_agg, lb_incl;
+  DevBuf<uint8_t> recs;
+  DevBuf<uint8_t> out;
+  DevBuf<unsigned long long> row_off, line_idx;
+  DevBuf<double> tile_fsum;
+  DevBuf<double> block_f;
+  DevBuf<unsigned long long> block_lines;
+  DevBuf<uint32_t> deep;
+  // group table
+  DevBuf<unsigned long long> g_slots, g_key_off, g_count, g_numeric, g_isum_lo, g_isum_hi, g_n_int,
+      g_min, g_max;
+  DevBuf<uint32_t> g_key_len;
+  DevBuf<uint8_t> g_key_kind, g_key_esc;
+  DevBuf<double> g_fsum;
+  DevBuf<unsigned int> g_saw;
+
+  // current capacities
+  unsigned long long rec_cap_per_cta = 0;
+  unsigned long long out_cap = 0;
+  unsigned long long rows_cap = 0;
+  uint32_t g_cap = 0;      // table slots (power of two)
+  uint32_t g_key_cap = 0;
+  unsigned long long deep_levels = 0;
+
+  void release() {
+    ctr.release(); tiles.release(); lb_flag.release(); lb_agg.release(); lb_incl.release();
+    recs.release(); out.release(); row_off.release(); line_idx.release(); tile_fsum.release();
+    block_f.release(); block_lines.release(); deep.release(); g_slots.release();
+    g_key_off.release(); g_count.release(); g_numeric.release(); g_isum_lo.release();
+    g_isum_hi.release(); g_n_int.release(); g_min.release(); g_max.release();
+    g_key_len.release(); g_key_kind.release(); g_key_esc.release(); g_fsum.release();
+    g_saw.release();
+  }
+};
+
+constexpr unsigned kReduceBlocks = 256;
+
+__global__ void k_reset_run(RunCounters *ctr, unsigned int *lb_flag, unsigned long long n_tiles,
+                            GroupTable g, uint32_t g_cap, uint32_t key_cap) {
+  unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  if (tid == 0) {
+    RunCounters z;
+    memset(&z, 0, sizeof(z));
+    z.first_invalid_tile = ~0ull;
+    z.first_type_tile = ~0ull;
+    z.first_type_error = ~0ull;
+    z.agg_min_bits = ~0ull;
+    z.first_invalid = ~0ull;
+    *ctr = z;
+  }
+  if (lb_flag)
+    for (unsigned long long i = tid; i < n_tiles; i += stride) lb_flag[i] = 0;
+  if (g.slots) {
+    for (unsigned long long i = tid; i < g_cap; i += stride) g.slots[i] = 0;
+    for (unsigned long long i = tid; i < key_cap; i += stride) {
+      g.count[i] = 0;
+      g.numeric[i] = 0;
+      g.isum_lo[i] = 0;
+      g.isum_hi[i] = 0;
+      g.n_int[i] = 0;
+      g.min_bits[i] = ~0ull;
+      g.max_bits[i] = 0;
+      g.fsum[i] = 0.0;
+      g.saw_non_numeric[i] = 0;
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context.
+// ---------------------------------------------------------------------------
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  uint8_t *h_chunk = nullptr;  // pinned staging
+  uint8_t *d_chunk = nullptr;
+  unsigned long long n_bytes = 0;
+  RunBufs rb;
+  RunCounters *h_ctr = nullptr;  // pinned mirror
+  // pinned result mirrors
+  std::vector<uint8_t> dummy;
+  uint8_t *h_out = nullptr;
+  size_t h_out_cap = 0;
+  unsigned long long *h_row_off = nullptr;
+  unsigned long long *h_line64 = nullptr;
+  uint32_t *h_line32 = nullptr;
+  size_t h_rows_cap = 0;
+  warpjq_group *h_groups = nullptr;
+  size_t h_groups_cap = 0;
+  bool launched = false;
+  uint32_t kernels = 0;
+  unsigned long long last_first_invalid = ~0ull;
+  unsigned long long last_first_type = ~0ull;
+};
+
+struct warpjq_ctx {
+  int device = 0;
+  int num_sms = 0;
+  DevPlan plan;
+  DevPlan *d_plan = nullptr;
+  unsigned long long chunk_cap = 0;
+  uint32_t tile_bytes = 32768;
+  uint32_t halo_bytes = 8192;
+  unsigned grid = 0;        // persistent CTAs for the scan kernel
+  size_t scan_smem = 0;
+  std::vector<Slot> slots;
+  // device-resident runs
+  Slot dev;
+  const uint8_t *dev_data = nullptr;
+  unsigned long long dev_n = 0;
+  cudaStream_t dev_stream = nullptr;
+  std::vector<warpjq_group_ext> dev_groups;
+};
+
+namespace {
+
+size_t scan_smem_bytes(uint32_t T, uint32_t H) {
+  size_t s = T + H + 16;
+  s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
+  s += 64 * sizeof(uint32_t);
+  s = (s + 7) & ~(size_t)7;
+  s += 64 * sizeof(unsigned long long) + 8;
+  return s;
+}
+
+warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
+  c->scan_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes);
+  int per_sm = 0;
+  CK(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)c->scan_smem),
+     "cudaFuncSetAttribute(scan rows)");
+  CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)c->scan_smem),
+     "cudaFuncSetAttribute(scan agg)");
+  int a = 0, b = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_scan<true>, kThreads, c->scan_smem),
+     "occupancy");
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scan<false>, kThreads, c->scan_smem),
+     "occupancy");
+  per_sm = std::max(1, std::min(a, b));
+  c->grid = (unsigned)(c->num_sms * per_sm);
+  return WARPJQ_OK;
+}
+
+// Sizes the buffers of `s` for an input of n bytes (first use, or growth).
+warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n, char *err,
+                          size_t err_len) {
+  RunBufs &rb = s.rb;
+  const DevPlan &P = c->plan;
+  unsigned long long n_tiles = (n + c->tile_bytes - 1) / c->tile_bytes;
+  if (n_tiles == 0) n_tiles = 1;
+  CK(rb.ctr.ensure(1), "alloc counters");
+  CK(rb.tiles.ensure(n_tiles), "alloc tiles");
+  CK(rb.tile_fsum.ensure(n_tiles), "alloc tile sums");
+  CK(rb.block_f.ensure(kReduceBlocks), "alloc reduce");
+  CK(rb.block_lines.ensure(2 * kReduceBlocks), "alloc reduce");
+  if (!rb.deep_levels) rb.deep_levels = 1u << 16;
+  CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32)), "alloc deep stack");
+  if (P.needs_rows) {
+    CK(rb.lb_flag.ensure(n_tiles), "alloc look-back");
+    CK(rb.lb_agg.ensure(n_tiles * 3), "alloc look-back");
+    CK(rb.lb_incl.ensure(n_tiles * 3), "alloc look-back");
+    if (!rb.rec_cap_per_cta) rb.rec_cap_per_cta = std::max<unsigned long long>(c->tile_bytes / 64, 256);
+    CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * P.rec_stride), "alloc records");
+    if (!rb.out_cap) rb.out_cap = n + n / 4 + (1u << 20);
+    CK(rb.out.ensure(rb.out_cap), "alloc output");
+    if (!rb.rows_cap) rb.rows_cap = n / 32 + 4096;
+    CK(rb.row_off.ensure(rb.rows_cap + 1), "alloc row offsets");
+    CK(rb.line_idx.ensure(rb.rows_cap), "alloc line index");
+  }
+  if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
+    if (!rb.g_cap) {
+      rb.g_cap = 1u << 17;
+      rb.g_key_cap = 1u << 16;
+    }
+    CK(rb.g_slots.ensure(rb.g_cap), "alloc group table");
+    size_t k = rb.g_key_cap;
+    CK(rb.g_key_off.ensure(k), "alloc groups");
+    CK(rb.g_key_len.ensure(k), "alloc groups");
+    CK(rb.g_key_kind.ensure(k), "alloc groups");
+    CK(rb.g_key_esc.ensure(k), "alloc groups");
+    CK(rb.g_count.ensure(k), "alloc groups");
+    CK(rb.g_numeric.ensure(k), "alloc groups");
+    CK(rb.g_isum_lo.ensure(k), "alloc groups");
+    CK(rb.g_isum_hi.ensure(k), "alloc groups");
+    CK(rb.g_n_int.ensure(k), "alloc groups");
+    CK(rb.g_min.ensure(k), "alloc groups");
+    CK(rb.g_max.ensure(k), "alloc groups");
+    CK(rb.g_fsum.ensure(k), "alloc groups");
+    CK(rb.g_saw.ensure(k), "alloc groups");
+  }
+  return WARPJQ_OK;
+}
+
+GroupTable group_view(RunBufs &rb, bool on) {
+  GroupTable g{};
+  if (!on) return g;
+  g.slots = rb.g_slots.p;
+  g.cap_mask = rb.g_cap - 1;
+  g.key_cap = rb.g_key_cap;
+  g.key_off = rb.g_key_off.p;
+  g.key_len = rb.g_key_len.p;
+  g.key_kind = rb.g_key_kind.p;
+  g.key_esc = rb.g_key_esc.p;
+  g.count = rb.g_count.p;
+  g.numeric = rb.g_numeric.p;
+  g.isum_lo = rb.g_isum_lo.p;
+  g.isum_hi = rb.g_isum_hi.p;
+  g.n_int = rb.g_n_int.p;
+  g.min_bits = rb.g_min.p;
+  g.max_bits = rb.g_max.p;
+  g.fsum = rb.g_fsum.p;
+  g.saw_non_numeric = rb.g_saw.p;
+  return g;
+}
+
+// Enqueues one run over n bytes at d_data on `st`.  No host synchronisation.
+warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigned long long n,
+                          cudaStream_t st, char *err, size_t err_len) {
+  warpjq_status rc = ensure_bufs(c, s, n, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  RunBufs &rb = s.rb;
+  const DevPlan &P = c->plan;
+  bool groups = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
+  unsigned long long n_tiles = (n + c->tile_bytes - 1) / c->tile_bytes;
+  GroupTable g = group_view(rb, groups);
+  s.kernels = 0;
+  k_reset_run<<<256, 256, 0, st>>>(rb.ctr.p, P.needs_rows ? rb.lb_flag.p : nullptr, n_tiles, g,
+                                   groups ? rb.g_cap : 0, groups ? rb.g_key_cap : 0);
+  s.kernels++;
+  CK(cudaGetLastError(), "launch reset");
+  if (n > 0) {
+    ScanParams sp{};
+    sp.data = d_data;
+    sp.n = n;
+    sp.plan = c->d_plan;
+    sp.tile_bytes = c->tile_bytes;
+    sp.halo_bytes = c->halo_bytes;
+    sp.n_tiles = n_tiles;
+    sp.ctr = rb.ctr.p;
+    sp.tiles = rb.tiles.p;
+    sp.lb_flag = rb.lb_flag.p;
+    sp.lb_agg = rb.lb_agg.p;
+    sp.lb_incl = rb.lb_incl.p;
+    sp.rec_scratch = rb.recs.p;
+    sp.rec_cap_per_cta = rb.rec_cap_per_cta;
+    sp.out = rb.out.p;
+    sp.out_cap = rb.out_cap;
+    sp.row_off = rb.row_off.p;
+    sp.line_idx = rb.line_idx.p;
+    sp.rows_cap = rb.rows_cap;
+    sp.tile_fsum = rb.tile_fsum.p;
+    sp.g = g;
+    sp.deep_words = rb.deep.p;
+    sp.deep_levels_per_cta = rb.deep_levels;
+    sp.spin_limit = 1ull << 24;
+    unsigned grid = (unsigned)std::min<unsigned long long>(c->grid, n_tiles);
+    if (P.needs_rows)
+      k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp);
+    else
+      k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp);
+    s.kernels++;
+    CK(cudaGetLastError(), "launch scan");
+    k_reduce_tiles<<<kReduceBlocks, kThreads, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
+                                                       n_tiles, rb.block_f.p, rb.tiles.p,
+                                                       rb.ctr.p, rb.block_lines.p);
+    s.kernels++;
+    CK(cudaGetLastError(), "launch reduce");
+    k_finalize<<<1, 32, 0, st>>>(rb.block_f.p, rb.block_lines.p, kReduceBlocks, rb.tiles.p,
+                                 rb.ctr.p, P.needs_rows ? rb.lb_incl.p : nullptr, n_tiles,
+                                 P.needs_rows ? rb.row_off.p : nullptr, rb.rows_cap);
+    s.kernels++;
+    CK(cudaGetLastError(), "launch finalize");
+  }
+  s.launched = true;
+  return WARPJQ_OK;
+}
+
+// After a run finished: grows whatever overflowed.  Returns true if the run
+// has to be repeated.
+bool grow_after_overflow(warpjq_ctx *c, Slot &s, const RunCounters &h, unsigned long long n) {
+  RunBufs &rb = s.rb;
+  bool again = false;
+  if (h.overflow & 1u) {  // records per tile
+    rb.rec_cap_per_cta = std::min<unsigned long long>(rb.rec_cap_per_cta * 4, c->tile_bytes);
+    rb.recs.release();
+    again = true;
+  }
+  if (h.overflow & 2u) {  // output bytes or row count; both totals are exact
+    unsigned long long need_rows = h.n_selected + 1;
+    if (need_rows > rb.rows_cap) {
+      rb.rows_cap = need_rows + need_rows / 8;
+      rb.row_off.release();
+      rb.line_idx.release();
+    }
+    if (h.out_len > rb.out_cap) {
+      rb.out_cap = h.out_len + h.out_len / 8 + 1;
+      rb.out.release();
+    }
+    again = true;
+  }
+  if (h.overflow & 4u) {  // group table
+    rb.g_key_cap = std::max<uint32_t>(rb.g_key_cap * 2, (uint32_t)std::min<unsigned long long>(h.n_keys * 2ull, 1u << 30));
+    rb.g_cap = 1;
+    while (rb.g_cap < rb.g_key_cap * 2u) rb.g_cap <<= 1;
+    rb.g_key_cap = rb.g_cap / 2;
+    rb.g_slots.release();
+    rb.g_key_off.release(); rb.g_key_len.release(); rb.g_key_kind.release(); rb.g_key_esc.release();
+    rb.g_count.release(); rb.g_numeric.release(); rb.g_isum_lo.release(); rb.g_isum_hi.release();
+    rb.g_n_int.release(); rb.g_min.release(); rb.g_max.release(); rb.g_fsum.release();
+    rb.g_saw.release();
+    again = true;
+  }
+  if (h.overflow & 8u) {  // deep nesting
+    rb.deep_levels = std::min<unsigned long long>(rb.deep_levels * 16, ((n + 31) / 32) * 32 + 64);
+    rb.deep.release();
+    again = true;
+  }
+  return again;
+}
+
+// Runs synchronously until the result is complete; leaves counters in h.
+warpjq_status run_to_completion(warpjq_ctx *c, Slot &s, const uint8_t *d_data,
+                                unsigned long long n, cudaStream_t st, RunCounters &h,
+                                bool already_enqueued, char *err, size_t err_len) {
+  for (int attempt = 0; attempt < 16; attempt++) {
+    if (!already_enqueued || attempt > 0) {
+      warpjq_status rc = enqueue_run(c, s, d_data, n, st, err, err_len);
+      if (rc != WARPJQ_OK) return rc;
+    }
+    CK(cudaMemcpyAsync(&h, s.rb.ctr.p, sizeof(RunCounters), cudaMemcpyDeviceToHost, st),
+       "D2H counters");
+    CK(cudaStreamSynchronize(st), "stream sync");
+    if (h.error) {
+      set_err(err, err_len, "a device-side wait gave up (look-back did not complete)");
+      return WARPJQ_ERR_CUDA;
+    }
+    if (!h.overflow) return WARPJQ_OK;
+    if (!grow_after_overflow(c, s, h, n)) return WARPJQ_OK;
+  }
+  set_err(err, err_len, "device buffers kept overflowing");
+  return WARPJQ_ERR_OOM;
+}
+
+double i128_to_double(unsigned long long lo, unsigned long long hi) {
+  __int128 v = (__int128)(((unsigned __int128)hi << 64) | lo);
+  return (double)v;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+warpjq_status warpjq_probe(char *err, size_t err_len) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_err(err, err_len, "no CUDA device: %s", e == cudaSuccess ? "none found" : cudaGetErrorString(e));
+    return WARPJQ_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp p;
+  e = cudaGetDeviceProperties(&p, 0);
+  if (e != cudaSuccess) {
+    set_err(err, err_len, "%s", cudaGetErrorString(e));
+    return WARPJQ_ERR_NO_DEVICE;
+  }
+  if (p.major < 10) {
+    set_err(err, err_len, "device 0 is sm_%d%d; this backend is built for sm_100a", p.major, p.minor);
+    return WARPJQ_ERR_NO_DEVICE;
+  }
+  return WARPJQ_OK;
+}
+
+// Sizes of step, path, cmp, cond_op, agg_partial, group, in that order
+// (reference warpjq_kernels.cu:2267-2277, gpu/ffi.rs:222-242).
+warpjq_status warpjq_abi_check(const uint64_t *sizes, size_t n) {
+  const uint64_t mine[6] = {sizeof(warpjq_step), sizeof(warpjq_path), sizeof(warpjq_cmp),
+                            sizeof(warpjq_cond_op), sizeof(warpjq_agg_partial),
+                            sizeof(warpjq_group)};
+  if (!sizes || n != 6) return WARPJQ_ERR_ABI;
+  for (int i = 0; i < 6; i++)
+    if (sizes[i] != mine[i]) return WARPJQ_ERR_ABI;
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_device_name(char *buf, size_t len) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, 0) != cudaSuccess) return WARPJQ_ERR_NO_DEVICE;
+  set_err(buf, len, "%s (sm_%d%d, %zu MiB)", p.name, p.major, p.minor,
+          (size_t)(p.totalGlobalMem >> 20));
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_ctx_create(const warpjq_program *prog, uint64_t max_chunk_bytes,
+                                uint32_t n_slots, warpjq_ctx **out, char *err, size_t err_len) {
+  if (!out || n_slots == 0 || n_slots > 8 || max_chunk_bytes >= (1ull << 40)) {
+    set_err(err, err_len, "invalid context arguments");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  warpjq_status rc = warpjq_probe(err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  std::unique_ptr<warpjq_ctx> c(new warpjq_ctx());
+  rc = build_plan(prog, c->plan, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  CK(cudaGetDevice(&c->device), "cudaGetDevice");
+  CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+  CK(cudaMalloc((void **)&c->d_plan, sizeof(DevPlan)), "alloc plan");
+  CK(cudaMemcpy(c->d_plan, &c->plan, sizeof(DevPlan), cudaMemcpyHostToDevice), "upload plan");
+  rc = configure_grid(c.get(), err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  c->chunk_cap = max_chunk_bytes;
+  c->slots.resize(n_slots);
+  for (auto &s : c->slots) {
+    CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream");
+    CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming), "event");
+    CK(cudaHostAlloc((void **)&s.h_chunk, std::max<uint64_t>(max_chunk_bytes, 16), cudaHostAllocDefault),
+       "pinned chunk");
+    CK(cudaMalloc((void **)&s.d_chunk, max_chunk_bytes + 16), "device chunk");
+    CK(cudaHostAlloc((void **)&s.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
+    if (max_chunk_bytes) {
+      rc = ensure_bufs(c.get(), s, max_chunk_bytes, err, err_len);
+      if (rc != WARPJQ_OK) return rc;
+    }
+  }
+  CK(cudaHostAlloc((void **)&c->dev.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
+  *out = c.release();
+  return WARPJQ_OK;
+}
+
+static void free_slot(Slot &s) {
+  s.rb.release();
+  if (s.stream) cudaStreamDestroy(s.stream);
+  if (s.done) cudaEventDestroy(s.done);
+  if (s.h_chunk) cudaFreeHost(s.h_chunk);
+  if (s.d_chunk) cudaFree(s.d_chunk);
+  if (s.h_ctr) cudaFreeHost(s.h_ctr);
+  if (s.h_out) cudaFreeHost(s.h_out);
+  if (s.h_row_off) cudaFreeHost(s.h_row_off);
+  if (s.h_line64) cudaFreeHost(s.h_line64);
+  if (s.h_line32) cudaFreeHost(s.h_line32);
+  if (s.h_groups) cudaFreeHost(s.h_groups);
+  s = Slot();
+}
+
+void warpjq_ctx_destroy(warpjq_ctx *ctx) {
+  if (!ctx) return;
+  cudaDeviceSynchronize();
+  for (auto &s : ctx->slots) free_slot(s);
+  free_slot(ctx->dev);
+  if (ctx->d_plan) cudaFree(ctx->d_plan);
+  delete ctx;
+}
+
+uint8_t *warpjq_slot_buffer(warpjq_ctx *ctx, uint32_t slot) {
+  if (!ctx || slot >= ctx->slots.size()) return nullptr;
+  return ctx->slots[slot].h_chunk;
+}
+
+uint64_t warpjq_slot_capacity(const warpjq_ctx *ctx) { return ctx ? ctx->chunk_cap : 0; }
+
+// Every line of a chunk is decided on the device, however short, so the
+// line budget is simply the byte capacity.
+uint64_t warpjq_max_lines(const warpjq_ctx *ctx) { return ctx ? ctx->chunk_cap + 1 : 0; }
+
+warpjq_status warpjq_submit(warpjq_ctx *ctx, uint32_t slot, uint64_t n_bytes, char *err,
+                            size_t err_len) {
+  if (!ctx || slot >= ctx->slots.size() || n_bytes > ctx->chunk_cap) {
+    set_err(err, err_len, "submit: bad slot or %llu bytes over the slot capacity",
+            (unsigned long long)n_bytes);
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  Slot &s = ctx->slots[slot];
+  s.n_bytes = n_bytes;
+  if (n_bytes)
+    CK(cudaMemcpyAsync(s.d_chunk, s.h_chunk, n_bytes, cudaMemcpyHostToDevice, s.stream), "H2D chunk");
+  warpjq_status rc = enqueue_run(ctx, s, s.d_chunk, n_bytes, s.stream, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  CK(cudaEventRecord(s.done, s.stream), "event record");
+  return WARPJQ_OK;
+}
+
+static warpjq_status ensure_pinned(Slot &s, size_t out_bytes, size_t rows, size_t groups,
+                                   char *err, size_t err_len) {
+  if (out_bytes > s.h_out_cap || !s.h_out) {
+    if (s.h_out) cudaFreeHost(s.h_out);
+    s.h_out = nullptr;
+    size_t cap = std::max<size_t>(out_bytes + out_bytes / 4, 1 << 16);
+    CK(cudaHostAlloc((void **)&s.h_out, cap, cudaHostAllocDefault), "pinned rows");
+    s.h_out_cap = cap;
+  }
+  if (rows + 1 > s.h_rows_cap || !s.h_row_off) {
+    if (s.h_row_off) cudaFreeHost(s.h_row_off);
+    if (s.h_line64) cudaFreeHost(s.h_line64);
+    if (s.h_line32) cudaFreeHost(s.h_line32);
+    size_t cap = std::max<size_t>(rows + rows / 4 + 1, 1024);
+    CK(cudaHostAlloc((void **)&s.h_row_off, cap * 8, cudaHostAllocDefault), "pinned row offsets");
+    CK(cudaHostAlloc((void **)&s.h_line64, cap * 8, cudaHostAllocDefault), "pinned line index");
+    CK(cudaHostAlloc((void **)&s.h_line32, cap * 4, cudaHostAllocDefault), "pinned line index");
+    s.h_rows_cap = cap;
+  }
+  if (groups > s.h_groups_cap || !s.h_groups) {
+    if (s.h_groups) cudaFreeHost(s.h_groups);
+    size_t cap = std::max<size_t>(groups + groups / 4, 256);
+    CK(cudaHostAlloc((void **)&s.h_groups, cap * sizeof(warpjq_group), cudaHostAllocDefault),
+       "pinned groups");
+    s.h_groups_cap = cap;
+  }
+  return WARPJQ_OK;
+}
+
+// Copies the compacted group table of a finished run to the host.
+static warpjq_status fetch_groups(warpjq_ctx *ctx, Slot &s, const RunCounters &h,
+                                  std::vector<warpjq_group_ext> &out, char *err, size_t err_len) {
+  out.clear();
+  uint32_t nk = std::min<uint32_t>(h.n_keys, s.rb.g_key_cap);
+  if (!nk) return WARPJQ_OK;
+  std::vector<unsigned long long> off(nk), cnt(nk), num(nk), lo(nk), hi(nk), ni(nk), mn(nk), mx(nk);
+  std::vector<uint32_t> len(nk);
+  std::vector<uint8_t> kind(nk);
+  std::vector<double> fs(nk);
+  RunBufs &rb = s.rb;
+  CK(cudaMemcpy(off.data(), rb.g_key_off.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(len.data(), rb.g_key_len.p, nk * 4, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(kind.data(), rb.g_key_kind.p, nk, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(cnt.data(), rb.g_count.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(num.data(), rb.g_numeric.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(lo.data(), rb.g_isum_lo.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(hi.data(), rb.g_isum_hi.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(ni.data(), rb.g_n_int.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(mn.data(), rb.g_min.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(mx.data(), rb.g_max.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(fs.data(), rb.g_fsum.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  for (uint32_t k = 0; k < nk; k++) {
+    if (cnt[k] == 0) continue;  // an id allocated by a racing insert that lost
+    warpjq_group_ext g{};
+    g.key_off = off[k];
+    g.key_len = len[k];
+    g.key_kind = kind[k];
+    g.count = cnt[k];
+    g.numeric = num[k];
+    g.isum_lo = lo[k];
+    g.isum_hi = hi[k];
+    g.n_int = ni[k];
+    g.fsum = fs[k];
+    g.min = num[k] ? from_order_bits(mn[k]) : 1.0 / 0.0;
+    g.max = num[k] ? from_order_bits(mx[k]) : -1.0 / 0.0;
+    g.sum = (ni[k] ? i128_to_double(lo[k], hi[k]) : 0.0) + fs[k];
+    out.push_back(g);
+  }
+  (void)ctx;
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_wait(warpjq_ctx *ctx, uint32_t slot, warpjq_chunk_result *out, char *err,
+                          size_t err_len) {
+  if (!ctx || slot >= ctx->slots.size() || !out) return WARPJQ_ERR_INVALID_ARG;
+  Slot &s = ctx->slots[slot];
+  std::memset(out, 0, sizeof(*out));
+  out->first_invalid = 0xFFFFFFFFu;
+  if (!s.launched) return WARPJQ_OK;
+  RunCounters h;
+  warpjq_status rc = run_to_completion(ctx, s, s.d_chunk, s.n_bytes, s.stream, h, true, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  const DevPlan &P = ctx->plan;
+  out->n_lines = h.n_lines;
+  out->n_blank = h.n_blank;
+  out->n_invalid = h.n_invalid;
+  out->n_type_error = h.n_type_error;
+  out->n_selected = P.needs_rows ? h.n_selected : 0;
+  out->first_invalid = h.first_invalid == ~0ull ? 0xFFFFFFFFu : (uint32_t)h.first_invalid;
+  s.last_first_invalid = h.first_invalid;
+  s.last_first_type = h.first_type_error;
+  if (P.output_kind == WARPJQ_OUT_AGG) {
+    out->n_selected = 0;
+    if (P.group_slot < 0) {
+      out->agg.count = h.agg_count;
+      out->agg.numeric = h.agg_numeric;
+      out->agg.sum = (h.agg_n_int ? i128_to_double(h.agg_isum_lo, h.agg_isum_hi) : 0.0) + h.fsum_total;
+      out->agg.min = h.agg_numeric ? from_order_bits(h.agg_min_bits) : 1.0 / 0.0;
+      out->agg.max = h.agg_numeric ? from_order_bits(h.agg_max_bits) : -1.0 / 0.0;
+      out->agg.saw_non_numeric = h.agg_saw_non_numeric;
+    } else {
+      std::vector<warpjq_group_ext> gs;
+      rc = fetch_groups(ctx, s, h, gs, err, err_len);
+      if (rc != WARPJQ_OK) return rc;
+      rc = ensure_pinned(s, 0, 0, gs.size(), err, err_len);
+      if (rc != WARPJQ_OK) return rc;
+      for (size_t k = 0; k < gs.size(); k++) {
+        warpjq_group &d = s.h_groups[k];
+        d.key_off = (uint32_t)gs[k].key_off;
+        d.key_len = gs[k].key_len;
+        d.key_kind = gs[k].key_kind;
+        d._pad = 0;
+        d.count = gs[k].count;
+        d.numeric = gs[k].numeric;
+        d.sum = gs[k].sum;
+        d.min = gs[k].min;
+        d.max = gs[k].max;
+      }
+      out->groups = s.h_groups;
+      out->n_groups = (uint32_t)gs.size();
+    }
+    return WARPJQ_OK;
+  }
+  size_t nsel = h.n_selected;
+  rc = ensure_pinned(s, h.out_len, nsel, 0, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  if (nsel) {
+    CK(cudaMemcpy(s.h_row_off, s.rb.row_off.p, (nsel + 1) * 8, cudaMemcpyDeviceToHost), "D2H row offsets");
+    CK(cudaMemcpy(s.h_line64, s.rb.line_idx.p, nsel * 8, cudaMemcpyDeviceToHost), "D2H line index");
+    if (h.out_len)
+      CK(cudaMemcpy(s.h_out, s.rb.out.p, h.out_len, cudaMemcpyDeviceToHost), "D2H rows");
+    for (size_t k = 0; k < nsel; k++) s.h_line32[k] = (uint32_t)s.h_line64[k];
+  } else {
+    s.h_row_off[0] = 0;
+  }
+  out->out_bytes = s.h_out;
+  out->out_len = h.out_len;
+  out->out_line_idx = s.h_line32;
+  out->out_row_off = (const uint64_t *)s.h_row_off;
+  return WARPJQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident extension
+// ---------------------------------------------------------------------------
+
+warpjq_status warpjq_slot_first_errors(warpjq_ctx *ctx, uint32_t slot, uint64_t *first_invalid,
+                                       uint64_t *first_type_error) {
+  if (!ctx || slot >= ctx->slots.size()) return WARPJQ_ERR_INVALID_ARG;
+  if (first_invalid) *first_invalid = ctx->slots[slot].last_first_invalid;
+  if (first_type_error) *first_type_error = ctx->slots[slot].last_first_type;
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t halo_bytes) {
+  char *err = nullptr;
+  size_t err_len = 0;
+  if (!ctx) return WARPJQ_ERR_INVALID_ARG;
+  uint32_t T = tile_bytes ? tile_bytes : ctx->tile_bytes;
+  uint32_t H = halo_bytes ? halo_bytes : ctx->halo_bytes;
+  if (T % 1024 || H % 1024 || T < 4096 || T + H > 65535 - 16) return WARPJQ_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize(), "sync");
+  ctx->tile_bytes = T;
+  ctx->halo_bytes = H;
+  for (auto &s : ctx->slots) s.rb.release();
+  ctx->dev.rb.release();
+  return configure_grid(ctx, err, err_len);
+}
+
+warpjq_status warpjq_launch_device(warpjq_ctx *ctx, const uint8_t *d_data, uint64_t n_bytes,
+                                   void *stream, char *err, size_t err_len) {
+  if (!ctx || (!d_data && n_bytes)) return WARPJQ_ERR_INVALID_ARG;
+  if (((uintptr_t)d_data & 15u) != 0) {
+    set_err(err, err_len, "device input must be 16-byte aligned");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  ctx->dev_data = d_data;
+  ctx->dev_n = n_bytes;
+  ctx->dev_stream = (cudaStream_t)stream;
+  return enqueue_run(ctx, ctx->dev, d_data, n_bytes, (cudaStream_t)stream, err, err_len);
+}
+
+warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, char *err,
+                                    size_t err_len) {
+  if (!ctx || !out) return WARPJQ_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  Slot &s = ctx->dev;
+  if (!s.launched) return WARPJQ_ERR_INVALID_ARG;
+  RunCounters h;
+  warpjq_status rc =
+      run_to_completion(ctx, s, ctx->dev_data, ctx->dev_n, ctx->dev_stream, h, true, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  const DevPlan &P = ctx->plan;
+  out->n_lines = h.n_lines;
+  out->n_blank = h.n_blank;
+  out->n_invalid = h.n_invalid;
+  out->n_type_error = h.n_type_error;
+  out->n_selected = h.n_selected;
+  out->first_invalid = h.first_invalid;
+  out->first_type_error = h.first_type_error;
+  if (P.needs_rows) {
+    out->d_out_bytes = s.rb.out.p;
+    out->out_len = h.out_len;
+    out->d_out_line_idx = (const uint64_t *)s.rb.line_idx.p;
+    out->d_out_row_off = (const uint64_t *)s.rb.row_off.p;
+  }
+  out->count = h.agg_count;
+  out->numeric = h.agg_numeric;
+  out->isum_lo = h.agg_isum_lo;
+  out->isum_hi = h.agg_isum_hi;
+  out->n_int = h.agg_n_int;
+  out->fsum = h.fsum_total;
+  out->min = h.agg_numeric ? from_order_bits(h.agg_min_bits) : 1.0 / 0.0;
+  out->max = h.agg_numeric ? from_order_bits(h.agg_max_bits) : -1.0 / 0.0;
+  out->sum = (h.agg_n_int ? i128_to_double(h.agg_isum_lo, h.agg_isum_hi) : 0.0) + h.fsum_total;
+  out->saw_non_numeric = h.agg_saw_non_numeric;
+  if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
+    rc = fetch_groups(ctx, s, h, ctx->dev_groups, err, err_len);
+    if (rc != WARPJQ_OK) return rc;
+    out->groups = ctx->dev_groups.data();
+    out->n_groups = (uint32_t)ctx->dev_groups.size();
+  }
+  out->kernels_launched = s.kernels;
+  return WARPJQ_OK;
+}
+
+}  // extern "C"

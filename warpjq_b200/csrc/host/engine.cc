@@ -1,0 +1,591 @@
+// Host driver of the GPU backend: the role the reference's Rust host plays
+// around the device ABI (crates/warpjq-core/src/gpu/mod.rs:244-1259 and the
+// formatting of agg.rs / output.rs / exec/mod.rs).
+//
+// It splits the input into newline-aligned chunks, keeps two device slots in
+// flight (fill n+1 while n computes), merges every chunk's rows and
+// aggregates in input order, and formats the output bytes.  There is no CPU
+// evaluation of any line: every line of every chunk is decided on the device.
+#include <algorithm>
+#include <charconv>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../../include/warpjq_ext.h"
+#include "../../../include/warpjq_host.h"
+#include "query.h"
+
+namespace wjqh {
+
+// ---------------------------------------------------------------------------
+// Number formatting and value rendering (agg.rs:253-278, output.rs:24-81)
+// ---------------------------------------------------------------------------
+
+// Integral values below 2^53 print as integers; others print their shortest
+// round-trip digits, placed as the `ryu` crate's pretty printer places them,
+// with an explicit `+` on positive exponents.
+std::string format_number(double v) {
+  if (std::isnan(v)) return "null";
+  if (std::isinf(v)) return v > 0 ? "1.7976931348623157e+308" : "-1.7976931348623157e+308";
+  if (std::trunc(v) == v && std::fabs(v) < 9007199254740992.0) return std::to_string((long long)v);
+  char buf[64];
+  auto r = std::to_chars(buf, buf + sizeof buf, v, std::chars_format::scientific);
+  std::string s(buf, r.ptr), digits;
+  bool neg = s[0] == '-';
+  size_t e = s.find('e');
+  for (size_t k = neg; k < e; k++)
+    if (s[k] != '.') digits += s[k];
+  long exp10 = std::strtol(s.c_str() + e + 1, nullptr, 10);
+  long len = (long)digits.size(), kk = exp10 + 1, k = kk - len;
+  std::string o = neg ? "-" : "";
+  if (k >= 0 && kk <= 16) {
+    o += digits + std::string((size_t)k, '0') + ".0";
+  } else if (kk > 0 && kk <= 16) {
+    o += digits.substr(0, (size_t)kk) + "." + digits.substr((size_t)kk);
+  } else if (kk > -5 && kk <= 0) {
+    o += "0." + std::string((size_t)-kk, '0') + digits;
+  } else {
+    o += digits.substr(0, 1);
+    if (len > 1) o += "." + digits.substr(1);
+    o += "e" + std::string(kk - 1 >= 0 ? "+" : "") + std::to_string(kk - 1);
+  }
+  return o;
+}
+
+void json_string(std::string &o, const uint8_t *p, size_t n) {
+  o += '"';
+  for (size_t i = 0; i < n; i++) {
+    uint8_t c = p[i];
+    switch (c) {
+      case '"': o += "\\\""; break;
+      case '\\': o += "\\\\"; break;
+      case '\n': o += "\\n"; break;
+      case '\r': o += "\\r"; break;
+      case '\t': o += "\\t"; break;
+      case 0x08: o += "\\b"; break;
+      case 0x0C: o += "\\f"; break;
+      default:
+        if (c < 0x20) {
+          char b[8];
+          snprintf(b, sizeof b, "\\u%04x", c);
+          o += b;
+        } else o += (char)c;
+    }
+  }
+  o += '"';
+}
+
+void csv_cell(std::string &o, const uint8_t *p, size_t n) {
+  bool q = false;
+  for (size_t i = 0; i < n && !q; i++) q = p[i] == ',' || p[i] == '"' || p[i] == '\n' || p[i] == '\r';
+  if (!q) {
+    o.append((const char *)p, n);
+    return;
+  }
+  o += '"';
+  for (size_t i = 0; i < n; i++) {
+    if (p[i] == '"') o += '"';
+    o += (char)p[i];
+  }
+  o += '"';
+}
+
+// Decodes a validated JSON string body (json.rs:594-654).
+std::string unescape(const uint8_t *p, size_t n) {
+  std::string o;
+  auto hex4 = [&](size_t at) {
+    uint32_t v = 0;
+    for (int k = 0; k < 4; k++) {
+      uint8_t c = p[at + k];
+      v = v * 16 + (c <= '9' ? c - '0' : (c | 0x20) - 'a' + 10);
+    }
+    return v;
+  };
+  for (size_t i = 0; i < n;) {
+    if (p[i] != '\\') {
+      o += (char)p[i++];
+      continue;
+    }
+    uint8_t e = p[i + 1];
+    i += 2;
+    if (e != 'u') {
+      const char *from = "\"\\/bfnrt", *to = "\"\\/\b\f\n\r\t";
+      o += to[strchr(from, e) - from];
+      continue;
+    }
+    uint32_t cp = hex4(i);
+    i += 4;
+    if (cp >= 0xD800 && cp < 0xDC00 && i + 6 <= n && p[i] == '\\' && p[i + 1] == 'u') {
+      uint32_t lo = hex4(i + 2);
+      if (lo >= 0xDC00 && lo < 0xE000) {
+        cp = 0x10000 + ((cp - 0xD800) << 10) + (lo - 0xDC00);
+        i += 6;
+      }
+    }
+    if (cp >= 0xD800 && cp < 0xE000) cp = 0xFFFD;
+    if (cp < 0x80) o += (char)cp;
+    else if (cp < 0x800) {
+      o += (char)(0xC0 | cp >> 6);
+      o += (char)(0x80 | (cp & 0x3F));
+    } else if (cp < 0x10000) {
+      o += (char)(0xE0 | cp >> 12);
+      o += (char)(0x80 | ((cp >> 6) & 0x3F));
+      o += (char)(0x80 | (cp & 0x3F));
+    } else {
+      o += (char)(0xF0 | cp >> 18);
+      o += (char)(0x80 | ((cp >> 12) & 0x3F));
+      o += (char)(0x80 | ((cp >> 6) & 0x3F));
+      o += (char)(0x80 | (cp & 0x3F));
+    }
+  }
+  return o;
+}
+
+// ---------------------------------------------------------------------------
+// Aggregation state and group keys (agg.rs:17-249)
+// ---------------------------------------------------------------------------
+
+struct Agg {
+  uint64_t count = 0, numeric = 0;
+  double sum = 0, min = INFINITY, max = -INFINITY;
+  void merge(uint64_t c, uint64_t nu, double s, double mn, double mx) {
+    count += c;
+    numeric += nu;
+    sum += s;
+    if (mn < min) min = mn;
+    if (mx > max) max = mx;
+  }
+  bool finish(uint32_t kind, double &v) const {
+    switch (kind) {
+      case WARPJQ_AGG_COUNT: v = (double)count; return true;
+      case WARPJQ_AGG_SUM: v = sum; return true;
+      case WARPJQ_AGG_MIN: v = min; return numeric > 0;
+      case WARPJQ_AGG_MAX: v = max; return numeric > 0;
+      default: v = sum / (double)numeric; return numeric > 0;
+    }
+  }
+};
+
+uint64_t order_bits(double v) {
+  uint64_t b;
+  memcpy(&b, &v, 8);
+  return (b >> 63) ? ~b : (b ^ (1ull << 63));
+}
+
+// rank: 0 null, 1 false, 2 true, 3 number, 4 string, 5 array/object
+struct GroupKey {
+  uint8_t rank = 0;
+  std::string bytes;
+  uint64_t bits = 0;
+  bool operator==(const GroupKey &o) const { return rank == o.rank && bytes == o.bytes; }
+  // jq order; equal numbers with different spellings tie-break on the text.
+  bool operator<(const GroupKey &o) const {
+    if (rank != o.rank) return rank < o.rank;
+    if (rank == 3 && bits != o.bits) return bits < o.bits;
+    return bytes < o.bytes;
+  }
+  std::string json() const {
+    if (rank == 0) return "null";
+    if (rank == 1) return "false";
+    if (rank == 2) return "true";
+    if (rank == 4) {
+      std::string o;
+      json_string(o, (const uint8_t *)bytes.data(), bytes.size());
+      return o;
+    }
+    return bytes;
+  }
+  std::string plain() const { return rank == 4 ? bytes : json(); }
+};
+struct KeyHash {
+  size_t operator()(const GroupKey &k) const { return std::hash<std::string>()(k.bytes) ^ k.rank; }
+};
+
+// Rebuilds a key from a device group entry (gpu/mod.rs:1198-1221).
+GroupKey device_key(const uint8_t *data, uint64_t off, uint32_t len, uint32_t kind) {
+  GroupKey k;
+  const uint8_t *raw = data + off;
+  switch (kind) {
+    case 0: case 1: k.rank = 0; break;
+    case 2: k.rank = (len == 4 && memcmp(raw, "true", 4) == 0) ? 2 : 1; break;
+    case 3: {
+      k.rank = 3;
+      k.bytes.assign((const char *)raw, len);
+      k.bits = order_bits(strtod(k.bytes.c_str(), nullptr));
+      break;
+    }
+    case 4:
+      k.rank = 4;
+      k.bytes = memchr(raw, '\\', len) ? unescape(raw, len) : std::string((const char *)raw, len);
+      break;
+    default:
+      k.rank = 5;
+      k.bytes.assign((const char *)raw, len);
+  }
+  return k;
+}
+
+// ---------------------------------------------------------------------------
+// Output writer (output.rs:87-334)
+// ---------------------------------------------------------------------------
+
+struct Writer {
+  std::string buf;
+  uint32_t fmt;  // WARPJQ_FMT_*
+  uint64_t rows = 0;
+  void header(const Program &p) {
+    if (fmt != WARPJQ_FMT_CSV) return;
+    std::vector<std::string> cols;
+    if (!p.csv_headers(cols)) return;
+    for (size_t i = 0; i < cols.size(); i++) {
+      if (i) buf += ',';
+      csv_cell(buf, (const uint8_t *)cols[i].data(), cols[i].size());
+    }
+    buf += '\n';
+  }
+  void bulk(const uint8_t *p, size_t n, uint64_t r) {
+    rows += r;
+    if (fmt != WARPJQ_FMT_COUNT) buf.append((const char *)p, n);
+  }
+  void aggregate(uint32_t kind, const Agg &a) {
+    rows++;
+    double v;
+    std::string val = a.finish(kind, v) ? format_number(v) : "null";
+    if (fmt == WARPJQ_FMT_COUNT) {
+      rows = 0;
+      buf = val + "\n";
+      fmt = WARPJQ_FMT_NDJSON;
+      return;
+    }
+    buf += val + "\n";
+  }
+  void groups(const std::string &name, uint32_t kind, const std::vector<std::pair<GroupKey, Agg>> &gs) {
+    for (auto &g : gs) {
+      rows++;
+      double v;
+      std::string val = g.second.finish(kind, v) ? format_number(v) : "null";
+      if (fmt == WARPJQ_FMT_CSV) {
+        std::string pl = g.first.plain();
+        csv_cell(buf, (const uint8_t *)pl.data(), pl.size());
+        buf += "," + val;
+      } else {
+        buf += '{';
+        json_string(buf, (const uint8_t *)name.data(), name.size());
+        buf += ':' + g.first.json() + ',';
+        const char *an = agg_name(kind);
+        json_string(buf, (const uint8_t *)an, strlen(an));
+        buf += ':' + val + '}';
+      }
+      buf += '\n';
+    }
+  }
+  std::string finish() {
+    if (fmt == WARPJQ_FMT_COUNT) buf = std::to_string(rows) + "\n";
+    return buf;
+  }
+};
+
+}  // namespace wjqh
+
+using namespace wjqh;
+
+struct warpjq_query {
+  Program prog;
+  Lowered low;
+  uint32_t fmt = WARPJQ_FMT_NDJSON;
+  warpjq_ctx *ctx = nullptr;
+  uint64_t cap = 0;
+  uint32_t n_slots = 2;
+};
+
+namespace {
+
+void put_err(char *err, size_t n, const std::string &m) {
+  if (!err || !n) return;
+  size_t k = std::min(m.size(), n - 1);
+  memcpy(err, m.data(), k);
+  err[k] = 0;
+}
+
+// Copies into pinned memory with several threads (gpu/mod.rs:934-956).
+void copy_to_pinned(uint8_t *dst, const uint8_t *src, size_t n) {
+  const size_t kMin = 1 << 20;
+  unsigned t = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 16);
+  if (n < kMin || t == 1) {
+    memcpy(dst, src, n);
+    return;
+  }
+  size_t piece = (n + t - 1) / t;
+  std::vector<std::thread> ws;
+  for (unsigned i = 0; i < t; i++) {
+    size_t a = i * piece, b = std::min(n, a + piece);
+    if (a >= b) break;
+    ws.emplace_back([=] { memcpy(dst + a, src + a, b - a); });
+  }
+  for (auto &w : ws) w.join();
+}
+
+struct Totals {
+  Agg scalar;
+  std::unordered_map<GroupKey, Agg, KeyHash> groups;
+};
+
+}  // namespace
+
+extern "C" {
+
+void warpjq_host_free(void *p) { free(p); }
+
+int warpjq_query_open(const char *query, uint32_t format, uint64_t chunk_bytes, warpjq_query **out,
+                      char *err, size_t err_len) {
+  *out = nullptr;
+  auto *q = new warpjq_query();
+  QueryError qe;
+  std::string src = query ? query : "";
+  if (!parse(src, q->prog, qe)) {
+    put_err(err, err_len, qe.render(src));
+    delete q;
+    return 2;
+  }
+  if (format == WARPJQ_FMT_CSV && q->prog.out == Out::Passthrough) {  // exec/mod.rs:256-266
+    put_err(err, err_len,
+            "--csv needs a query with named columns, but this one emits whole lines\n  help: project "
+            "the fields you want, e.g. `{ts: .ts, status: .status}`, or use an aggregate");
+    delete q;
+    return 1;
+  }
+  q->fmt = format;
+  q->low.build(q->prog, format == WARPJQ_FMT_CSV);
+  // gpu/mod.rs:143-145: the GPU chunk is capped at 64 MiB.
+  uint64_t cap = chunk_bytes ? chunk_bytes : (256ull << 20);
+  cap = std::min<uint64_t>(cap, std::max<uint64_t>(64ull << 20, 1 << 20));
+  q->cap = std::max<uint64_t>(cap, 1);
+  char e[512] = {0};
+  warpjq_status rc = warpjq_ctx_create(&q->low.prog, q->cap, q->n_slots, &q->ctx, e, sizeof e);
+  if (rc != WARPJQ_OK) {
+    put_err(err, err_len, std::string("CUDA error in creating the device context: ") + e);
+    delete q;
+    return 1;
+  }
+  *out = q;
+  return 0;
+}
+
+void warpjq_query_close(warpjq_query *q) {
+  if (!q) return;
+  if (q->ctx) warpjq_ctx_destroy(q->ctx);
+  delete q;
+}
+
+warpjq_ctx *warpjq_query_ctx(warpjq_query *q) { return q ? q->ctx : nullptr; }
+
+int warpjq_query_is_aggregate(const warpjq_query *q) { return q && q->prog.is_aggregate(); }
+
+int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t on_invalid,
+                     uint64_t max_line_bytes, char **out, size_t *out_len, uint64_t *stats,
+                     char *err, size_t err_len) {
+  *out = nullptr;
+  if (out_len) *out_len = 0;
+  if (!max_line_bytes) max_line_bytes = 64ull << 20;
+  const Program &P = q->prog;
+  Writer w;
+  w.fmt = q->fmt;
+  w.header(P);
+  Totals tot;
+  uint64_t st_lines = 0, st_malformed = 0, st_type = 0, lines_seen = 0;
+  char e[512] = {0};
+
+  // Strip a UTF-8 byte-order mark (chunk.rs:210-212).
+  size_t pos = (len >= 3 && data[0] == 0xEF && data[1] == 0xBB && data[2] == 0xBF) ? 3 : 0;
+
+  struct Flight {
+    uint32_t slot;
+    const uint8_t *data;
+    uint64_t n;
+  };
+  std::vector<Flight> flight;
+  uint32_t next_slot = 0;
+
+  auto fail = [&](const std::string &m) {
+    put_err(err, err_len, m);
+    return 1;
+  };
+
+  auto drain = [&](const Flight &f) -> int {
+    warpjq_chunk_result r;
+    warpjq_status rc = warpjq_wait(q->ctx, f.slot, &r, e, sizeof e);
+    if (rc != WARPJQ_OK) return fail(std::string("CUDA error in waiting for a chunk: ") + e);
+    uint64_t first_line = lines_seen + 1;
+    lines_seen += r.n_lines;
+    st_lines += r.n_lines - r.n_blank;
+    st_malformed += r.n_invalid;
+    st_type += r.n_type_error;
+    if (on_invalid == WARPJQ_ON_INVALID_ABORT && (r.n_invalid || r.n_type_error)) {
+      uint64_t fi = r.first_invalid == 0xFFFFFFFFu ? ~0ull : r.first_invalid;
+      uint64_t ft = ~0ull, dummy = 0;
+      warpjq_slot_first_errors(q->ctx, f.slot, &dummy, &ft);
+      uint64_t bad = std::min(fi, ft);
+      return fail("malformed JSON on line " + std::to_string(first_line + (bad == ~0ull ? 0 : bad)) +
+                  " of <memory>: " + (fi <= ft ? "line is not valid JSON" : "a path hit a value of the wrong type") +
+                  "\n  help: pass --skip-invalid to drop bad lines instead of stopping");
+    }
+    if (P.is_aggregate()) {
+      if (!P.has_group) {
+        tot.scalar.merge(r.agg.count, r.agg.numeric, r.agg.sum, r.agg.min, r.agg.max);
+      } else {
+        for (uint32_t k = 0; k < r.n_groups; k++) {
+          const warpjq_group &g = r.groups[k];
+          GroupKey key = device_key(f.data, g.key_off, g.key_len, g.key_kind);
+          tot.groups[key].merge(g.count, g.numeric, g.sum, g.min, g.max);
+        }
+      }
+    } else if (r.n_selected) {
+      w.bulk(r.out_bytes + r.out_row_off[0], (size_t)(r.out_row_off[r.n_selected] - r.out_row_off[0]),
+             r.n_selected);
+    }
+    return 0;
+  };
+
+  while (pos < len) {
+    // Next newline-aligned chunk of at most `cap` bytes (chunk.rs:234-278).
+    uint64_t want = std::min<uint64_t>(q->cap, len - pos);
+    uint64_t end = pos + want;
+    if (end < len) {
+      const uint8_t *nl = nullptr;
+      for (uint64_t k = end; k > pos; k--)
+        if (data[k - 1] == '\n') {
+          nl = data + k - 1;
+          break;
+        }
+      if (nl) {
+        end = (uint64_t)(nl - data) + 1;
+      } else {
+        // One line longer than a slot: grow the slots to hold it.
+        const uint8_t *n2 = (const uint8_t *)memchr(data + end, '\n', len - end);
+        end = n2 ? (uint64_t)(n2 - data) + 1 : len;
+      }
+    }
+    uint64_t n = end - pos;
+    // --max-line-bytes (chunk.rs:259-270): only a chunk without any newline
+    // but its last byte can hold an over-long line.
+    if (n > max_line_bytes) {
+      const uint8_t *inner = (const uint8_t *)memchr(data + pos, '\n', n - 1 > 0 ? n - 1 : 0);
+      if (!inner)
+        return fail("line " + std::to_string(lines_seen + 1) + " is at least " + std::to_string(n) +
+                    " bytes, over the " + std::to_string(max_line_bytes) +
+                    " byte limit (raise it with --max-line-bytes)");
+    }
+    if (n > q->cap) {
+      for (auto &f : flight)
+        if (drain(f)) return 1;
+      flight.clear();
+      warpjq_ctx_destroy(q->ctx);
+      q->ctx = nullptr;
+      q->cap = n;
+      if (warpjq_ctx_create(&q->low.prog, q->cap, q->n_slots, &q->ctx, e, sizeof e) != WARPJQ_OK)
+        return fail(std::string("CUDA error in creating the device context: ") + e);
+      next_slot = 0;
+    }
+    uint32_t slot = next_slot;
+    next_slot = (next_slot + 1) % q->n_slots;
+    // The slot being refilled must have been drained (two slots: n and n-2).
+    if (flight.size() >= q->n_slots) {
+      if (drain(flight.front())) return 1;
+      flight.erase(flight.begin());
+    }
+    copy_to_pinned(warpjq_slot_buffer(q->ctx, slot), data + pos, n);
+    if (warpjq_submit(q->ctx, slot, n, e, sizeof e) != WARPJQ_OK)
+      return fail(std::string("CUDA error in submitting a chunk: ") + e);
+    flight.push_back({slot, data + pos, n});
+    if (flight.size() > 1) {
+      if (drain(flight.front())) return 1;
+      flight.erase(flight.begin());
+    }
+    pos = end;
+  }
+  for (auto &f : flight)
+    if (drain(f)) return 1;
+
+  // exec/mod.rs:321-339
+  if (P.is_aggregate()) {
+    if (!P.has_group) {
+      w.aggregate(P.agg, tot.scalar);
+    } else {
+      std::vector<std::pair<GroupKey, Agg>> gs(tot.groups.begin(), tot.groups.end());
+      std::sort(gs.begin(), gs.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+      w.groups(P.group_key_name(), P.agg, gs);
+    }
+  }
+  uint64_t rows = w.rows;
+  std::string res = w.finish();
+  if (stats) {
+    stats[0] = len;
+    stats[1] = st_lines;
+    stats[2] = rows;
+    stats[3] = st_malformed;
+    stats[4] = st_type;
+  }
+  char *buf = (char *)malloc(res.size() + 1);
+  memcpy(buf, res.data(), res.size());
+  buf[res.size()] = 0;
+  *out = buf;
+  if (out_len) *out_len = res.size();
+  return 0;
+}
+
+int warpjq_run_bytes(const char *query, const uint8_t *data, size_t len, uint32_t format,
+                     uint32_t on_invalid, uint64_t chunk_bytes, uint64_t max_line_bytes, char **out,
+                     size_t *out_len, uint64_t *stats, char *err, size_t err_len) {
+  warpjq_query *q = nullptr;
+  *out = nullptr;
+  int rc = warpjq_query_open(query, format, chunk_bytes, &q, err, err_len);
+  if (rc) return rc;
+  rc = warpjq_query_run(q, data, len, on_invalid, max_line_bytes, out, out_len, stats, err, err_len);
+  warpjq_query_close(q);
+  return rc;
+}
+
+// Formats the result of a device-resident aggregate run (warpjq_ext.h) the
+// way the CLI prints it.  `data` is a host copy of the input, needed to
+// render group keys.
+int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r, const uint8_t *data,
+                               char **out, size_t *out_len) {
+  const Program &P = q->prog;
+  Writer w;
+  w.fmt = q->fmt;
+  w.header(P);
+  if (P.is_aggregate()) {
+    if (!P.has_group) {
+      Agg a;
+      a.merge(r->count, r->numeric, r->sum, r->min, r->max);
+      w.aggregate(P.agg, a);
+    } else {
+      std::vector<std::pair<GroupKey, Agg>> gs;
+      for (uint32_t k = 0; k < r->n_groups; k++) {
+        const warpjq_group_ext &g = r->groups[k];
+        Agg a;
+        a.merge(g.count, g.numeric, g.sum, g.min, g.max);
+        gs.push_back({device_key(data, g.key_off, g.key_len, g.key_kind), a});
+      }
+      std::sort(gs.begin(), gs.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+      w.groups(P.group_key_name(), P.agg, gs);
+    }
+  } else {
+    w.rows = r->n_selected;
+  }
+  std::string res = w.finish();
+  char *buf = (char *)malloc(res.size() + 1);
+  memcpy(buf, res.data(), res.size());
+  buf[res.size()] = 0;
+  *out = buf;
+  if (out_len) *out_len = res.size();
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,927 @@
+// The sm_100a scan kernels.
+//
+// One persistent kernel does the whole hot path of the reference's
+// k_nl_count / k_nl_write / k_build_lines / k_eval / DeviceSelect / k_row_len
+// / k_emit chain (warpjq_kernels.cu:1117-1849) in a single pass over the
+// input:
+//
+//   1. A CTA takes the next tile from a work ticket and stages tile + halo
+//      into shared memory with 16-byte loads, recording the newline mask.
+//   2. It lists the lines that start in the tile, in order.
+//   3. Each thread walks one line (walker.cuh), evaluates the filter and
+//      computes the row it will emit, or folds the line into the aggregate.
+//   4. Rows: the tile's row count and byte count are published and the
+//      exclusive prefix over all earlier tiles is obtained by decoupled
+//      look-back (tiles are taken in ticket order, so every earlier tile is
+//      owned by a running CTA); the CTA then writes its rows, in line order,
+//      straight from shared memory to the output.
+//
+// No host synchronisation happens inside a run; every wait is bounded.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "devutil.cuh"
+#include "plan.h"
+#include "walker.cuh"
+
+namespace wjq {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kMaxLinesPerPass = 4096;  // line-start list capacity per pass
+
+// Record of one selected row, staged per CTA until the look-back resolves.
+struct RowRec {
+  unsigned long long line_start;  // absolute offset of the line
+  uint32_t line_len;              // without '\n' and without a trailing '\r'
+  uint32_t ordinal;               // line index within the tile
+  uint32_t local_off;             // row offset within the tile's output
+  uint32_t row_len;
+  uint32_t in_window;             // line bytes are in the shared window
+  uint32_t pad;
+  // followed by n_fields x {uint32 off (relative to line), uint32 len|kind<<28|esc<<27}
+};
+
+struct GroupTable {
+  unsigned long long *slots;  // 0 = empty, else (hash << 32) | (key_id + 1)
+  uint32_t cap_mask;
+  uint32_t key_cap;
+  unsigned long long *key_off;
+  uint32_t *key_len;
+  uint8_t *key_kind;
+  uint8_t *key_esc;
+  unsigned long long *count;
+  unsigned long long *numeric;
+  unsigned long long *isum_lo;
+  unsigned long long *isum_hi;
+  unsigned long long *n_int;
+  unsigned long long *min_bits;
+  unsigned long long *max_bits;
+  double *fsum;
+  unsigned int *saw_non_numeric;
+};
+
+struct ScanParams {
+  const uint8_t *data;
+  unsigned long long n;
+  const DevPlan *plan;
+  uint32_t tile_bytes;
+  uint32_t halo_bytes;
+  unsigned long long n_tiles;
+  RunCounters *ctr;
+  TileDesc *tiles;
+  // look-back state, rows mode: per tile flag + aggregate + inclusive values
+  unsigned int *lb_flag;
+  unsigned long long *lb_agg;   // 3 per tile: rows, bytes, lines
+  unsigned long long *lb_incl;  // 3 per tile
+  // per-CTA record scratch
+  uint8_t *rec_scratch;
+  unsigned long long rec_cap_per_cta;  // records
+  // outputs
+  uint8_t *out;
+  unsigned long long out_cap;
+  unsigned long long *row_off;    // rows_cap + 1
+  unsigned long long *line_idx;   // rows_cap
+  unsigned long long rows_cap;
+  // per-tile FP partial sums (fixed-order reduction)
+  double *tile_fsum;
+  GroupTable g;
+  // deep-nesting scratch, per CTA
+  uint32_t *deep_words;
+  unsigned long long deep_levels_per_cta;
+  unsigned long long spin_limit;
+};
+
+// ---------------------------------------------------------------------------
+// Small block utilities
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Block-wide exclusive scan of (a, b) in thread order.
+__device__ __forceinline__ void block_scan2(uint32_t a, unsigned long long b, uint32_t &ea,
+                                            unsigned long long &eb, uint32_t &ta,
+                                            unsigned long long &tb, uint32_t *s_a,
+                                            unsigned long long *s_b) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t ia = a;
+  unsigned long long ib = b;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t xa = __shfl_up_sync(0xffffffffu, ia, d);
+    unsigned long long xb = __shfl_up_sync(0xffffffffu, ib, d);
+    if (lane >= d) {
+      ia += xa;
+      ib += xb;
+    }
+  }
+  if (lane == 31) {
+    s_a[warp] = ia;
+    s_b[warp] = ib;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t wa = lane < kThreads / 32 ? s_a[lane] : 0;
+    unsigned long long wb = lane < kThreads / 32 ? s_b[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t xa = __shfl_up_sync(0xffffffffu, wa, d);
+      unsigned long long xb = __shfl_up_sync(0xffffffffu, wb, d);
+      if (lane >= d) {
+        wa += xa;
+        wb += xb;
+      }
+    }
+    if (lane < kThreads / 32) {
+      s_a[lane + 32] = wa;  // inclusive warp prefix
+      s_b[lane + 32] = wb;
+    }
+  }
+  __syncthreads();
+  uint32_t wpa = warp ? s_a[32 + warp - 1] : 0;
+  unsigned long long wpb = warp ? s_b[32 + warp - 1] : 0;
+  ea = wpa + ia - a;
+  eb = wpb + ib - b;
+  ta = s_a[32 + kThreads / 32 - 1];
+  tb = s_b[32 + kThreads / 32 - 1];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Group table (open addressing; the key is published with one 64-bit CAS
+// that carries its hash and a dense key id whose descriptor was written and
+// fenced before the CAS).
+// ---------------------------------------------------------------------------
+
+struct KeyRef {
+  const uint8_t *p;  // key bytes (string: body)
+  uint32_t len;
+  uint8_t kind;      // JK_NULL for missing/null keys
+  uint8_t esc;
+  unsigned long long abs_off;
+};
+
+__device__ __forceinline__ bool key_bytes_equal(const KeyRef &a, const uint8_t *bp, uint32_t blen,
+                                                uint8_t besc) {
+  if (!a.esc && !besc) {
+    if (a.len != blen) return false;
+    for (uint32_t k = 0; k < blen; k++)
+      if (a.p[k] != bp[k]) return false;
+    return true;
+  }
+  StrDecoder x(a.p, a.len), y(bp, blen);
+  for (;;) {
+    int u = x.next(), w = y.next();
+    if (u != w) return false;
+    if (u < 0) return true;
+  }
+}
+
+// Returns the key id, or 0xFFFFFFFF when the table is full (the overflow flag
+// is raised and the run is repeated with a bigger table).
+__device__ uint32_t group_find_or_insert(const ScanParams &sp, const KeyRef &k, uint32_t h) {
+  const GroupTable &g = sp.g;
+  uint32_t pos = h & g.cap_mask;
+  uint32_t mine = 0xFFFFFFFFu;
+  for (uint32_t probe = 0; probe <= g.cap_mask; probe++) {
+    unsigned long long w = *(volatile unsigned long long *)&g.slots[pos];
+    if (w == 0) {
+      if (mine == 0xFFFFFFFFu) {
+        mine = atomicAdd(&sp.ctr->n_keys, 1u);
+        if (mine >= g.key_cap) {
+          atomicOr(&sp.ctr->overflow, 4u);
+          return 0xFFFFFFFFu;
+        }
+        g.key_off[mine] = k.abs_off;
+        g.key_len[mine] = k.len;
+        g.key_kind[mine] = k.kind;
+        g.key_esc[mine] = k.esc;
+        __threadfence();
+      }
+      unsigned long long want = ((unsigned long long)h << 32) | (mine + 1ull);
+      unsigned long long old = atomicCAS(&g.slots[pos], 0ull, want);
+      if (old == 0) return mine;
+      w = old;
+    }
+    if ((uint32_t)(w >> 32) == h) {
+      uint32_t kid = (uint32_t)w - 1;
+      __threadfence();
+      if (g.key_kind[kid] == k.kind &&
+          key_bytes_equal(k, sp.data + g.key_off[kid], g.key_len[kid], g.key_esc[kid]))
+        return kid;
+    }
+    pos = (pos + 1) & g.cap_mask;
+  }
+  atomicOr(&sp.ctr->overflow, 4u);
+  return 0xFFFFFFFFu;
+}
+
+// ---------------------------------------------------------------------------
+// Row rendering.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t csv_cell_len(const uint8_t *p, uint32_t n, bool decode) {
+  // RFC 4180 quoting as output.rs:45-61 does it, over raw or decoded bytes.
+  uint32_t len = 0, quotes = 0;
+  bool need = false;
+  if (!decode) {
+    for (uint32_t k = 0; k < n; k++) {
+      uint32_t c = p[k];
+      if (c == '"') quotes++;
+      if (c == ',' || c == '"' || c == '\n' || c == '\r') need = true;
+    }
+    len = n;
+  } else {
+    StrDecoder d(p, n);
+    for (int c; (c = d.next()) >= 0;) {
+      len++;
+      if (c == '"') quotes++;
+      if (c == ',' || c == '"' || c == '\n' || c == '\r') need = true;
+    }
+  }
+  return need ? len + quotes + 2 : len;
+}
+
+__device__ __forceinline__ uint32_t csv_cell_write(uint8_t *dst, const uint8_t *p, uint32_t n,
+                                                   bool decode, uint32_t expect_len) {
+  // expect_len tells whether quoting applies (it differs from the bare length).
+  uint32_t w = 0;
+  uint32_t bare = 0;
+  if (!decode) bare = n;
+  else {
+    StrDecoder d(p, n);
+    while (d.next() >= 0) bare++;
+  }
+  bool quote = expect_len != bare;
+  if (quote) dst[w++] = '"';
+  if (!decode) {
+    for (uint32_t k = 0; k < n; k++) {
+      if (quote && p[k] == '"') dst[w++] = '"';
+      dst[w++] = p[k];
+    }
+  } else {
+    StrDecoder d(p, n);
+    for (int c; (c = d.next()) >= 0;) {
+      if (quote && c == '"') dst[w++] = '"';
+      dst[w++] = (uint8_t)c;
+    }
+  }
+  if (quote) dst[w++] = '"';
+  return w;
+}
+
+// Length of a value cell in CSV mode (output.rs:65-81).
+__device__ __forceinline__ uint32_t csv_value_len(const uint8_t *line, const SlotVal &s) {
+  if (s.kind == JK_MISSING || s.kind == JK_NULL) return 0;
+  if (s.kind == JK_STR) return csv_cell_len(line + s.off + 1, s.len - 2, s.esc);
+  return csv_cell_len(line + s.off, s.len, false);
+}
+
+// Computes the row length of a selected line.
+__device__ __forceinline__ uint32_t row_length(const DevPlan &P, const uint8_t *line,
+                                               uint32_t line_len, const SlotVal *slots) {
+  switch (P.output_kind) {
+    case 0:  // passthrough (output.rs:204-217)
+      return (P.csv_mode ? csv_cell_len(line, line_len, false) : line_len) + 1;
+    case 1: {  // single value (output.rs:220-231)
+      const SlotVal &s = slots[P.out_slot];
+      if (P.csv_mode) return csv_value_len(line, s) + 1;
+      return (s.kind == JK_MISSING ? 4 : s.len) + 1;
+    }
+    default: {  // projection (output.rs:234-264, prefixes rendered by lower.rs:63-87)
+      uint32_t len = P.suffix_len + 1;
+      for (uint32_t f = 0; f < P.n_fields; f++) {
+        const SlotVal &s = slots[P.field_slot[f]];
+        len += P.prefix_len[f];
+        if (P.csv_mode) len += csv_value_len(line, s);
+        else len += s.kind == JK_MISSING ? 4 : s.len;
+      }
+      return len;
+    }
+  }
+}
+
+// Warp-cooperative copy of n bytes (lanes stride by 32: coalesced stores).
+__device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint32_t n, int lane) {
+  for (uint32_t k = lane; k < n; k += 32) dst[k] = src[k];
+}
+
+// Writes one row.  All lanes of the warp call it together.
+__device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
+                         const uint32_t *fields, uint8_t *dst, int lane) {
+  const uint8_t *kNull = (const uint8_t *)"null";
+  if (P.output_kind == 0) {
+    if (!P.csv_mode) {
+      warp_copy(dst, line, r.line_len, lane);
+      if (lane == 0) dst[r.line_len] = '\n';
+    } else if (lane == 0) {
+      uint32_t w = csv_cell_write(dst, line, r.line_len, false, r.row_len - 1);
+      dst[w] = '\n';
+    }
+    return;
+  }
+  uint32_t nf = P.output_kind == 1 ? 1 : P.n_fields;
+  if (P.csv_mode) {
+    if (lane != 0) return;
+    uint32_t w = 0;
+    for (uint32_t f = 0; f < nf; f++) {
+      if (P.output_kind == 2)
+        for (uint32_t k = 0; k < P.prefix_len[f]; k++) dst[w++] = P.blob[P.prefix_off[f] + k];
+      uint32_t off = fields[2 * f], lk = fields[2 * f + 1];
+      uint32_t kind = lk >> 28, esc = (lk >> 27) & 1, len = lk & 0x07FFFFFFu;
+      if (kind == JK_MISSING || kind == JK_NULL) continue;
+      const uint8_t *vp = line + off;
+      if (kind == JK_STR) {
+        uint32_t L = csv_cell_len(vp + 1, len - 2, esc);
+        w += csv_cell_write(dst + w, vp + 1, len - 2, esc, L);
+      } else {
+        uint32_t L = csv_cell_len(vp, len, false);
+        w += csv_cell_write(dst + w, vp, len, false, L);
+      }
+    }
+    dst[w] = '\n';
+    return;
+  }
+  uint32_t w = 0;
+  for (uint32_t f = 0; f < nf; f++) {
+    if (P.output_kind == 2) {
+      warp_copy(dst + w, P.blob + P.prefix_off[f], P.prefix_len[f], lane);
+      w += P.prefix_len[f];
+    }
+    uint32_t off = fields[2 * f], lk = fields[2 * f + 1];
+    uint32_t kind = lk >> 28, len = lk & 0x07FFFFFFu;
+    if (kind == JK_MISSING) {
+      warp_copy(dst + w, kNull, 4, lane);
+      w += 4;
+    } else {
+      warp_copy(dst + w, line + off, len, lane);
+      w += len;
+    }
+  }
+  if (P.output_kind == 2) {
+    warp_copy(dst + w, P.blob + P.suffix_off, P.suffix_len, lane);
+    w += P.suffix_len;
+  }
+  if (lane == 0) dst[w] = '\n';
+}
+
+// ---------------------------------------------------------------------------
+// The scan kernel.
+// ---------------------------------------------------------------------------
+
+struct ThreadAgg {
+  unsigned long long count, numeric, isum_lo, isum_hi, n_int, min_bits, max_bits;
+  unsigned int saw;
+  __device__ void init() {
+    count = numeric = isum_lo = isum_hi = n_int = 0;
+    min_bits = ~0ull;
+    max_bits = 0;
+    saw = 0;
+  }
+  __device__ void add_int(long long v) {
+    unsigned long long lo = isum_lo + (unsigned long long)v;
+    unsigned long long carry = lo < isum_lo;
+    isum_lo = lo;
+    isum_hi += (v < 0 ? ~0ull : 0ull) + carry;
+  }
+};
+
+__device__ __forceinline__ bool is_line_blank_byte(uint32_t c) {
+  return c == ' ' || c == '\t' || c == '\r' || c == 0x0C;
+}
+
+template <bool kRows>
+__global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const DevPlan &P = *sp.plan;
+  const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
+  uint8_t *win = smem;                                            // T + H + 16
+  uint16_t *lstart = (uint16_t *)(smem + T + H + 16);             // kMaxLinesPerPass + 1
+  uint32_t *scan_a = (uint32_t *)(lstart + kMaxLinesPerPass + 2); // 64
+  unsigned long long *scan_b = (unsigned long long *)(((uintptr_t)(scan_a + 64) + 7) & ~(uintptr_t)7);
+  __shared__ unsigned long long s_tile;
+  __shared__ unsigned int s_prev_nl;
+  __shared__ unsigned int s_first_invalid;
+  __shared__ unsigned int s_first_type;
+  __shared__ unsigned long long s_excl[3];
+  __shared__ double s_fsum[kThreads / 32];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
+  const uint32_t rec_stride = P.rec_stride;
+  uint8_t *my_recs = sp.rec_scratch + (unsigned long long)blockIdx.x * sp.rec_cap_per_cta * rec_stride;
+  DeepStack deep;
+  deep.words = sp.deep_words + (unsigned long long)blockIdx.x * (sp.deep_levels_per_cta / 32);
+  deep.cap_levels = sp.deep_levels_per_cta;
+
+  ThreadAgg agg;
+  agg.init();
+  unsigned long long c_lines = 0, c_blank = 0, c_invalid = 0, c_type = 0, c_sel = 0;
+  NodeVals nv;
+  SlotVal slots[kMaxSlots];
+
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(&sp.ctr->next_tile, 1ull);
+    __syncthreads();
+    const unsigned long long tile = s_tile;
+    if (tile >= sp.n_tiles) break;
+    const unsigned long long ts = tile * T;
+    const unsigned long long te = min(ts + T, sp.n);
+    const uint32_t tlen = (uint32_t)(te - ts);
+    const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, sp.n - ts);
+    const bool win_reaches_end = ts + wlen == sp.n;
+
+    // 1. stage tile + halo.
+    const uint32_t nfull = wlen >> 4;
+    for (uint32_t c = tid; c < nfull; c += kThreads)
+      ((uint4 *)win)[c] = __ldg((const uint4 *)(sp.data + ts) + c);
+    for (uint32_t b = (nfull << 4) + tid; b < wlen; b += kThreads) win[b] = sp.data[ts + b];
+    if (tid == 0) {
+      s_prev_nl = (ts == 0 || sp.data[ts - 1] == '\n') ? 1u : 0u;
+      s_first_invalid = 0xFFFFFFFFu;
+      s_first_type = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+
+    // 2. count line starts: ts itself (after a newline) and q+1 for every
+    //    newline q in [ts, te-1).  Thread t owns bytes [t*S, (t+1)*S).
+    const uint32_t S = T / kThreads;  // T is a multiple of 1024, so S is a multiple of 4
+    const uint32_t seg0 = tid * S;
+    const uint32_t seg1 = min(seg0 + S, tlen ? tlen - 1 : 0);
+    uint32_t my_nl = 0;
+    {
+      uint32_t b = seg0;
+      for (; b + 4 <= seg1; b += 4)
+        my_nl += __popc(swar_movemask(swar_newline_exact(*(const uint32_t *)(win + b))));
+      for (; b < seg1; b++) my_nl += win[b] == '\n';
+    }
+    uint32_t first_nl, tot_nl;
+    unsigned long long dummy_e, dummy_t;
+    block_scan2(my_nl, 0ull, first_nl, dummy_e, tot_nl, dummy_t, scan_a, scan_b);
+    const uint32_t lead = s_prev_nl;
+    const uint32_t n_lines_tile = tot_nl + lead;
+
+    // 3. walk the lines, pass by pass.
+    unsigned long long tile_rows = 0, tile_bytes = 0;
+    double fsum_thread = 0.0;
+    for (uint32_t base = 0; base < n_lines_tile; base += kMaxLinesPerPass) {
+      const uint32_t cnt = min(n_lines_tile - base, kMaxLinesPerPass);
+      // list line starts [base, base + cnt] (one extra as the end marker)
+      if (lead && tid == 0 && base == 0) lstart[0] = 0;
+      {
+        uint32_t idx = first_nl + lead;
+        if (my_nl && idx <= base + cnt && idx + my_nl > base) {
+          uint32_t b = seg0;
+          for (; b + 4 <= seg1; b += 4) {
+            uint32_t m = swar_movemask(swar_newline_exact(*(const uint32_t *)(win + b)));
+            while (m) {
+              uint32_t k = __ffs(m) - 1;
+              m &= m - 1;
+              if (idx >= base && idx <= base + cnt) lstart[idx - base] = (uint16_t)(b + k + 1);
+              idx++;
+            }
+          }
+          for (; b < seg1; b++) {
+            if (win[b] == '\n') {
+              if (idx >= base && idx <= base + cnt) lstart[idx - base] = (uint16_t)(b + 1);
+              idx++;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      for (uint32_t b0 = 0; b0 < cnt; b0 += kThreads) {
+        const uint32_t li = b0 + tid;  // line index within the pass
+        int status = -1;
+        uint32_t has_row = 0, row_len = 0;
+        unsigned long long line_abs = 0;
+        uint32_t line_len = 0, ordinal = base + li;
+        bool in_window = true;
+        const uint8_t *lp = nullptr;
+        bool has_group = false;
+        KeyRef gk;
+        uint32_t gh = 0;
+        SlotVal aggv;
+        aggv.kind = JK_MISSING;
+        if (li < cnt) {
+          uint32_t s = lstart[li];
+          uint32_t e;  // window offset of the newline (or of the data end)
+          bool found = true;
+          if (base + li + 1 < n_lines_tile) {
+            // the next line's start is listed (the list keeps one entry past
+            // the pass for exactly this)
+            e = (uint32_t)lstart[li + 1] - 1;
+          } else {
+            // last line of the tile: its newline is at or after te - 1
+            uint32_t q = tlen ? tlen - 1 : 0;
+            if (q < s) q = s;
+            while (q < wlen && win[q] != '\n') q++;
+            if (q < wlen) e = q;
+            else if (win_reaches_end) e = wlen;
+            else found = false;
+          }
+          line_abs = ts + s;
+          if (found) {
+            lp = win + s;
+            line_len = e - s;
+          } else {
+            // longer than the window: walk it from global memory
+            in_window = false;
+            unsigned long long q = ts + wlen;
+            while (q < sp.n && sp.data[q] != '\n') q++;
+            lp = sp.data + line_abs;
+            line_len = (uint32_t)(q - line_abs);
+          }
+          status = walk_line(P, lp, line_len, nv, nullptr);
+        }
+        // Lines nesting past 64 levels share this CTA's deep stack, so they
+        // are walked one at a time.
+        if (__syncthreads_or(status == LS_DEEP)) {
+          for (int t = 0; t < kThreads; t++) {
+            if (tid == t && status == LS_DEEP) {
+              status = walk_line(P, lp, line_len, nv, &deep);
+              if (status == LS_DEEP_FULL) {
+                atomicOr(&sp.ctr->overflow, 8u);
+                status = LS_INVALID;
+              }
+            }
+            __syncthreads();
+          }
+        }
+        // `line_len` for output excludes a trailing '\r' (chunk.rs:433-435).
+        uint32_t out_len = line_len;
+        if (status >= 0 && out_len && lp[out_len - 1] == '\r') out_len--;
+
+        if (status == LS_OK) {
+          uint32_t type_err_filter = 0, type_err_post = 0;
+          for (uint32_t s = 0; s < P.n_slots; s++) {
+            slots[s] = resolve_slot(P, nv, s);
+            if (slots[s].state == SS_TYPE_ERROR) {
+              if ((P.filter_slot_mask >> s) & 1) type_err_filter = 1;
+              else type_err_post = 1;
+            }
+          }
+          if (type_err_filter) {
+            status = LS_TYPE_ERROR;
+          } else if (P.has_filter && !eval_filter(P, lp, slots)) {
+            status = 100;  // filtered out
+          } else if (type_err_post) {
+            status = LS_TYPE_ERROR;
+          } else {
+            status = 101;  // selected
+          }
+        }
+        if (status == LS_BLANK) c_blank++;
+        else if (status == LS_INVALID) {
+          c_invalid++;
+          atomicMin(&s_first_invalid, ordinal);
+        } else if (status == LS_TYPE_ERROR) {
+          c_type++;
+          atomicMin(&s_first_type, ordinal);
+        }
+        else if (status == 101) {
+          c_sel++;
+          if (kRows) {
+            has_row = 1;
+            row_len = row_length(P, lp, out_len, slots);
+          } else {
+            // aggregate (exec/cpu.rs:358-369, agg.rs:44-71)
+            if (P.agg_slot >= 0) aggv = slots[P.agg_slot];
+            if (P.group_slot >= 0) {
+              const SlotVal &g = slots[P.group_slot];
+              has_group = true;
+              gk.esc = 0;
+              if (g.kind == JK_MISSING || g.kind == JK_NULL) {
+                gk.kind = JK_NULL;
+                gk.p = lp;
+                gk.len = 0;
+                gk.abs_off = line_abs;
+              } else if (g.kind == JK_STR) {
+                gk.kind = JK_STR;
+                gk.p = lp + g.off + 1;
+                gk.len = g.len - 2;
+                gk.esc = g.esc;
+                gk.abs_off = line_abs + g.off + 1;
+              } else {
+                gk.kind = g.kind;
+                gk.p = lp + g.off;
+                gk.len = g.len;
+                gk.abs_off = line_abs + g.off;
+              }
+              gh = (gk.kind == JK_STR ? hash_str_body(gk.p, gk.len, gk.esc) : hash_raw(gk.p, gk.len)) ^
+                   (gk.kind * 0x9E3779B9u);
+              if (gh == 0) gh = 1;
+            }
+          }
+        }
+
+        // Aggregate contribution of this line.
+        bool contrib = !kRows && status == 101;
+        unsigned long long v_num = 0, v_int = 0;
+        long long iv = 0;
+        double fv = 0.0;
+        bool is_int = false, is_num = false;
+        if (contrib && P.agg_slot >= 0) {
+          if (aggv.kind == JK_NUM) {
+            fv = parse_number(lp + aggv.off, aggv.len, is_int, iv);
+            is_num = true;
+          } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL) {
+            agg.saw = 1;
+          }
+        }
+        (void)v_num;
+        (void)v_int;
+        if (contrib && !has_group) {
+          agg.count++;
+          if (is_num) {
+            agg.numeric++;
+            unsigned long long ob = order_bits(fv);
+            agg.min_bits = min(agg.min_bits, ob);
+            agg.max_bits = max(agg.max_bits, ob);
+            if (is_int) {
+              agg.add_int(iv);
+              agg.n_int++;
+            } else {
+              fsum_thread += fv;
+            }
+          }
+        }
+        if (!kRows && P.group_slot >= 0) {
+          // Group updates, aggregated per warp on the key id.
+          uint32_t kid = 0xFFFFFFFFu;
+          if (has_group) kid = group_find_or_insert(sp, gk, gh);
+          const GroupTable &g = sp.g;
+          if (kid != 0xFFFFFFFFu) {
+            atomicAdd(&g.count[kid], 1ull);
+            if (is_num) {
+              atomicAdd(&g.numeric[kid], 1ull);
+              unsigned long long ob = order_bits(fv);
+              atomicMin(&g.min_bits[kid], ob);
+              atomicMax(&g.max_bits[kid], ob);
+              if (is_int) {
+                unsigned long long old = atomicAdd(&g.isum_lo[kid], (unsigned long long)iv);
+                unsigned long long carry = (old + (unsigned long long)iv) < old;
+                unsigned long long hi = (iv < 0 ? ~0ull : 0ull) + carry;
+                if (hi) atomicAdd(&g.isum_hi[kid], hi);
+                atomicAdd(&g.n_int[kid], 1ull);
+              } else {
+                atomicAdd(&g.fsum[kid], fv);
+              }
+            } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0) {
+              g.saw_non_numeric[kid] = 1;
+            }
+          }
+        }
+
+        if (kRows) {
+          uint32_t er;
+          unsigned long long eb;
+          uint32_t tr;
+          unsigned long long tb;
+          block_scan2(has_row, (unsigned long long)row_len, er, eb, tr, tb, scan_a, scan_b);
+          if (has_row) {
+            unsigned long long ri = tile_rows + er;
+            if (ri < sp.rec_cap_per_cta) {
+              RowRec *r = (RowRec *)(my_recs + ri * rec_stride);
+              r->line_start = line_abs;
+              r->line_len = out_len;
+              r->ordinal = ordinal;
+              r->local_off = (uint32_t)(tile_bytes + eb);
+              r->row_len = row_len;
+              r->in_window = in_window;
+              uint32_t *fl = (uint32_t *)(r + 1);
+              for (uint32_t f = 0; f < nf; f++) {
+                const SlotVal &s = slots[P.output_kind == 1 ? P.out_slot : P.field_slot[f]];
+                fl[2 * f] = s.off;
+                fl[2 * f + 1] = s.len | ((uint32_t)s.kind << 28) | ((uint32_t)s.esc << 27);
+              }
+            } else {
+              atomicOr(&sp.ctr->overflow, 1u);
+            }
+          }
+          tile_rows += tr;
+          tile_bytes += tb;
+        }
+      }
+      __syncthreads();
+    }
+    c_lines += (tid == 0) ? n_lines_tile : 0;
+
+    // Per-tile bookkeeping.
+    if (tid == 0) {
+      sp.tiles[tile].n_lines = n_lines_tile;
+      sp.tiles[tile].first_invalid = s_first_invalid;
+      sp.tiles[tile].first_type_error = s_first_type;
+      if (s_first_invalid != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_invalid_tile, tile);
+      if (s_first_type != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_type_tile, tile);
+    }
+    if (!kRows) {
+      // fixed-order tree: warp shuffle tree, then warps in order
+      double f = fsum_thread;
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) f += __shfl_down_sync(0xffffffffu, f, d);
+      if (lane == 0) s_fsum[warp] = f;
+      __syncthreads();
+      if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; w++) t += s_fsum[w];
+        sp.tile_fsum[tile] = t;
+      }
+      __syncthreads();
+      continue;
+    }
+
+    // 4. look-back for this tile's row / byte / line prefix.
+    if (tid == 0) {
+      unsigned long long mine[3] = {tile_rows, tile_bytes, (unsigned long long)n_lines_tile};
+      unsigned long long ex[3] = {0, 0, 0};
+      if (tile == 0) {
+        for (int k = 0; k < 3; k++) sp.lb_incl[k] = mine[k];
+        __threadfence();
+        st_release(&sp.lb_flag[0], 2u);
+      } else {
+        for (int k = 0; k < 3; k++) sp.lb_agg[tile * 3 + k] = mine[k];
+        __threadfence();
+        st_release(&sp.lb_flag[tile], 1u);
+        long long j = (long long)tile - 1;
+        unsigned long long spins = 0;
+        while (j >= 0) {
+          unsigned f = ld_acquire(&sp.lb_flag[j]);
+          if (f == 0) {
+            if (++spins > sp.spin_limit) {
+              atomicOr(&sp.ctr->error, 1u);
+              break;
+            }
+            __nanosleep(64);
+            continue;
+          }
+          const unsigned long long *src = f == 2 ? sp.lb_incl : sp.lb_agg;
+          for (int k = 0; k < 3; k++) ex[k] += src[j * 3 + k];
+          if (f == 2) break;
+          j--;
+        }
+        for (int k = 0; k < 3; k++) sp.lb_incl[tile * 3 + k] = ex[k] + mine[k];
+        __threadfence();
+        st_release(&sp.lb_flag[tile], 2u);
+      }
+      for (int k = 0; k < 3; k++) s_excl[k] = ex[k];
+    }
+    __syncthreads();
+
+    // 5. emit this tile's rows in line order, one warp per row.
+    {
+      const unsigned long long row0 = s_excl[0], byte0 = s_excl[1], line0 = s_excl[2];
+      const unsigned long long nrec = min(tile_rows, sp.rec_cap_per_cta);
+      for (unsigned long long r = warp; r < nrec; r += kThreads / 32) {
+        const RowRec *rr = (const RowRec *)(my_recs + r * rec_stride);
+        const uint32_t *fl = (const uint32_t *)(rr + 1);
+        unsigned long long dst_off = byte0 + rr->local_off;
+        unsigned long long ri = row0 + r;
+        if (dst_off + rr->row_len > sp.out_cap || ri >= sp.rows_cap) {
+          if (lane == 0) atomicOr(&sp.ctr->overflow, 2u);
+          continue;
+        }
+        const uint8_t *line =
+            rr->in_window ? win + (uint32_t)(rr->line_start - ts) : sp.data + rr->line_start;
+        emit_row(P, line, *rr, fl, sp.out + dst_off, lane);
+        if (lane == 0) {
+          sp.row_off[ri] = dst_off;
+          sp.line_idx[ri] = line0 + rr->ordinal;
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // Flush this CTA's counters.
+  auto wsum = [](unsigned long long x) {
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+    return x;
+  };
+  c_lines = wsum(c_lines);
+  c_blank = wsum(c_blank);
+  c_invalid = wsum(c_invalid);
+  c_type = wsum(c_type);
+  c_sel = wsum(c_sel);
+  if (lane == 0) {
+    if (c_lines) atomicAdd(&sp.ctr->n_lines, c_lines);
+    if (c_blank) atomicAdd(&sp.ctr->n_blank, c_blank);
+    if (c_invalid) atomicAdd(&sp.ctr->n_invalid, c_invalid);
+    if (c_type) atomicAdd(&sp.ctr->n_type_error, c_type);
+    if (c_sel) atomicAdd(&sp.ctr->n_selected, c_sel);
+  }
+  if (!kRows && P.group_slot < 0 && P.output_kind == 3) {
+    unsigned long long cnt = wsum(agg.count), num = wsum(agg.numeric), ni = wsum(agg.n_int);
+    // 128-bit sums: reduce the low words with carry counting, per lane pair
+    unsigned long long lo = agg.isum_lo, hi = agg.isum_hi;
+    for (int d = 16; d > 0; d >>= 1) {
+      unsigned long long olo = __shfl_down_sync(0xffffffffu, lo, d);
+      unsigned long long ohi = __shfl_down_sync(0xffffffffu, hi, d);
+      if (lane + d < 32) {
+        unsigned long long s = lo + olo;
+        hi += ohi + (s < lo);
+        lo = s;
+      }
+    }
+    unsigned long long mn = agg.min_bits, mx = agg.max_bits;
+    for (int d = 16; d > 0; d >>= 1) {
+      mn = min(mn, __shfl_down_sync(0xffffffffu, mn, d));
+      mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
+    }
+    unsigned int saw = __any_sync(0xffffffffu, agg.saw);
+    if (lane == 0) {
+      if (cnt) atomicAdd(&sp.ctr->agg_count, cnt);
+      if (num) atomicAdd(&sp.ctr->agg_numeric, num);
+      if (ni) atomicAdd(&sp.ctr->agg_n_int, ni);
+      if (lo || hi) {
+        unsigned long long old = atomicAdd(&sp.ctr->agg_isum_lo, lo);
+        unsigned long long carry = (old + lo) < old;
+        if (hi + carry) atomicAdd(&sp.ctr->agg_isum_hi, hi + carry);
+      }
+      if (num) {
+        atomicMin(&sp.ctr->agg_min_bits, mn);
+        atomicMax(&sp.ctr->agg_max_bits, mx);
+      }
+      if (saw) atomicOr(&sp.ctr->agg_saw_non_numeric, 1u);
+    }
+  } else if (!kRows) {
+    unsigned int saw = __any_sync(0xffffffffu, agg.saw);
+    if (lane == 0 && saw) atomicOr(&sp.ctr->agg_saw_non_numeric, 1u);
+  }
+}
+
+// Fixed-order reduction of the per-tile FP partials (pass 1: contiguous
+// blocks; pass 2: one CTA over the block partials), plus the first invalid
+// line index.
+__global__ void k_reduce_tiles(const double *tile_fsum, unsigned long long n_tiles,
+                               double *block_out, const TileDesc *tiles, RunCounters *ctr,
+                               unsigned long long *block_lines) {
+  __shared__ double s_f[kThreads];
+  __shared__ unsigned long long s_l[kThreads], s_t[kThreads];
+  unsigned long long per = (n_tiles + gridDim.x - 1) / gridDim.x;
+  unsigned long long b0 = blockIdx.x * per, b1 = min(b0 + per, n_tiles);
+  unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
+  double f = 0.0;
+  unsigned long long lines = 0, lines_t = 0;
+  unsigned long long chunk = (b1 > b0 ? b1 - b0 : 0);
+  unsigned long long cper = (chunk + kThreads - 1) / kThreads;
+  unsigned long long c0 = b0 + threadIdx.x * cper, c1 = min(c0 + cper, b1);
+  for (unsigned long long t = c0; t < c1; t++) {
+    if (tile_fsum) f += tile_fsum[t];
+    if (t < cut) lines += tiles[t].n_lines;
+    if (t < cut_t) lines_t += tiles[t].n_lines;
+  }
+  s_f[threadIdx.x] = f;
+  s_l[threadIdx.x] = lines;
+  s_t[threadIdx.x] = lines_t;
+  __syncthreads();
+  for (int d = kThreads / 2; d > 0; d >>= 1) {
+    if (threadIdx.x < d) {
+      s_f[threadIdx.x] += s_f[threadIdx.x + d];
+      s_l[threadIdx.x] += s_l[threadIdx.x + d];
+      s_t[threadIdx.x] += s_t[threadIdx.x + d];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    block_out[blockIdx.x] = s_f[0];
+    block_lines[2 * blockIdx.x] = s_l[0];
+    block_lines[2 * blockIdx.x + 1] = s_t[0];
+  }
+}
+
+__global__ void k_finalize(const double *block_f, const unsigned long long *block_lines,
+                           unsigned nblocks, const TileDesc *tiles, RunCounters *ctr,
+                           const unsigned long long *lb_incl, unsigned long long n_tiles,
+                           unsigned long long *row_off, unsigned long long rows_cap) {
+  if (threadIdx.x != 0) return;
+  double f = 0.0;
+  unsigned long long lines = 0, lines_t = 0;
+  for (unsigned b = 0; b < nblocks; b++) {
+    f += block_f[b];
+    lines += block_lines[2 * b];
+    lines_t += block_lines[2 * b + 1];
+  }
+  ctr->fsum_total = f;
+  unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
+  ctr->first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
+  ctr->first_type_error = cut_t == ~0ull ? ~0ull : lines_t + tiles[cut_t].first_type_error;
+  if (row_off && n_tiles > 0) {
+    // The last tile's inclusive prefix holds the totals.
+    unsigned long long rows = lb_incl[(n_tiles - 1) * 3 + 0];
+    unsigned long long bytes = lb_incl[(n_tiles - 1) * 3 + 1];
+    ctr->out_len = bytes;
+    if (rows <= rows_cap) row_off[rows] = bytes;
+  }
+}
+
+}  // namespace wjq

@@ -1,0 +1,441 @@
+// Per-line walker: one thread validates one NDJSON line end to end and, in
+// the same pass, records the value of every trie node of the query plan.
+//
+// Semantics restated from the reference CPU engine:
+//   - strict RFC 8259 validation of exactly one value per line
+//     (json.rs:198-421): strings reject raw bytes < 0x20 and bad escapes,
+//     numbers follow the JSON grammar, literals must be exact, brackets must
+//     match;
+//   - blank lines are those made only of ASCII whitespace including form
+//     feed (chunk.rs:436);
+//   - path resolution follows json.rs:444-508: last duplicate key wins,
+//     missing/null propagate as Missing, indexing a scalar is a type error,
+//     and an invalid line beats a type error.
+// The walk is iterative; container depth is tracked in a 64-bit register
+// and, for the rare deeper line, in a caller-provided bit stack.
+#pragma once
+
+#include "devutil.cuh"
+#include "plan.h"
+
+namespace wjq {
+
+enum LineStatus : int {
+  LS_OK = 0,
+  LS_INVALID = 1,
+  LS_TYPE_ERROR = 2,
+  LS_BLANK = 4,
+  LS_DEEP = 5,       // deeper than the register stack; caller retries with a deep stack
+  LS_DEEP_FULL = 6,  // deeper than the deep stack provided
+};
+
+// Values recorded per trie node for one line; offsets are relative to the
+// line start.
+struct NodeVals {
+  uint8_t kind[kMaxNodes];
+  uint8_t esc[kMaxNodes];
+  uint32_t off[kMaxNodes];
+  uint32_t len[kMaxNodes];
+};
+
+// A deep bit stack for levels >= 64 (bit = 1 for arrays), in global memory.
+struct DeepStack {
+  uint32_t *words;
+  uint64_t cap_levels;
+};
+
+namespace detail {
+
+enum Expect : int {
+  EX_VALUE = 0,
+  EX_KEY_OR_CLOSE = 1,
+  EX_KEY = 2,
+  EX_COLON = 3,
+  EX_COMMA_OR_CLOSE = 4,
+  EX_VALUE_OR_CLOSE = 5,
+  EX_END = 6,
+};
+
+// Scans the string whose opening quote is at `s`.  Returns the index of the
+// closing quote, or -1 when the string is malformed or unterminated.
+__device__ __forceinline__ long long scan_string(const uint8_t *line, uint32_t n, uint32_t s,
+                                                 bool &esc) {
+  uint32_t j = s + 1;
+  esc = false;
+  for (;;) {
+    // Aligned word steps over runs of ordinary bytes.
+    while (((uintptr_t)(line + j) & 3u) == 0 && j + 4 <= n &&
+           swar_string_special(*(const uint32_t *)(line + j)) == 0)
+      j += 4;
+    if (j >= n) return -1;
+    uint32_t c = line[j];
+    if (c == '"') return j;
+    if (c == '\\') {
+      if (j + 1 >= n) return -1;
+      uint32_t e = line[j + 1];
+      esc = true;
+      if (e == '"' || e == '\\' || e == '/' || e == 'b' || e == 'f' || e == 'n' || e == 'r' ||
+          e == 't') {
+        j += 2;
+      } else if (e == 'u') {
+        if (j + 6 > n) return -1;
+        if (hex_val(line[j + 2]) < 0 || hex_val(line[j + 3]) < 0 || hex_val(line[j + 4]) < 0 ||
+            hex_val(line[j + 5]) < 0)
+          return -1;
+        j += 6;
+      } else {
+        return -1;
+      }
+      continue;
+    }
+    if (c < 0x20) return -1;
+    j++;
+  }
+}
+
+// Validates an atom (number or literal) occupying [s, e).
+__device__ __forceinline__ bool valid_atom(const uint8_t *p, uint32_t n) {
+  uint32_t c = p[0];
+  if (c == 't') return n == 4 && p[1] == 'r' && p[2] == 'u' && p[3] == 'e';
+  if (c == 'f') return n == 5 && p[1] == 'a' && p[2] == 'l' && p[3] == 's' && p[4] == 'e';
+  if (c == 'n') return n == 4 && p[1] == 'u' && p[2] == 'l' && p[3] == 'l';
+  // number: -?(0|[1-9][0-9]*)(\.[0-9]+)?([eE][+-]?[0-9]+)?   (json.rs:370-410)
+  uint32_t i = 0;
+  if (c == '-') i = 1;
+  if (i >= n || !is_digit(p[i])) return false;
+  if (p[i] == '0') {
+    i++;
+  } else {
+    while (i < n && is_digit(p[i])) i++;
+  }
+  if (i < n && p[i] == '.') {
+    i++;
+    if (i >= n || !is_digit(p[i])) return false;
+    while (i < n && is_digit(p[i])) i++;
+  }
+  if (i < n && (p[i] == 'e' || p[i] == 'E')) {
+    i++;
+    if (i < n && (p[i] == '+' || p[i] == '-')) i++;
+    if (i >= n || !is_digit(p[i])) return false;
+    while (i < n && is_digit(p[i])) i++;
+  }
+  return i == n;
+}
+
+__device__ __forceinline__ uint8_t kind_of(uint32_t c) {
+  switch (c) {
+    case '{': return JK_OBJ;
+    case '[': return JK_ARR;
+    case '"': return JK_STR;
+    case 't': case 'f': return JK_BOOL;
+    case 'n': return JK_NULL;
+    default: return JK_NUM;
+  }
+}
+
+// Key child of `node` whose decoded key equals the key body, or kNoNode.
+__device__ __forceinline__ uint8_t match_key(const DevPlan &P, uint8_t node, const uint8_t *body,
+                                             uint32_t len, bool esc) {
+  for (uint8_t c = P.nodes[node].first_child; c != kNoNode; c = P.nodes[c].next_sibling) {
+    const PlanNode &nd = P.nodes[c];
+    if (nd.is_index) continue;
+    if (!esc) {
+      if (nd.key_len != len) continue;
+      if (len && body[0] != nd.key_first) continue;
+      const uint8_t *k = P.blob + nd.key_off;
+      uint32_t t = 1;
+      while (t < len && body[t] == k[t]) t++;
+      if (t >= len) return c;
+    } else if (cmp_str_body(body, len, true, P.blob + nd.key_off, nd.key_len) == 0) {
+      return c;
+    }
+  }
+  return kNoNode;
+}
+
+__device__ __forceinline__ uint8_t index_child(const DevPlan &P, uint8_t node, uint32_t idx) {
+  if (node == kNoNode || !P.nodes[node].has_index_children) return kNoNode;
+  for (uint8_t c = P.nodes[node].first_child; c != kNoNode; c = P.nodes[c].next_sibling) {
+    const PlanNode &nd = P.nodes[c];
+    if (nd.is_index && nd.index == idx) return c;
+  }
+  return kNoNode;
+}
+
+}  // namespace detail
+
+// Walks `line[0, n)` (no newline; a trailing '\r' is JSON whitespace).
+// `deep` may be null: a line nesting past 64 levels then returns LS_DEEP.
+__device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uint32_t n,
+                                      NodeVals &v, const DeepStack *deep) {
+  using namespace detail;
+  const uint32_t n_nodes = P.n_nodes;
+  for (uint32_t k = 0; k < n_nodes; k++) v.kind[k] = JK_MISSING;
+
+  uint32_t i = 0;
+  while (i < n && is_ws(line[i])) i++;
+  if (i == n) return LS_BLANK;
+  if (line[i] == 0x0C) {  // form feed counts toward a blank line, not toward JSON
+    for (uint32_t j = i; j < n; j++) {
+      uint32_t c = line[j];
+      if (!(c == ' ' || c == '\t' || c == '\r' || c == 0x0C)) return LS_INVALID;
+    }
+    return LS_BLANK;
+  }
+
+  uint8_t node_at[kMaxDepthFast];  // trie node of the open container at each level
+  uint32_t arr_idx[kMaxDepthFast];
+  uint64_t stk = 0;                // bit d: container at level d is an array
+  uint64_t depth = 0;
+  uint8_t pending = n_nodes ? 0 : kNoNode;  // node the next value lands on
+  int expect = EX_VALUE;
+
+  for (;;) {
+    while (i < n && is_ws(line[i])) i++;
+    if (i >= n) break;
+    uint32_t c = line[i];
+    bool close = false;
+
+    if (expect == EX_COLON) {
+      if (c != ':') return LS_INVALID;
+      i++;
+      expect = EX_VALUE;
+      continue;
+    }
+    if (expect == EX_KEY_OR_CLOSE || expect == EX_KEY) {
+      if (c == '}' && expect == EX_KEY_OR_CLOSE) {
+        close = true;
+      } else {
+        if (c != '"') return LS_INVALID;
+        bool esc;
+        long long e = scan_string(line, n, i, esc);
+        if (e < 0) return LS_INVALID;
+        uint8_t parent = depth <= kMaxDepthFast ? node_at[depth - 1] : kNoNode;
+        pending = kNoNode;
+        if (parent != kNoNode && P.nodes[parent].has_key_children)
+          pending = match_key(P, parent, line + i + 1, (uint32_t)e - i - 1, esc);
+        i = (uint32_t)e + 1;
+        expect = EX_COLON;
+        continue;
+      }
+    } else if (expect == EX_COMMA_OR_CLOSE) {
+      uint32_t lvl = (uint32_t)depth - 1;
+      bool arr;
+      if (lvl < 64) {
+        arr = (stk >> lvl) & 1;
+      } else {
+        uint64_t b = lvl - 64;
+        arr = (deep->words[b >> 5] >> (b & 31)) & 1;
+      }
+      if (c == ',') {
+        i++;
+        if (arr) {
+          pending = kNoNode;
+          if (lvl < kMaxDepthFast) {
+            uint32_t idx = ++arr_idx[lvl];
+            pending = index_child(P, node_at[lvl], idx);
+          }
+          expect = EX_VALUE;
+        } else {
+          expect = EX_KEY;
+        }
+        continue;
+      }
+      if ((c == '}' && !arr) || (c == ']' && arr)) {
+        close = true;
+      } else {
+        return LS_INVALID;
+      }
+    } else if (expect == EX_END) {
+      return LS_INVALID;
+    } else if (expect == EX_VALUE_OR_CLOSE && c == ']') {
+      close = true;
+    }
+
+    if (close) {
+      depth--;
+      if (depth < kMaxDepthFast) {
+        uint8_t cn = node_at[depth];
+        if (cn != kNoNode) v.len[cn] = i + 1 - v.off[cn];
+      }
+      i++;
+      expect = depth == 0 ? EX_END : EX_COMMA_OR_CLOSE;
+      continue;
+    }
+
+    // A value starts at i (expect is EX_VALUE or EX_VALUE_OR_CLOSE).
+    uint8_t vn = pending;
+    if (vn != kNoNode) {
+      for (uint32_t k = vn + 1u; k < P.nodes[vn].subtree_end; k++) v.kind[k] = JK_MISSING;
+      v.kind[vn] = kind_of(c);
+      v.off[vn] = i;
+      v.esc[vn] = 0;
+    }
+    if (c == '{' || c == '[') {
+      bool arr = c == '[';
+      if (depth < 64) {
+        if (arr) stk |= 1ull << depth;
+        else stk &= ~(1ull << depth);
+      } else {
+        if (!deep) return LS_DEEP;
+        uint64_t b = depth - 64;
+        if (b >= deep->cap_levels) return LS_DEEP_FULL;
+        uint32_t m = 1u << (b & 31);
+        if (arr) deep->words[b >> 5] |= m;
+        else deep->words[b >> 5] &= ~m;
+      }
+      if (depth < kMaxDepthFast) {
+        node_at[depth] = vn;
+        arr_idx[depth] = 0;
+      }
+      pending = arr ? index_child(P, vn, 0) : kNoNode;
+      depth++;
+      i++;
+      expect = arr ? EX_VALUE_OR_CLOSE : EX_KEY_OR_CLOSE;
+      continue;
+    }
+    uint32_t vend;
+    if (c == '"') {
+      bool esc;
+      long long e = scan_string(line, n, i, esc);
+      if (e < 0) return LS_INVALID;
+      vend = (uint32_t)e + 1;
+      if (vn != kNoNode) v.esc[vn] = esc;
+    } else {
+      uint32_t j = i + 1;
+      while (j < n && !ends_atom(line[j])) j++;
+      if (!valid_atom(line + i, j - i)) return LS_INVALID;
+      vend = j;
+    }
+    if (vn != kNoNode) v.len[vn] = vend - i;
+    i = vend;
+    expect = depth == 0 ? EX_END : EX_COMMA_OR_CLOSE;
+  }
+  return expect == EX_END ? LS_OK : LS_INVALID;
+}
+
+// ---------------------------------------------------------------------------
+// Evaluation of a walked line.
+// ---------------------------------------------------------------------------
+
+enum SlotState : uint8_t { SS_FOUND = 0, SS_MISSING = 1, SS_TYPE_ERROR = 2 };
+
+struct SlotVal {
+  uint8_t state;  // SlotState
+  uint8_t kind;   // JKind (JK_MISSING when not found)
+  uint8_t esc;
+  uint32_t off;
+  uint32_t len;
+};
+
+// Resolves slot `s` from the node values (json.rs:461-507).  Walking up from
+// the terminal node, the shallowest failing step decides Missing vs type
+// error, exactly as the top-down lookup does.
+__device__ __forceinline__ SlotVal resolve_slot(const DevPlan &P, const NodeVals &v, uint32_t s) {
+  SlotVal r;
+  uint8_t t = P.slot_node[s];
+  uint8_t st = SS_FOUND;
+  for (uint8_t c = t; c != 0;) {
+    uint8_t p = P.nodes[c].parent;
+    uint8_t kp = v.kind[p];
+    if (kp == JK_MISSING || kp == JK_NULL) st = SS_MISSING;
+    else if (!P.nodes[c].is_index && kp != JK_OBJ) st = SS_TYPE_ERROR;
+    else if (P.nodes[c].is_index && kp != JK_ARR) st = SS_TYPE_ERROR;
+    c = p;
+  }
+  r.state = st;
+  if (st == SS_FOUND && v.kind[t] != JK_MISSING) {
+    r.kind = v.kind[t];
+    r.esc = v.esc[t];
+    r.off = v.off[t];
+    r.len = v.len[t];
+  } else {
+    if (st == SS_FOUND) r.state = SS_MISSING;
+    r.kind = JK_MISSING;
+    r.esc = 0;
+    r.off = 0;
+    r.len = 0;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t slot_rank(const uint8_t *line, const SlotVal &s) {
+  switch (s.kind) {
+    case JK_MISSING: case JK_NULL: return 0;
+    case JK_BOOL: return line[s.off] == 't' ? 2 : 1;
+    case JK_NUM: return 3;
+    case JK_STR: return 4;
+    case JK_ARR: return 5;
+    default: return 6;
+  }
+}
+
+// Three-way compare of a slot with a literal (json.rs:662-693).
+__device__ __forceinline__ int compare_slot(const DevPlan &P, const uint8_t *line, const SlotVal &s,
+                                            const PlanCmp &c) {
+  uint32_t sr = slot_rank(line, s);
+  if (sr != c.lit_rank) return sr < c.lit_rank ? -1 : 1;
+  if (c.lit_kind == 3 /* NUM */) {
+    bool is_int;
+    long long iv;
+    double d = parse_number(line + s.off, s.len, is_int, iv);
+    if (d < c.lit_num) return -1;
+    if (d > c.lit_num) return 1;
+    return 0;
+  }
+  if (c.lit_kind == 4 /* STR */)
+    return cmp_str_body(line + s.off + 1, s.len - 2, s.esc, P.blob + c.lit_off, c.lit_len);
+  return 0;
+}
+
+__device__ __forceinline__ bool op_accepts(uint32_t op, int o) {
+  switch (op) {
+    case 0: return o == 0;
+    case 1: return o != 0;
+    case 2: return o < 0;
+    case 3: return o <= 0;
+    case 4: return o > 0;
+    default: return o >= 0;
+  }
+}
+
+__device__ __forceinline__ bool truthy(const uint8_t *line, const SlotVal &s) {
+  if (s.kind == JK_MISSING || s.kind == JK_NULL) return false;
+  return !(s.kind == JK_BOOL && line[s.off] == 'f');
+}
+
+// Evaluates the RPN condition (exec/cpu.rs:443-453; And/Or short-circuit
+// has no side effects here, so a strict evaluation gives the same verdict).
+__device__ __forceinline__ bool eval_filter(const DevPlan &P, const uint8_t *line,
+                                            const SlotVal *slots) {
+  uint64_t st = 0;  // bit stack, top at bit 0
+  for (uint32_t k = 0; k < P.n_cond; k++) {
+    const PlanCond &o = P.cond[k];
+    switch (o.op) {
+      case 0: {
+        const PlanCmp &c = P.cmps[o.arg];
+        bool r = op_accepts(c.op, compare_slot(P, line, slots[c.slot], c));
+        st = (st << 1) | (r ? 1u : 0u);
+        break;
+      }
+      case 1:
+        st = (st << 1) | (truthy(line, slots[o.arg]) ? 1u : 0u);
+        break;
+      case 2: {
+        uint64_t b = st & 1, a = (st >> 1) & 1;
+        st = (st >> 2 << 1) | (a & b);
+        break;
+      }
+      case 3: {
+        uint64_t b = st & 1, a = (st >> 1) & 1;
+        st = (st >> 2 << 1) | (a | b);
+        break;
+      }
+      default:
+        st ^= 1;
+    }
+  }
+  return st & 1;
+}
+
+}  // namespace wjq
