@@ -257,3 +257,92 @@ double oracle_parse_f64(const uint8_t *p, size_t n) {
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Per physical line, in the same shape as the walker test harness:
+//   blank | invalid | type | filtered | selected<TAB>kind:raw[=hexfloat]...
+// following exec/cpu.rs:299-371 with the chunk.rs line rules.
+int oracle_eval_lines(const char *query, const uint8_t *data, size_t len, char **out,
+                      size_t *out_len) {
+  Program prog;
+  QueryError qe;
+  if (!parse_query(query, prog, qe)) return 2;
+  std::vector<PathId> req = prog.required_paths(), fpaths;
+  if (prog.filter) prog.filter->visit_paths(fpaths);
+  std::string o;
+  size_t pos = 0;
+  std::vector<Slot> slots(prog.paths.size(), missing_slot());
+  std::function<bool(const Cond &)> ev = [&](const Cond &c) -> bool {
+    switch (c.tag) {
+      case Cond::Cmp: return cmp_accepts(c.op, compare(slots[c.path], c.lit));
+      case Cond::Truthy: return slots[c.path].is_truthy();
+      case Cond::And: return ev(*c.a) && ev(*c.b);
+      case Cond::Or: return ev(*c.a) || ev(*c.b);
+      default: return !ev(*c.a);
+    }
+  };
+  while (pos < len) {
+    const uint8_t *nl = (const uint8_t *)std::memchr(data + pos, '\n', len - pos);
+    size_t end = nl ? (size_t)(nl - data) : len;
+    const uint8_t *line = data + pos;
+    size_t n = end - pos;
+    pos = end + 1;
+    size_t e = n;
+    if (e && line[e - 1] == '\r') e--;
+    bool blank = true;
+    for (size_t k = 0; k < e; k++) {
+      uint8_t c = line[k];
+      if (!(c == ' ' || c == '\t' || c == '\n' || c == 0x0C || c == '\r')) blank = false;
+    }
+    if (blank) {
+      o += "blank\n";
+      continue;
+    }
+    JsonError je;
+    if (!validate(line, e, je)) {
+      o += "invalid\n";
+      continue;
+    }
+    for (auto &s : slots) s = missing_slot();
+    bool type = false;
+    for (PathId id : fpaths) {
+      std::string msg;
+      if (lookup(line, e, prog.paths[id].steps, slots[id], msg) != LookupRes::Found) type = true;
+    }
+    if (type) {
+      o += "type\n";
+      continue;
+    }
+    if (prog.filter && !ev(*prog.filter)) {
+      o += "filtered\n";
+      continue;
+    }
+    for (PathId id : req) {
+      std::string msg;
+      if (lookup(line, e, prog.paths[id].steps, slots[id], msg) != LookupRes::Found) type = true;
+    }
+    if (type) {
+      o += "type\n";
+      continue;
+    }
+    o += "selected";
+    for (PathId id : req) {
+      const Slot &s = slots[id];
+      o += "\t" + std::to_string((int)s.kind) + ":";
+      if (s.kind != Kind::Missing) o.append((const char *)s.p, s.n);
+      if (s.kind == Kind::Num) {
+        double d;
+        s.as_f64(d);
+        char b[64];
+        std::snprintf(b, sizeof b, "=%a", d);
+        o += b;
+      }
+    }
+    o += "\n";
+  }
+  *out = dup_out(o, out_len);
+  return 0;
+}
+
+}  // extern "C"

@@ -42,6 +42,7 @@ struct RowRec {
   uint32_t pad;
   // followed by n_fields x {uint32 off (relative to line), uint32 len|kind<<28|esc<<27}
 };
+static_assert(sizeof(RowRec) == kRowRecBytes, "row record header size");
 
 struct GroupTable {
   unsigned long long *slots;  // 0 = empty, else (hash << 32) | (key_id + 1)

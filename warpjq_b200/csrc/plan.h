@@ -20,6 +20,7 @@ constexpr int kMaxFields = 16;
 constexpr int kMaxBlob = 4096;
 constexpr int kMaxDepthFast = 64;  // container depth tracked in registers
 constexpr uint8_t kNoNode = 0xFF;
+constexpr uint32_t kRowRecBytes = 32;  // header of a staged row record (kernels.cuh RowRec)
 
 // JSON kind codes shared with the ABI (warpjq_group.key_kind).
 enum JKind : uint8_t {
