@@ -1,0 +1,351 @@
+"""Benchmark: GB/s scanned per query over 8 GB of device-resident nginx-style
+NDJSON on B200, for the four queries of the headline workload.
+
+One step = the four queries, each a full pass of the scan over the input:
+    select(.status == 500) | count
+    select(.status >= 500) | {p: .path, b: .bytes}
+    group_by(.host) | sum(.bytes)
+    select(.status == 500)                  (passthrough of whole lines)
+
+value   -- input bytes scanned by all ranks / device time (CUDA events on the
+           launch stream, max over ranks); inputs resident in HBM.
+e2e     -- the same queries through the host C ABI (warpjq_query_run: pinned
+           staging, 64 MiB chunks, H2D + kernels + D2H of results) from host
+           memory, wall clock.
+roofline -- the scan kernel: (input + output bytes) per launch / its
+           CUDA-event duration, against the measured HBM copy bandwidth.
+cpu_baseline -- the oracle (a C++ restatement of the reference CPU engine) on
+           all host cores over a bounded sample of the same input.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+QUERIES = [
+    "select(.status == 500) | count",
+    "select(.status >= 500) | {p: .path, b: .bytes}",
+    "group_by(.host) | sum(.bytes)",
+    "select(.status == 500)",
+]
+METRIC = "GB/s scanned per query (8 GB, device-resident); batched vs plain GB/s; p99 ms"
+WORKLOAD = ("nginx-style NDJSON (ts, host, method, path, status, bytes, latency_ms, ua), "
+            "8 GB device-resident, 4 queries per step")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def scan_traffic_ratio():
+    """DRAM bytes per input byte of the scan kernel, from the committed ncu
+    summary (profiles/k_scan_nginx.txt), or None."""
+    p = os.path.join(ROOT, "profiles", "k_scan_nginx.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_input_byte:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(data: bytes, queries, threads=0):
+    from oracle import pyoracle as orc
+    t = time.perf_counter()
+    for q in queries:
+        r = orc.run(q, data, threads=threads)
+        if r.rc != 0:
+            raise RuntimeError(r.err)
+    return time.perf_counter() - t
+
+
+def run_reference(args, rank):
+    """The reference arm: the reference's CPU engine, as restated by the
+    oracle (the Rust crate cannot be built here), on all host cores."""
+    if rank != 0:
+        return
+    import numpy as np
+    import warpjq_b200 as wjq
+    cores = os.cpu_count() or 1
+    # Size each step to ~120 s / (steps + warmup) of CPU work in total.
+    probe, used, _ = wjq.gen_nginx(64 << 20, seed=1)
+    data = bytes(probe[:used])
+    dt = cpu_baseline(data, QUERIES)
+    rate = len(data) * len(QUERIES) / dt
+    per_step = 120.0 / max(1, args.steps + args.warmup)
+    sample = int(min(1 << 30, max(16 << 20, rate * per_step / len(QUERIES))))
+    buf, used, lines = wjq.gen_nginx(sample, seed=1)
+    data = bytes(buf[:used])
+    for _ in range(args.warmup):
+        cpu_baseline(data, QUERIES)
+    t = 0.0
+    for _ in range(args.steps):
+        t += cpu_baseline(data, QUERIES)
+    value = len(data) * len(QUERIES) * args.steps / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_bytes_per_query": used, "sample_lines": lines,
+                   "queries": QUERIES},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": "port",
+                         "sample": f"{used} bytes x {len(QUERIES)} queries per step"},
+        "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--bytes", type=int, default=8_000_000_000, help="input bytes per GPU")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=256 << 20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import warpjq_b200 as wjq
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    why = wjq.probe()
+    if why:
+        raise SystemExit(f"no usable device: {why}")
+
+    # Input: generated once on the host, uploaded once.
+    n_target = args.bytes
+    host = torch.empty(n_target, dtype=torch.uint8).pin_memory()
+    hnp = host.numpy()
+    _, n, lines = wjq.gen_nginx(n_target, seed=1 + rank, into=hnp)
+    dev = torch.empty(n + 16, dtype=torch.uint8, device="cuda")
+    dev[:n].copy_(host[:n], non_blocking=False)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    qs = [wjq.Query(q) for q in QUERIES]
+    ptr = dev.data_ptr()
+
+    def step(events=None):
+        for i, q in enumerate(qs):
+            if events is not None:
+                events[i][0].record(stream)
+            q.launch_device(ptr, n, sptr)
+            if events is not None:
+                events[i][1].record(stream)
+
+    # Warm-up: grows every device buffer to its final size.
+    for _ in range(args.warmup):
+        step()
+        results = [q.collect_device() for q in qs]
+    kernels_per_step = sum(r.kernels_launched for r in results)
+    first = [(r.n_selected, r.count, r.out_len, r.isum(), r.n_groups) for r in results]
+    # Consistency: passthrough and count select the same lines; the host
+    # groups' exact sums add up to an integer.
+    assert results[0].count == results[3].n_selected, "count vs passthrough mismatch"
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [[[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
+            for _ in qs] for _ in range(args.steps)]
+    scan_ms = [0.0] * len(qs)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    per_q_ms = [sum(evs[k][i][0].elapsed_time(evs[k][i][1]) for k in range(args.steps)) / args.steps
+                for i in range(len(qs))]
+    results = [q.collect_device() for q in qs]
+    for i, r in enumerate(results):
+        scan_ms[i] = r.scan_ms
+        assert (r.n_selected, r.count, r.out_len, r.isum(), r.n_groups) == first[i], "results changed"
+
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    scanned = n * len(qs) * args.steps * world
+    value = scanned / (max_ms / 1e3) / 1e9
+
+    # Roofline of the scan kernel: algorithmic bytes = input + output.
+    hbm, which = peaks()
+    alg_bytes = sum(n + r.out_len for r in results)
+    scan_total_ms = sum(scan_ms)
+    achieved = alg_bytes / (scan_total_ms / 1e3) / 1e9 if scan_total_ms > 0 else None
+    ratio = scan_traffic_ratio()
+    traffic = int(ratio * n) if ratio else None
+
+    # End to end through the host C ABI from host memory.
+    e2e_val, h2d, d2h = None, 0, 0
+    if args.e2e_steps > 0:
+        data_np = hnp[:n]
+        host_qs = [wjq.Query(q) for q in QUERIES]
+        for q in host_qs:  # warm: allocates slots and result buffers
+            q.run(data_np[: 64 << 20])
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        te = time.perf_counter()
+        outs = 0
+        for _ in range(args.e2e_steps):
+            for q in host_qs:
+                r = q.run(data_np)
+                if r.rc != 0:
+                    raise RuntimeError(r.err)
+                outs += len(r.out)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - te
+        tt = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_val = n * len(QUERIES) * args.e2e_steps * world / float(tt.item()) / 1e9
+        h2d = n * len(QUERIES)
+        d2h = outs // args.e2e_steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample = bytes(hnp[: min(args.cpu_sample, n)])
+        cut = sample.rfind(b"\n") + 1
+        sample = sample[:cut]
+        ct = cpu_baseline(sample, QUERIES)
+        cpu = {"value": round(len(sample) * len(QUERIES) / ct / 1e9, 4), "unit": "GB/s",
+               "cores": os.cpu_count(), "kind": "port",
+               "sample": f"first {len(sample)} bytes of the input, 4 queries"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator, BASELINE nginx schema)",
+            "config": {
+                "workload": WORKLOAD, "input_bytes_per_gpu": n, "lines_per_gpu": lines,
+                "mean_line_bytes": round(n / lines, 1), "queries": QUERIES,
+                "per_query_gbs": {q: round(n / (ms / 1e3) / 1e9, 2) for q, ms in zip(QUERIES, per_q_ms)},
+                "per_query_ms": {q: round(ms, 3) for q, ms in zip(QUERIES, per_q_ms)},
+                "l2": "inputs (8 GB) larger than L2 (126 MB); no flush needed",
+                "parallelism": f"dp{world} (independent shards, no collective)",
+            },
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+                         "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4) if achieved else None,
+                         "traffic": traffic, "peak_source": which,
+                         "kernel": "k_scan (one launch per query; algorithmic bytes = input + output)"},
+            "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "GB/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": kernels_per_step * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -69,8 +69,11 @@ typedef struct {
   const warpjq_group_ext *groups;
   uint32_t n_groups;
 
-  /* Device kernels launched by the last run (for launch accounting). */
+  /* Device kernels launched by the last run (for launch accounting), and
+   * the duration of its scan kernel, from CUDA events recorded around it on
+   * the launch stream (the final attempt's, if the run was repeated). */
   uint32_t kernels_launched;
+  double scan_ms;
 } warpjq_device_result;
 
 /* Enqueues the context's query over `n_bytes` of input at device address

@@ -81,7 +81,7 @@ def _load():
     h.warpjq_query_ctx.restype = vp
     h.warpjq_query_is_aggregate.argtypes = [vp]
     h.warpjq_query_is_aggregate.restype = ctypes.c_int
-    h.warpjq_query_run.argtypes = [vp, cp, sz, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
+    h.warpjq_query_run.argtypes = [vp, vp, sz, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
                                    ctypes.POINTER(u64), cp, sz]
     h.warpjq_query_run.restype = ctypes.c_int
     h.warpjq_run_bytes.argtypes = [cp, cp, sz, u32, u32, u64, u64, ctypes.POINTER(vp),
@@ -157,7 +157,8 @@ class DeviceResult(ctypes.Structure):
                 ("n_int", ctypes.c_uint64), ("fsum", ctypes.c_double), ("min", ctypes.c_double),
                 ("max", ctypes.c_double), ("sum", ctypes.c_double),
                 ("saw_non_numeric", ctypes.c_uint32), ("groups", ctypes.POINTER(_GroupExt)),
-                ("n_groups", ctypes.c_uint32), ("kernels_launched", ctypes.c_uint32)]
+                ("n_groups", ctypes.c_uint32), ("kernels_launched", ctypes.c_uint32),
+                ("scan_ms", ctypes.c_double)]
 
     def isum(self) -> int:
         v = (self.isum_hi << 64) | self.isum_lo
@@ -199,12 +200,18 @@ class Query:
     def is_aggregate(self) -> bool:
         return bool(self._h.warpjq_query_is_aggregate(self._q))
 
-    def run(self, data: bytes, on_invalid: str = "skip", max_line_bytes: int = 0) -> RunResult:
+    def run(self, data, on_invalid: str = "skip", max_line_bytes: int = 0) -> RunResult:
+        """Runs over host memory: `data` is bytes, or a numpy uint8 array."""
+        if isinstance(data, (bytes, bytearray)):
+            keep = ctypes.c_char_p(bytes(data))
+            addr, n_bytes = ctypes.cast(keep, ctypes.c_void_p), len(data)
+        else:
+            addr, n_bytes = ctypes.c_void_p(data.ctypes.data), int(data.nbytes)
         out = ctypes.c_void_p()
         n = ctypes.c_size_t()
         st = (ctypes.c_uint64 * 5)()
         err = ctypes.create_string_buffer(4096)
-        rc = self._h.warpjq_query_run(self._q, data, len(data), ON_INVALID[on_invalid],
+        rc = self._h.warpjq_query_run(self._q, addr, n_bytes, ON_INVALID[on_invalid],
                                       max_line_bytes, ctypes.byref(out), ctypes.byref(n), st, err,
                                       len(err))
         return RunResult(rc, _take(out, n), _stats(st), err.value.decode(errors="replace"))

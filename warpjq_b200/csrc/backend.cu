@@ -161,6 +161,7 @@ struct Slot {
   size_t h_groups_cap = 0;
   bool launched = false;
   uint32_t kernels = 0;
+  cudaEvent_t scan_t0 = nullptr, scan_t1 = nullptr;  // around the scan kernel
   unsigned long long last_first_invalid = ~0ull;
   unsigned long long last_first_type = ~0ull;
 };
@@ -327,12 +328,18 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.deep_levels_per_cta = rb.deep_levels;
     sp.spin_limit = 1ull << 24;
     unsigned grid = (unsigned)std::min<unsigned long long>(c->grid, n_tiles);
+    if (!s.scan_t0) {
+      CK(cudaEventCreate(&s.scan_t0), "event");
+      CK(cudaEventCreate(&s.scan_t1), "event");
+    }
+    CK(cudaEventRecord(s.scan_t0, st), "event record");
     if (P.needs_rows)
       k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp);
     else
       k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp);
     s.kernels++;
     CK(cudaGetLastError(), "launch scan");
+    CK(cudaEventRecord(s.scan_t1, st), "event record");
     k_reduce_tiles<<<kReduceBlocks, kThreads, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
                                                        n_tiles, rb.block_f.p, rb.tiles.p,
                                                        rb.ctr.p, rb.block_lines.p);
@@ -516,6 +523,8 @@ static void free_slot(Slot &s) {
   if (s.h_line64) cudaFreeHost(s.h_line64);
   if (s.h_line32) cudaFreeHost(s.h_line32);
   if (s.h_groups) cudaFreeHost(s.h_groups);
+  if (s.scan_t0) cudaEventDestroy(s.scan_t0);
+  if (s.scan_t1) cudaEventDestroy(s.scan_t1);
   s = Slot();
 }
 
@@ -779,6 +788,11 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
     out->n_groups = (uint32_t)ctx->dev_groups.size();
   }
   out->kernels_launched = s.kernels;
+  out->scan_ms = 0.0;
+  if (s.scan_t0 && ctx->dev_n) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s.scan_t0, s.scan_t1) == cudaSuccess) out->scan_ms = ms;
+  }
   return WARPJQ_OK;
 }
 
