@@ -102,6 +102,50 @@ warpjq_status warpjq_slot_first_errors(warpjq_ctx *ctx, uint32_t slot, uint64_t 
  * 0 keeps the current value.  Both must be multiples of 1024. */
 warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t halo_bytes);
 
+/* Result of warpjq_aggregate_noalloc, written to device memory the caller
+ * owns. */
+typedef struct {
+  uint64_t n_lines;
+  uint64_t n_blank;
+  uint64_t n_invalid;
+  uint64_t n_type_error;
+  uint64_t n_selected;
+  uint64_t first_invalid; /* lowest invalid line index, or UINT64_MAX */
+  uint64_t count;
+  uint64_t numeric;
+  uint64_t isum_lo;       /* exact sum of integer-literal values, two's complement */
+  uint64_t isum_hi;
+  uint64_t n_int;
+  double fsum;            /* fixed-order FP64 sum of the other numbers */
+  double min;
+  double max;
+  double sum;             /* isum + fsum; exact while |isum| < 2^53 and fsum == 0 */
+  uint32_t saw_non_numeric;
+  uint32_t status;        /* 0 complete; 1 a fixed limit was hit, do not use the counts */
+} warpjq_noalloc_result;
+
+/* An ungrouped aggregate scan (count / sum / min / max / avg, with or without
+ * select()) that allocates no device memory; it has no counterpart in the
+ * reference.  It is for callers that cannot call cudaMalloc: an engine that
+ * gives the whole device memory to its own pool allocator at start-up leaves
+ * nothing for a library to allocate, and cudaMalloc may synchronise the
+ * device, which a caller in the middle of a latency-critical stream schedule
+ * cannot afford.
+ *
+ * The caller passes the program tables, its input in device memory (16-byte
+ * aligned, at most 4 GiB, larger inputs are rejected with
+ * WARPJQ_ERR_INVALID_ARG) and a warpjq_noalloc_result in device memory, which
+ * is written when the work on `stream` completes.  All scratch lives in one
+ * fixed array of about 7 MiB that every GPU loading this library holds
+ * until exit; every call shares it and it keeps the last call's contents, so
+ * calls that overlap on the GPU race -- order them on one stream.  The first
+ * call on each device does a one-time set-up (it looks up the array's device
+ * address); make that first call before any stream capture.  Lines nesting
+ * deeper than 65,600 levels exceed the fixed nesting stack and set status 1. */
+warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, const uint8_t *d_data,
+                                       uint64_t n_bytes, void *stream,
+                                       warpjq_noalloc_result *d_result, char *err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
-KERNEL_SRCS = [os.path.join(CSRC, "backend.cu")]
+KERNEL_SRCS = [os.path.join(CSRC, "backend.cu"), os.path.join(CSRC, "noalloc.cu")]
 KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "plan.h")]
 HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc")]
 CLI_SRCS = [os.path.join(CSRC, "host", "cli.cc")]
@@ -52,12 +52,16 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> None:
         _run([NVCC, *NVFLAGS, *extra, "-shared", "-o", so, *KERNEL_SRCS])
     static = os.path.join(LIB, "libwarpjq_kernels.a")
     if force or _stale(static, deps):
-        obj = os.path.join(LIB, "backend.o")
-        _run([NVCC, *NVFLAGS, "-c", "-o", obj, *KERNEL_SRCS])
+        objs = []
+        for src in KERNEL_SRCS:
+            obj = os.path.join(LIB, os.path.basename(src) + ".o")
+            _run([NVCC, *NVFLAGS, "-c", "-o", obj, src])
+            objs.append(obj)
         if os.path.exists(static):
             os.remove(static)
-        _run(["ar", "rcs", static, obj])
-        os.remove(obj)
+        _run(["ar", "rcs", static, *objs])
+        for obj in objs:
+            os.remove(obj)
     host = os.path.join(LIB, "libwarpjq_host.so")
     hdeps = HOST_SRCS + [os.path.join(CSRC, "host", "query.h")] + HEADERS + [so]
     if force or _stale(host, hdeps):
