@@ -99,7 +99,8 @@ warpjq_status warpjq_slot_first_errors(warpjq_ctx *ctx, uint32_t slot, uint64_t 
                                        uint64_t *first_type_error);
 
 /* Device-resident scan tunables: bytes per tile and the halo staged after it.
- * 0 keeps the current value.  Both must be multiples of 1024. */
+ * 0 keeps the current value.  The tile must be a multiple of 4096 bytes and
+ * the halo of 1024, with tile + halo below 64 KiB. */
 warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t halo_bytes);
 
 /* Result of warpjq_aggregate_noalloc, written to device memory the caller

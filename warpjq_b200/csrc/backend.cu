@@ -172,8 +172,8 @@ struct warpjq_ctx {
   DevPlan plan;
   DevPlan *d_plan = nullptr;
   unsigned long long chunk_cap = 0;
-  uint32_t tile_bytes = 32768;
-  uint32_t halo_bytes = 8192;
+  uint32_t tile_bytes = 16384;
+  uint32_t halo_bytes = 4096;
   unsigned grid = 0;        // persistent CTAs for the scan kernel
   size_t scan_smem = 0;
   std::vector<Slot> slots;
@@ -187,14 +187,6 @@ struct warpjq_ctx {
 
 namespace {
 
-size_t scan_smem_bytes(uint32_t T, uint32_t H) {
-  size_t s = T + H + 16;
-  s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
-  s += 64 * sizeof(uint32_t);
-  s = (s + 7) & ~(size_t)7;
-  s += 64 * sizeof(unsigned long long) + 8;
-  return s;
-}
 
 warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
   c->scan_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes);
@@ -725,7 +717,7 @@ warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t h
   if (!ctx) return WARPJQ_ERR_INVALID_ARG;
   uint32_t T = tile_bytes ? tile_bytes : ctx->tile_bytes;
   uint32_t H = halo_bytes ? halo_bytes : ctx->halo_bytes;
-  if (T % 1024 || H % 1024 || T < 4096 || T + H > 65535 - 16) return WARPJQ_ERR_INVALID_ARG;
+  if (T % (32 * kThreads) || H % 1024 || T + H > 65535 - 64) return WARPJQ_ERR_INVALID_ARG;
   CK(cudaDeviceSynchronize(), "sync");
   ctx->tile_bytes = T;
   ctx->halo_bytes = H;

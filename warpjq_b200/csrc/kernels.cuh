@@ -28,8 +28,22 @@
 
 namespace wjq {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 constexpr uint32_t kMaxLinesPerPass = 4096;  // line-start list capacity per pass
+
+// Dynamic shared memory of k_scan for tile T and halo H (the layout is at the
+// top of k_scan).
+__host__ __device__ inline size_t scan_smem_bytes(uint32_t T, uint32_t H) {
+  size_t nchunk_max = (T + H) / 32 + 1;
+  size_t s = T + H + 32;
+  s += 2 * nchunk_max * sizeof(uint32_t);
+  s += (nchunk_max + 15) & ~(size_t)15;
+  s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
+  s += 64 * sizeof(uint32_t);
+  s = (s + 7) & ~(size_t)7;
+  s += 64 * sizeof(unsigned long long) + 8;
+  return s;
+}
 
 // Record of one selected row, staged per CTA until the look-back resolves.
 struct RowRec {
@@ -405,9 +419,15 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
   extern __shared__ __align__(16) uint8_t smem[];
   const DevPlan &P = *sp.plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
-  uint8_t *win = smem;                                            // T + H + 16
-  uint16_t *lstart = (uint16_t *)(smem + T + H + 16);             // kMaxLinesPerPass + 1
-  uint32_t *scan_a = (uint32_t *)(lstart + kMaxLinesPerPass + 2); // 64
+  // Shared layout: window bytes, per-32-byte-chunk quote and newline masks,
+  // chunk flags, the line-start list, scan scratch.
+  const uint32_t nchunk_max = (T + H) / 32 + 1;
+  uint8_t *win = smem;                                                  // T + H + 32
+  uint32_t *qmask = (uint32_t *)(smem + T + H + 32);                    // nchunk_max
+  uint32_t *nlmask = qmask + nchunk_max;                                // nchunk_max
+  uint8_t *cflag = (uint8_t *)(nlmask + nchunk_max);                    // nchunk_max (+pad)
+  uint16_t *lstart = (uint16_t *)(cflag + ((nchunk_max + 15) & ~15u));  // kMaxLinesPerPass + 2
+  uint32_t *scan_a = (uint32_t *)(lstart + kMaxLinesPerPass + 2);       // 64
   unsigned long long *scan_b = (unsigned long long *)(((uintptr_t)(scan_a + 64) + 7) & ~(uintptr_t)7);
   __shared__ unsigned long long s_tile;
   __shared__ unsigned int s_prev_nl;
@@ -441,30 +461,72 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
     const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, sp.n - ts);
     const bool win_reaches_end = ts + wlen == sp.n;
 
-    // 1. stage tile + halo.
-    const uint32_t nfull = wlen >> 4;
-    for (uint32_t c = tid; c < nfull; c += kThreads)
-      ((uint4 *)win)[c] = __ldg((const uint4 *)(sp.data + ts) + c);
-    for (uint32_t b = (nfull << 4) + tid; b < wlen; b += kThreads) win[b] = sp.data[ts + b];
+    // 1. Stage tile + halo and classify it, 32 bytes per thread per step:
+    //    exact quote and newline bit masks, and a flag when the chunk holds
+    //    a backslash (1) or a control byte other than '\n' (2).
+    const uint32_t nchunks = (wlen + 31) >> 5;
+    for (uint32_t c = tid; c < nchunks; c += kThreads) {
+      uint32_t w[8];
+      if (c * 32 + 32 <= wlen) {
+        uint4 a = __ldg((const uint4 *)(sp.data + ts) + 2 * c);
+        uint4 b = __ldg((const uint4 *)(sp.data + ts) + 2 * c + 1);
+        w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+        w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+      } else {
+        for (int k = 0; k < 8; k++) {
+          uint32_t x = 0;
+          for (int t = 0; t < 4; t++) {
+            uint32_t at = c * 32 + k * 4 + t;
+            if (at < wlen) x |= (uint32_t)sp.data[ts + at] << (8 * t);
+          }
+          w[k] = x;
+        }
+      }
+      ((uint4 *)win)[2 * c] = make_uint4(w[0], w[1], w[2], w[3]);
+      ((uint4 *)win)[2 * c + 1] = make_uint4(w[4], w[5], w[6], w[7]);
+      uint32_t q = 0, nl = 0, anyb = 0, anyc = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        uint32_t x = w[k];
+        uint32_t tq = x ^ 0x22222222u;
+        uint32_t qf = ~(((tq & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | tq) & 0x80808080u;
+        uint32_t tn = x ^ 0x0A0A0A0Au;
+        uint32_t nfl = ~(((tn & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | tn) & 0x80808080u;
+        uint32_t tb = x ^ 0x5C5C5C5Cu;
+        anyb |= (tb - 0x01010101u) & ~tb & 0x80808080u;
+        uint32_t ctl = ~(((x & 0x7F7F7F7Fu) + 0x60606060u) | x) & 0x80808080u;  // bytes < 0x20
+        anyc |= ctl & ~nfl;
+        q |= swar_movemask(qf) << (4 * k);
+        nl |= swar_movemask(nfl) << (4 * k);
+      }
+      qmask[c] = q;
+      nlmask[c] = nl;
+      cflag[c] = (anyb ? 1u : 0u) | (anyc ? 2u : 0u);
+    }
     if (tid == 0) {
+      qmask[nchunks] = 0;
+      nlmask[nchunks] = 0;
+      cflag[nchunks] = 0;
       s_prev_nl = (ts == 0 || sp.data[ts - 1] == '\n') ? 1u : 0u;
       s_first_invalid = 0xFFFFFFFFu;
       s_first_type = 0xFFFFFFFFu;
     }
     __syncthreads();
 
-    // 2. count line starts: ts itself (after a newline) and q+1 for every
-    //    newline q in [ts, te-1).  Thread t owns bytes [t*S, (t+1)*S).
-    const uint32_t S = T / kThreads;  // T is a multiple of 1024, so S is a multiple of 4
-    const uint32_t seg0 = tid * S;
-    const uint32_t seg1 = min(seg0 + S, tlen ? tlen - 1 : 0);
+    // 2. Line starts: ts itself (after a newline) and q+1 for every newline
+    //    q in [ts, te-1).  Thread t owns chunks [t*K, (t+1)*K) of the tile.
+    const uint32_t K = T / 32 / kThreads;
+    const uint32_t nl_limit = tlen ? tlen - 1 : 0;  // newline positions below this start lines
+    auto nl_bits = [&](uint32_t c) -> uint32_t {
+      uint32_t base = c * 32;
+      if (base >= nl_limit) return 0u;
+      uint32_t m = nlmask[c];
+      if (nl_limit - base < 32) m &= (1u << (nl_limit - base)) - 1u;
+      return m;
+    };
+    const uint32_t c0 = tid * K;
     uint32_t my_nl = 0;
-    {
-      uint32_t b = seg0;
-      for (; b + 4 <= seg1; b += 4)
-        my_nl += __popc(swar_movemask(swar_newline_exact(*(const uint32_t *)(win + b))));
-      for (; b < seg1; b++) my_nl += win[b] == '\n';
-    }
+    for (uint32_t k = 0; k < K; k++) my_nl += __popc(nl_bits(c0 + k));
     uint32_t first_nl, tot_nl;
     unsigned long long dummy_e, dummy_t;
     block_scan2(my_nl, 0ull, first_nl, dummy_e, tot_nl, dummy_t, scan_a, scan_b);
@@ -481,18 +543,11 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
       {
         uint32_t idx = first_nl + lead;
         if (my_nl && idx <= base + cnt && idx + my_nl > base) {
-          uint32_t b = seg0;
-          for (; b + 4 <= seg1; b += 4) {
-            uint32_t m = swar_movemask(swar_newline_exact(*(const uint32_t *)(win + b)));
+          for (uint32_t k = 0; k < K; k++) {
+            uint32_t m = nl_bits(c0 + k);
             while (m) {
-              uint32_t k = __ffs(m) - 1;
+              uint32_t b = (c0 + k) * 32 + (uint32_t)__ffs(m) - 1;
               m &= m - 1;
-              if (idx >= base && idx <= base + cnt) lstart[idx - base] = (uint16_t)(b + k + 1);
-              idx++;
-            }
-          }
-          for (; b < seg1; b++) {
-            if (win[b] == '\n') {
               if (idx >= base && idx <= base + cnt) lstart[idx - base] = (uint16_t)(b + 1);
               idx++;
             }
@@ -525,7 +580,10 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             // last line of the tile: its newline is at or after te - 1
             uint32_t q = tlen ? tlen - 1 : 0;
             if (q < s) q = s;
-            while (q < wlen && win[q] != '\n') q++;
+            uint32_t c = q >> 5;
+            uint32_t m = nlmask[c] & (0xFFFFFFFFu << (q & 31));
+            while (!m && ++c < nchunks) m = nlmask[c];
+            q = m ? c * 32 + (uint32_t)__ffs(m) - 1 : wlen;
             if (q < wlen) e = q;
             else if (win_reaches_end) e = wlen;
             else found = false;
@@ -542,7 +600,8 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             lp = sp.data + line_abs;
             line_len = (uint32_t)(q - line_abs);
           }
-          status = walk_line(P, lp, line_len, nv, nullptr);
+          MaskView mv{qmask, cflag, s};
+          status = walk_line(P, lp, line_len, nv, nullptr, in_window ? &mv : nullptr);
         }
         // Lines nesting past 64 levels share this CTA's deep stack, so they
         // are walked one at a time.

@@ -98,9 +98,7 @@ warpjq_status noalloc_setup(int dev, DeviceSetup *&out, char *err, size_t err_le
       set_err(err, err_len, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
       return WARPJQ_ERR_CUDA;
     }
-    size_t smem = kNoAllocTile + kNoAllocHalo + 16 + (kMaxLinesPerPass + 2) * sizeof(uint16_t) +
-                  64 * sizeof(uint32_t);
-    smem = ((smem + 7) & ~(size_t)7) + 64 * sizeof(unsigned long long) + 8;
+    size_t smem = scan_smem_bytes(kNoAllocTile, kNoAllocHalo);
     e = cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
       set_err(err, err_len, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));

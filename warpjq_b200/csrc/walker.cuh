@@ -38,6 +38,16 @@ struct NodeVals {
   uint32_t len[kMaxNodes];
 };
 
+// Per-32-byte-chunk classification of the shared-memory window, made by the
+// scan kernel before the walk: raw quote positions (bit i = byte 32c+i) and
+// flags (1: the chunk holds a backslash, 2: a control byte other than '\n').
+// A string whose chunks carry no flag ends at the next raw quote.
+struct MaskView {
+  const uint32_t *q;
+  const uint8_t *cf;
+  uint32_t lo;  // window offset of the line's first byte
+};
+
 // A deep bit stack for levels >= 64 (bit = 1 for arrays), in global memory.
 struct DeepStack {
   uint32_t *words;
@@ -58,8 +68,8 @@ enum Expect : int {
 
 // Scans the string whose opening quote is at `s`.  Returns the index of the
 // closing quote, or -1 when the string is malformed or unterminated.
-__device__ __forceinline__ long long scan_string(const uint8_t *line, uint32_t n, uint32_t s,
-                                                 bool &esc) {
+__device__ __forceinline__ long long scan_string_bytes(const uint8_t *line, uint32_t n, uint32_t s,
+                                                       bool &esc) {
   uint32_t j = s + 1;
   esc = false;
   for (;;) {
@@ -91,6 +101,30 @@ __device__ __forceinline__ long long scan_string(const uint8_t *line, uint32_t n
     if (c < 0x20) return -1;
     j++;
   }
+}
+
+// With the window masks: the next raw quote closes the string unless a chunk
+// it spans holds a backslash or a control byte, in which case the bytes are
+// scanned.
+__device__ __forceinline__ long long scan_string(const uint8_t *line, uint32_t n, uint32_t s,
+                                                 bool &esc, const MaskView *mv) {
+  if (!mv) return scan_string_bytes(line, n, s, esc);
+  uint32_t a = mv->lo + s + 1;
+  uint32_t limit = mv->lo + n;
+  uint32_t wi = a >> 5;
+  uint32_t bits = mv->q[wi] & (0xFFFFFFFFu << (a & 31));
+  uint32_t f = mv->cf[wi];
+  while (bits == 0) {
+    wi++;
+    if ((wi << 5) >= limit) return -1;
+    bits = mv->q[wi];
+    f |= mv->cf[wi];
+  }
+  uint32_t close = (wi << 5) + (uint32_t)__ffs(bits) - 1;
+  if (close >= limit) return -1;
+  if (f) return scan_string_bytes(line, n, s, esc);
+  esc = false;
+  return (long long)(close - mv->lo);
 }
 
 // Validates an atom (number or literal) occupying [s, e).
@@ -167,7 +201,8 @@ __device__ __forceinline__ uint8_t index_child(const DevPlan &P, uint8_t node, u
 // Walks `line[0, n)` (no newline; a trailing '\r' is JSON whitespace).
 // `deep` may be null: a line nesting past 64 levels then returns LS_DEEP.
 __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uint32_t n,
-                                      NodeVals &v, const DeepStack *deep) {
+                                      NodeVals &v, const DeepStack *deep,
+                                      const MaskView *mv = nullptr) {
   using namespace detail;
   const uint32_t n_nodes = P.n_nodes;
   for (uint32_t k = 0; k < n_nodes; k++) v.kind[k] = JK_MISSING;
@@ -208,7 +243,7 @@ __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uin
       } else {
         if (c != '"') return LS_INVALID;
         bool esc;
-        long long e = scan_string(line, n, i, esc);
+        long long e = scan_string(line, n, i, esc, mv);
         if (e < 0) return LS_INVALID;
         uint8_t parent = depth <= kMaxDepthFast ? node_at[depth - 1] : kNoNode;
         pending = kNoNode;
@@ -297,7 +332,7 @@ __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uin
     uint32_t vend;
     if (c == '"') {
       bool esc;
-      long long e = scan_string(line, n, i, esc);
+      long long e = scan_string(line, n, i, esc, mv);
       if (e < 0) return LS_INVALID;
       vend = (uint32_t)e + 1;
       if (vn != kNoNode) v.esc[vn] = esc;
