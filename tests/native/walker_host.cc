@@ -17,6 +17,7 @@ static inline long long __double_as_longlong(double d) {
   std::memcpy(&x, &d, 8);
   return x;
 }
+static inline int __ffs(unsigned x) { return __builtin_ffs((int)x); }
 static inline double __longlong_as_double(long long x) {
   double d;
   std::memcpy(&d, &x, 8);
