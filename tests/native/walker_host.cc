@@ -18,6 +18,13 @@ static inline long long __double_as_longlong(double d) {
   return x;
 }
 static inline int __ffs(unsigned x) { return __builtin_ffs((int)x); }
+static inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
+  sh &= 31u;
+  return sh ? (lo >> sh) | (hi << (32u - sh)) : lo;
+}
+struct uint4 {
+  unsigned x, y, z, w;
+};
 static inline double __longlong_as_double(long long x) {
   double d;
   std::memcpy(&d, &x, 8);
@@ -32,10 +39,14 @@ using namespace wjq;
 
 extern "C" {
 
-// One output line per physical input line:
+// One output line per physical input line (mode 0: the bounded walker
+// walk_line; mode 1: the window walker walk_window, with the line copied at
+// a varying alignment into a window whose bytes past the newline are
+// quotes, backslashes and digits):
 //   blank | invalid | type | filtered | selected<TAB>kind:raw<TAB>...
 // Returns 0, or 2 for a query error, 3 for a plan error.
-int wh_eval(const char *query, const uint8_t *data, size_t len, char **out, size_t *out_len) {
+int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char **out,
+            size_t *out_len) {
   wjqh::Program prog;
   wjqh::QueryError qe;
   if (!wjqh::parse(query, prog, qe)) return 2;
@@ -48,14 +59,27 @@ int wh_eval(const char *query, const uint8_t *data, size_t len, char **out, size
   DeepStack deep{deep_words.data(), (uint64_t)deep_words.size() * 32};
   static NodeVals nv;
   std::string o;
-  size_t pos = 0;
+  std::vector<uint32_t> winbuf;
+  size_t pos = 0, line_no = 0;
   while (pos < len) {
     const uint8_t *nl = (const uint8_t *)std::memchr(data + pos, '\n', len - pos);
     size_t end = nl ? (size_t)(nl - data) : len;
     const uint8_t *line = data + pos;
     uint32_t n = (uint32_t)(end - pos);
     pos = end + 1;
-    int st = walk_line(P, line, n, nv, nullptr);
+    int st;
+    if (mode == 1) {
+      uint32_t s = (uint32_t)(line_no++ * 7 % 16);
+      winbuf.assign((s + n + 64) / 4 + 1, 0);
+      uint8_t *w = (uint8_t *)winbuf.data();
+      std::memcpy(w + s, line, n);
+      w[s + n] = '\n';
+      for (uint32_t k = 1; k < 40; k++) w[s + n + k] = "\"\\9"[k % 3];
+      line = w + s;
+      st = walk_window(P, w, s, s + n, nv);
+    } else {
+      st = walk_line(P, line, n, nv, nullptr);
+    }
     if (st == LS_DEEP) st = walk_line(P, line, n, nv, &deep);
     if (st == LS_BLANK) {
       o += "blank\n";

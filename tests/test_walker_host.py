@@ -1,5 +1,6 @@
-"""The device line walker and evaluator (warpjq_b200/csrc/walker.cuh),
-compiled for the host, against the oracle's per-line semantics
+"""The device line walkers (the bounded walk_line and the window walker
+walk_window) and evaluator (warpjq_b200/csrc/walker.cuh), compiled for the
+host, against the oracle's per-line semantics
 (exec/cpu.rs:299-371): same verdict per line -- blank, invalid, type error,
 filtered, selected -- and, for selected lines, the same resolved value of
 every needed path (kind, raw bytes, and the correctly rounded number)."""
@@ -28,7 +29,7 @@ def harness():
         subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-o", OUT, SRC,
                         os.path.join(ROOT, "warpjq_b200", "csrc", "host", "query.cc")], check=True)
     L = ctypes.CDLL(OUT)
-    L.wh_eval.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
+    L.wh_eval.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int,
                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]
     L.wh_free.argtypes = [ctypes.c_void_p]
     o = orc.lib()
@@ -37,10 +38,10 @@ def harness():
     return L, o
 
 
-def _run(fn, free, query, data):
+def _run(fn, free, query, data, *mode):
     p = ctypes.c_void_p()
     n = ctypes.c_size_t()
-    rc = fn(query.encode(), data, len(data), ctypes.byref(p), ctypes.byref(n))
+    rc = fn(query.encode(), data, len(data), *mode, ctypes.byref(p), ctypes.byref(n))
     assert rc == 0, (query, rc)
     out = ctypes.string_at(p.value, n.value) if p.value else b""
     free(p)
@@ -50,11 +51,12 @@ def _run(fn, free, query, data):
 def check(harness, data, queries, label):
     L, o = harness
     for q in queries:
-        dev = _run(L.wh_eval, L.wh_free, q, data)
         ref = _run(o.oracle_eval_lines, o.oracle_free, q, data)
-        assert len(dev) == len(ref), (label, q)
-        for i, (a, b) in enumerate(zip(dev, ref)):
-            assert a == b, f"{label}: `{q}` line {i}:\n walker: {a[:300]!r}\n oracle: {b[:300]!r}"
+        for mode, name in ((0, "walk_line"), (1, "walk_window")):
+            dev = _run(L.wh_eval, L.wh_free, q, data, mode)
+            assert len(dev) == len(ref), (label, q, name)
+            for i, (a, b) in enumerate(zip(dev, ref)):
+                assert a == b, f"{label}: `{q}` line {i} ({name}):\n walker: {a[:300]!r}\n oracle: {b[:300]!r}"
 
 
 def test_walker_on_hostile_corpora(harness, golden):
@@ -116,3 +118,31 @@ def test_walker_number_parsing_is_correctly_rounded(harness):
             vals.append(repr(2.0 ** rng.randrange(-1000, 1000)) + "1")
     data = "".join('{"a":%s}\n' % v for v in vals).encode()
     check(harness, data, [".a", "select(.a > 0)"], "numbers")
+
+
+def test_walker_on_mutated_lines(harness):
+    """Random byte edits of valid lines: backslash runs of every length at
+    every alignment, truncated literals and numbers, stray structure, raw
+    control bytes inside strings."""
+    import random
+    rng = random.Random(17)
+    base = corpus.corpus(9, 400).split(b"\n")[:-1]
+    base += [b'{"a":"' + b"\\" * k + b'","b":"x' + b"\\\\" * k + b'"}' for k in range(1, 12)]
+    base += [b'{"a":"' + b"y" * k + b'\\"' + b"z" * (k % 5) + b'"}' for k in range(40)]
+    alphabet = list(b'"\\{}[]:,0123456789.eE+-tfnrulsa \t\r\x0c\x01\x1f\x7f') + [0xC3, 0xA9]
+    lines = []
+    for _ in range(4000):
+        b = bytearray(rng.choice(base))
+        for _ in range(rng.randrange(1, 4)):
+            k = rng.randrange(3)
+            at = rng.randrange(len(b) + 1)
+            if k == 0:
+                b[at:at] = bytes([rng.choice(alphabet)])
+            elif k == 1 and at < len(b):
+                del b[at]
+            elif at < len(b):
+                b[at] = rng.choice(alphabet)
+        lines.append(bytes(b).replace(b"\n", b" "))
+    data = b"\n".join(lines) + b"\n"
+    check(harness, data, [".", ".a", ".status", "select(.a)", '{a: .a, b: .b}', ".arr[1]",
+                          ".nested.deep.v"], "mutated")

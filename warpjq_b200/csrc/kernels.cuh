@@ -36,8 +36,7 @@ constexpr uint32_t kMaxLinesPerPass = 4096;  // line-start list capacity per pas
 __host__ __device__ inline size_t scan_smem_bytes(uint32_t T, uint32_t H) {
   size_t nchunk_max = (T + H) / 32 + 1;
   size_t s = T + H + 32;
-  s += 2 * nchunk_max * sizeof(uint32_t);
-  s += (nchunk_max + 15) & ~(size_t)15;
+  s += ((nchunk_max + 3) & ~(size_t)3) * sizeof(uint32_t);
   s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
   s += 64 * sizeof(uint32_t);
   s = (s + 7) & ~(size_t)7;
@@ -419,14 +418,12 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
   extern __shared__ __align__(16) uint8_t smem[];
   const DevPlan &P = *sp.plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
-  // Shared layout: window bytes, per-32-byte-chunk quote and newline masks,
-  // chunk flags, the line-start list, scan scratch.
+  // Shared layout: window bytes, per-32-byte-chunk newline masks, the
+  // line-start list, scan scratch.
   const uint32_t nchunk_max = (T + H) / 32 + 1;
   uint8_t *win = smem;                                                  // T + H + 32
-  uint32_t *qmask = (uint32_t *)(smem + T + H + 32);                    // nchunk_max
-  uint32_t *nlmask = qmask + nchunk_max;                                // nchunk_max
-  uint8_t *cflag = (uint8_t *)(nlmask + nchunk_max);                    // nchunk_max (+pad)
-  uint16_t *lstart = (uint16_t *)(cflag + ((nchunk_max + 15) & ~15u));  // kMaxLinesPerPass + 2
+  uint32_t *nlmask = (uint32_t *)(smem + T + H + 32);                   // nchunk_max (+pad)
+  uint16_t *lstart = (uint16_t *)(nlmask + ((nchunk_max + 3) & ~3u));   // kMaxLinesPerPass + 2
   uint32_t *scan_a = (uint32_t *)(lstart + kMaxLinesPerPass + 2);       // 64
   unsigned long long *scan_b = (unsigned long long *)(((uintptr_t)(scan_a + 64) + 7) & ~(uintptr_t)7);
   __shared__ unsigned long long s_tile;
@@ -461,13 +458,17 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
     const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, sp.n - ts);
     const bool win_reaches_end = ts + wlen == sp.n;
 
-    // 1. Stage tile + halo and classify it, 32 bytes per thread per step:
-    //    exact quote and newline bit masks, and a flag when the chunk holds
-    //    a backslash (1) or a control byte other than '\n' (2).
+    // 1. Stage tile + halo, 32 bytes per thread per step, and mark its
+    //    newlines.  The newline flags of the eight words are gathered
+    //    in a permuted order (bit 8j+k = byte 4k+j), which costs one shift
+    //    per word, and put in byte order only for chunks that hold one.
+    //    When the window ends at the data end, a '\n' stored after the last
+    //    byte ends the last line for the walker (it is not in the masks).
     const uint32_t nchunks = (wlen + 31) >> 5;
     for (uint32_t c = tid; c < nchunks; c += kThreads) {
       uint32_t w[8];
-      if (c * 32 + 32 <= wlen) {
+      const bool full = c * 32 + 32 <= wlen;
+      if (full) {
         uint4 a = __ldg((const uint4 *)(sp.data + ts) + 2 * c);
         uint4 b = __ldg((const uint4 *)(sp.data + ts) + 2 * c + 1);
         w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
@@ -482,31 +483,32 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           w[k] = x;
         }
       }
-      ((uint4 *)win)[2 * c] = make_uint4(w[0], w[1], w[2], w[3]);
-      ((uint4 *)win)[2 * c + 1] = make_uint4(w[4], w[5], w[6], w[7]);
-      uint32_t q = 0, nl = 0, anyb = 0, anyc = 0;
+      uint32_t nl = 0;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        uint32_t x = w[k];
-        uint32_t tq = x ^ 0x22222222u;
-        uint32_t qf = ~(((tq & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | tq) & 0x80808080u;
-        uint32_t tn = x ^ 0x0A0A0A0Au;
-        uint32_t nfl = ~(((tn & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | tn) & 0x80808080u;
-        uint32_t tb = x ^ 0x5C5C5C5Cu;
-        anyb |= (tb - 0x01010101u) & ~tb & 0x80808080u;
-        uint32_t ctl = ~(((x & 0x7F7F7F7Fu) + 0x60606060u) | x) & 0x80808080u;  // bytes < 0x20
-        anyc |= ctl & ~nfl;
-        q |= swar_movemask(qf) << (4 * k);
-        nl |= swar_movemask(nfl) << (4 * k);
+        uint32_t t = w[k] ^ 0x0A0A0A0Au;
+        nl |= (~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u) >> (7 - k);
       }
-      qmask[c] = q;
+      if (nl) {
+        uint32_t nat = 0;
+        while (nl) {
+          uint32_t bit = (uint32_t)__ffs(nl) - 1u;
+          nl &= nl - 1u;
+          nat |= 1u << (((bit & 7u) << 2) | (bit >> 3));
+        }
+        nl = nat;
+      }
       nlmask[c] = nl;
-      cflag[c] = (anyb ? 1u : 0u) | (anyc ? 2u : 0u);
+      if (!full && win_reaches_end) {
+        uint32_t at = wlen - c * 32;
+        w[at >> 2] |= (uint32_t)'\n' << (8 * (at & 3));
+      }
+      ((uint4 *)win)[2 * c] = make_uint4(w[0], w[1], w[2], w[3]);
+      ((uint4 *)win)[2 * c + 1] = make_uint4(w[4], w[5], w[6], w[7]);
     }
     if (tid == 0) {
-      qmask[nchunks] = 0;
       nlmask[nchunks] = 0;
-      cflag[nchunks] = 0;
+      if (win_reaches_end && (wlen & 31u) == 0) win[wlen] = '\n';
       s_prev_nl = (ts == 0 || sp.data[ts - 1] == '\n') ? 1u : 0u;
       s_first_invalid = 0xFFFFFFFFu;
       s_first_type = 0xFFFFFFFFu;
@@ -600,8 +602,8 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             lp = sp.data + line_abs;
             line_len = (uint32_t)(q - line_abs);
           }
-          MaskView mv{qmask, cflag, s};
-          status = walk_line(P, lp, line_len, nv, nullptr, in_window ? &mv : nullptr);
+          status = in_window ? walk_window(P, win, s, s + line_len, nv)
+                             : walk_line(P, lp, line_len, nv, nullptr);
         }
         // Lines nesting past 64 levels share this CTA's deep stack, so they
         // are walked one at a time.

@@ -38,16 +38,6 @@ struct NodeVals {
   uint32_t len[kMaxNodes];
 };
 
-// Per-32-byte-chunk classification of the shared-memory window, made by the
-// scan kernel before the walk: raw quote positions (bit i = byte 32c+i) and
-// flags (1: the chunk holds a backslash, 2: a control byte other than '\n').
-// A string whose chunks carry no flag ends at the next raw quote.
-struct MaskView {
-  const uint32_t *q;
-  const uint8_t *cf;
-  uint32_t lo;  // window offset of the line's first byte
-};
-
 // A deep bit stack for levels >= 64 (bit = 1 for arrays), in global memory.
 struct DeepStack {
   uint32_t *words;
@@ -101,30 +91,6 @@ __device__ __forceinline__ long long scan_string_bytes(const uint8_t *line, uint
     if (c < 0x20) return -1;
     j++;
   }
-}
-
-// With the window masks: the next raw quote closes the string unless a chunk
-// it spans holds a backslash or a control byte, in which case the bytes are
-// scanned.
-__device__ __forceinline__ long long scan_string(const uint8_t *line, uint32_t n, uint32_t s,
-                                                 bool &esc, const MaskView *mv) {
-  if (!mv) return scan_string_bytes(line, n, s, esc);
-  uint32_t a = mv->lo + s + 1;
-  uint32_t limit = mv->lo + n;
-  uint32_t wi = a >> 5;
-  uint32_t bits = mv->q[wi] & (0xFFFFFFFFu << (a & 31));
-  uint32_t f = mv->cf[wi];
-  while (bits == 0) {
-    wi++;
-    if ((wi << 5) >= limit) return -1;
-    bits = mv->q[wi];
-    f |= mv->cf[wi];
-  }
-  uint32_t close = (wi << 5) + (uint32_t)__ffs(bits) - 1;
-  if (close >= limit) return -1;
-  if (f) return scan_string_bytes(line, n, s, esc);
-  esc = false;
-  return (long long)(close - mv->lo);
 }
 
 // Validates an atom (number or literal) occupying [s, e).
@@ -201,8 +167,7 @@ __device__ __forceinline__ uint8_t index_child(const DevPlan &P, uint8_t node, u
 // Walks `line[0, n)` (no newline; a trailing '\r' is JSON whitespace).
 // `deep` may be null: a line nesting past 64 levels then returns LS_DEEP.
 __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uint32_t n,
-                                      NodeVals &v, const DeepStack *deep,
-                                      const MaskView *mv = nullptr) {
+                                      NodeVals &v, const DeepStack *deep) {
   using namespace detail;
   const uint32_t n_nodes = P.n_nodes;
   for (uint32_t k = 0; k < n_nodes; k++) v.kind[k] = JK_MISSING;
@@ -243,7 +208,7 @@ __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uin
       } else {
         if (c != '"') return LS_INVALID;
         bool esc;
-        long long e = scan_string(line, n, i, esc, mv);
+        long long e = scan_string_bytes(line, n, i, esc);
         if (e < 0) return LS_INVALID;
         uint8_t parent = depth <= kMaxDepthFast ? node_at[depth - 1] : kNoNode;
         pending = kNoNode;
@@ -332,7 +297,7 @@ __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uin
     uint32_t vend;
     if (c == '"') {
       bool esc;
-      long long e = scan_string(line, n, i, esc, mv);
+      long long e = scan_string_bytes(line, n, i, esc);
       if (e < 0) return LS_INVALID;
       vend = (uint32_t)e + 1;
       if (vn != kNoNode) v.esc[vn] = esc;
@@ -347,6 +312,280 @@ __device__ __noinline__ int walk_line(const DevPlan &P, const uint8_t *line, uin
     expect = depth == 0 ? EX_END : EX_COMMA_OR_CLOSE;
   }
   return expect == EX_END ? LS_OK : LS_INVALID;
+}
+
+// ---------------------------------------------------------------------------
+// The window walker: the same semantics as walk_line for a line staged in a
+// shared-memory window, where the line's own newline (or one stored after
+// the data end) terminates every scan, so no step needs a bounds check.
+// ---------------------------------------------------------------------------
+
+namespace detail {
+
+// JSON whitespace inside a line ('\n' ends the line).
+__device__ __forceinline__ bool is_ws3(uint32_t c) { return c == ' ' || c == '\t' || c == '\r'; }
+
+__device__ __forceinline__ uint32_t skip_ws3(const uint8_t *w, uint32_t i) {
+  while (is_ws3(w[i])) i++;
+  return i;
+}
+
+// Four bytes at any offset of a 4-byte-aligned window.
+__device__ __forceinline__ uint32_t load4(const uint8_t *w, uint32_t i) {
+  const uint32_t *p = (const uint32_t *)(w + (i & ~3u));
+  return __funnelshift_r(p[0], p[1], (i & 3u) * 8u);
+}
+
+// 0x80 in the byte lanes of `x` holding '"', '\\' or a byte below 0x20.  The
+// lowest flagged lane is exact; lanes above a flagged lane may be flagged
+// spuriously (a borrow), which callers check for.
+__device__ __forceinline__ uint32_t str_special(uint32_t x) {
+  uint32_t q = x ^ 0x22222222u;
+  uint32_t b = x ^ 0x5C5C5C5Cu;
+  return (((q - 0x01010101u) & ~q) | ((b - 0x01010101u) & ~b) | ((x - 0x20202020u) & ~x)) &
+         0x80808080u;
+}
+
+// Number of ASCII digits starting at w[j].
+__device__ __forceinline__ uint32_t digit_run(const uint8_t *w, uint32_t j) {
+  uint32_t n = 0;
+  for (;;) {
+    uint32_t x = load4(w, j + n);
+    // a byte is a digit when its high nibble is 3 and its low nibble is <= 9
+    uint32_t nd = ((x & 0xF0F0F0F0u) ^ 0x30303030u) | (((x & 0x0F0F0F0Fu) + 0x06060606u) & 0x10101010u);
+    if (nd) return n + (((uint32_t)__ffs(nd) - 1u) >> 3);
+    n += 4;
+  }
+}
+
+__device__ __forceinline__ bool simple_escape(uint32_t e) {
+  return e == '"' || e == '\\' || e == '/' || e == 'b' || e == 'f' || e == 'n' || e == 'r' ||
+         e == 't';
+}
+
+// Closing quote of the string opened at w[i], or 0 when the string is
+// malformed (a bad escape, a raw control byte) or reaches the newline.
+// `esc` reports whether the body holds a backslash.
+__device__ __forceinline__ uint32_t win_string(const uint8_t *w, uint32_t i, bool &esc) {
+  uint32_t p = i + 1;
+  esc = false;
+  for (;;) {
+    uint32_t wa = p & ~3u;
+    uint32_t f = str_special(*(const uint32_t *)(w + wa)) & (0xFFFFFFFFu << ((p & 3u) * 8u));
+    if (!f) {
+      wa += 4;
+      while (wa & 15u) {
+        f = str_special(*(const uint32_t *)(w + wa));
+        if (f) break;
+        wa += 4;
+      }
+      while (!f) {
+        uint4 x = *(const uint4 *)(w + wa);
+        uint32_t f0 = str_special(x.x), f1 = str_special(x.y), f2 = str_special(x.z),
+                 f3 = str_special(x.w);
+        if (f0 | f1 | f2 | f3) {
+          if (f0) {
+            f = f0;
+          } else if (f1) {
+            f = f1;
+            wa += 4;
+          } else if (f2) {
+            f = f2;
+            wa += 8;
+          } else {
+            f = f3;
+            wa += 12;
+          }
+        } else {
+          wa += 16;
+        }
+      }
+    }
+    p = wa + (((uint32_t)__ffs(f) - 1u) >> 3);
+    uint32_t c = w[p];
+    if (c == '"') return p;
+    if (c == '\\') {
+      esc = true;
+      uint32_t e = w[p + 1];
+      if (e == 'u') {
+        if (hex_val(w[p + 2]) < 0 || hex_val(w[p + 3]) < 0 || hex_val(w[p + 4]) < 0 ||
+            hex_val(w[p + 5]) < 0)
+          return 0;
+        p += 6;
+      } else {
+        if (!simple_escape(e)) return 0;
+        p += 2;
+      }
+      continue;
+    }
+    if (c < 0x20) return 0;
+    p++;  // a spurious flag above a masked-off lane
+  }
+}
+
+// End (exclusive) of the number or literal starting at w[i] == c, or 0 when
+// it is malformed.  The byte after it is checked by the caller.
+__device__ __forceinline__ uint32_t win_atom(const uint8_t *w, uint32_t i, uint32_t c) {
+  if (c == 't') return load4(w, i) == 0x65757274u ? i + 4 : 0;      // "true"
+  if (c == 'n') return load4(w, i) == 0x6C6C756Eu ? i + 4 : 0;      // "null"
+  if (c == 'f') return load4(w, i + 1) == 0x65736C61u ? i + 5 : 0;  // "alse"
+  // -?(0|[1-9][0-9]*)(\.[0-9]+)?([eE][+-]?[0-9]+)?   (json.rs:370-410)
+  uint32_t j = i;
+  if (c == '-') c = w[++j];
+  if (c - '0' >= 10u) return 0;
+  uint32_t d = digit_run(w, j);
+  if (c == '0' && d > 1) return 0;
+  j += d;
+  c = w[j];
+  if (c == '.') {
+    d = digit_run(w, j + 1);
+    if (!d) return 0;
+    j += 1 + d;
+    c = w[j];
+  }
+  if ((c | 0x20u) == 'e') {
+    c = w[++j];
+    if (c == '+' || c == '-') j++;
+    d = digit_run(w, j);
+    if (!d) return 0;
+    j += d;
+  }
+  return j;
+}
+
+}  // namespace detail
+
+// Walks the line w[s, e) of a window.  w must be 4-byte aligned, w[e] must
+// be '\n' and the 16 bytes after it readable.  Offsets recorded in `v` are
+// relative to s.  Lines nesting past 64 levels return LS_DEEP.
+__device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, uint32_t s,
+                                           uint32_t e, NodeVals &v) {
+  using namespace detail;
+  const uint32_t n_nodes = P.n_nodes;
+  for (uint32_t k = 0; k < n_nodes; k++) v.kind[k] = JK_MISSING;
+
+  uint32_t i = s;
+  uint32_t c = w[i];
+  if (is_ws3(c)) {
+    i = skip_ws3(w, i);
+    c = w[i];
+  }
+  if (c == '\n') return LS_BLANK;
+  if (c == 0x0C) {  // form feed counts toward a blank line, not toward JSON
+    for (; i < e; i++) {
+      c = w[i];
+      if (!(is_ws3(c) || c == 0x0C)) return LS_INVALID;
+    }
+    return LS_BLANK;
+  }
+
+  uint64_t arrs = 0;  // bit d: the container open at depth d is an array
+  uint32_t depth = 0;
+  uint32_t cur = kNoNode, idx = 0;  // trie node and element index of the innermost container
+  uint8_t stk_node[kMaxDepthFast];
+  uint32_t stk_idx[kMaxDepthFast];
+  uint32_t vn = n_nodes ? 0u : kNoNode;  // node the next value lands on
+  bool want_key = false;
+
+  for (;;) {
+    if (want_key) {
+      if (c != '"') return LS_INVALID;
+      bool esc;
+      uint32_t q = win_string(w, i, esc);
+      if (!q) return LS_INVALID;
+      vn = kNoNode;
+      if (cur != kNoNode && P.nodes[cur].has_key_children)
+        vn = match_key(P, (uint8_t)cur, w + i + 1, q - i - 1, esc);
+      i = q + 1;
+      c = w[i];
+      if (c != ':') {
+        if (!is_ws3(c)) return LS_INVALID;
+        i = skip_ws3(w, i);
+        if (w[i] != ':') return LS_INVALID;
+      }
+      c = w[++i];
+      if (is_ws3(c)) {
+        i = skip_ws3(w, i);
+        c = w[i];
+      }
+    }
+    // A value starts at w[i] == c.
+    if (vn != kNoNode) {
+      for (uint32_t k = vn + 1u; k < P.nodes[vn].subtree_end; k++) v.kind[k] = JK_MISSING;
+      v.kind[vn] = kind_of(c);
+      v.off[vn] = i - s;
+      v.esc[vn] = 0;
+    }
+    if (c == '{' || c == '[') {
+      if (depth >= kMaxDepthFast) return LS_DEEP;
+      const bool arr = c == '[';
+      if (arr) arrs |= 1ull << depth;
+      else arrs &= ~(1ull << depth);
+      stk_node[depth] = (uint8_t)cur;
+      stk_idx[depth] = idx;
+      depth++;
+      cur = vn;
+      idx = 0;
+      c = w[++i];
+      if (is_ws3(c)) {
+        i = skip_ws3(w, i);
+        c = w[i];
+      }
+      if (c != (arr ? (uint32_t)']' : (uint32_t)'}')) {
+        want_key = !arr;
+        vn = arr ? index_child(P, (uint8_t)cur, 0) : kNoNode;
+        continue;
+      }
+      // an empty container: its close is taken below
+    } else {
+      uint32_t j;
+      if (c == '"') {
+        bool esc;
+        j = win_string(w, i, esc);
+        if (!j) return LS_INVALID;
+        j++;
+        if (vn != kNoNode) v.esc[vn] = esc;
+      } else {
+        j = win_atom(w, i, c);
+        if (!j) return LS_INVALID;
+      }
+      if (vn != kNoNode) v.len[vn] = j - i;
+      i = j;
+      c = w[i];
+      if (is_ws3(c)) {
+        i = skip_ws3(w, i);
+        c = w[i];
+      }
+    }
+    // After a value: commas and closing brackets.
+    for (;;) {
+      if (depth == 0) return c == '\n' ? LS_OK : LS_INVALID;
+      const bool arr = (arrs >> (depth - 1)) & 1;
+      if (c == ',') {
+        c = w[++i];
+        if (is_ws3(c)) {
+          i = skip_ws3(w, i);
+          c = w[i];
+        }
+        if (arr) {
+          idx++;
+          vn = index_child(P, (uint8_t)cur, idx);
+        }
+        want_key = !arr;
+        break;
+      }
+      if (c != (arr ? (uint32_t)']' : (uint32_t)'}')) return LS_INVALID;
+      if (cur != kNoNode) v.len[cur] = i + 1 - s - v.off[cur];
+      depth--;
+      cur = stk_node[depth];
+      idx = stk_idx[depth];
+      c = w[++i];
+      if (is_ws3(c)) {
+        i = skip_ws3(w, i);
+        c = w[i];
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
