@@ -216,6 +216,7 @@ def main():
     sptr = stream.cuda_stream
 
     qs = [wjq.Query(q) for q in QUERIES]
+    tiling = [q.autotile(hnp[: 1 << 20]) for q in qs]
     ptr = dev.data_ptr()
 
     def step(events=None):
@@ -328,6 +329,7 @@ def main():
                 "per_query_gbs": {q: round(n / (ms / 1e3) / 1e9, 2) for q, ms in zip(QUERIES, per_q_ms)},
                 "per_query_ms": {q: round(ms, 3) for q, ms in zip(QUERIES, per_q_ms)},
                 "l2": "inputs (8 GB) larger than L2 (126 MB); no flush needed",
+                "tile_halo_bytes": list(tiling[0]),
                 "parallelism": f"dp{world} (independent shards, no collective)",
             },
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,

@@ -98,10 +98,22 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
 warpjq_status warpjq_slot_first_errors(warpjq_ctx *ctx, uint32_t slot, uint64_t *first_invalid,
                                        uint64_t *first_type_error);
 
-/* Device-resident scan tunables: bytes per tile and the halo staged after it.
- * 0 keeps the current value.  The tile must be a multiple of 4096 bytes and
- * the halo of 1024, with tile + halo below 64 KiB. */
+/* Device-resident scan tunables: bytes per tile (one warp walks the lines
+ * starting in a tile, one line per lane) and the halo staged after it (a line
+ * that runs past tile + halo is walked from global memory, more slowly).
+ * 0 keeps the current value.  Tile and halo must be multiples of 256 bytes,
+ * the tile at least 1024 and the halo at least 512, with tile + halo below
+ * 64 KiB.  Waits for the device and releases the context's buffers. */
 warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t halo_bytes);
+
+/* Chooses the tiling for input shaped like `sample` (host bytes, e.g. the
+ * first megabyte of the input): tiles holding close to a whole number of
+ * 32-line rounds, and a halo longer than the longest line seen.  With fewer
+ * than 16 complete lines in the sample the tiling is left alone.  Applies it
+ * with warpjq_set_tiling and reports it (either pointer may be null).  No
+ * reference counterpart. */
+warpjq_status warpjq_autotile(warpjq_ctx *ctx, const uint8_t *sample, uint64_t len,
+                              uint32_t *tile_bytes, uint32_t *halo_bytes);
 
 /* Result of warpjq_aggregate_noalloc, written to device memory the caller
  * owns. */

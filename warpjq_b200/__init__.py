@@ -34,7 +34,7 @@ ABI_SYMBOLS = [
 ]
 EXT_SYMBOLS = [
     "warpjq_launch_device", "warpjq_collect_device", "warpjq_slot_first_errors",
-    "warpjq_set_tiling",
+    "warpjq_set_tiling", "warpjq_autotile",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
@@ -74,6 +74,9 @@ def _load():
     k.warpjq_collect_device.restype = ctypes.c_int
     k.warpjq_set_tiling.argtypes = [vp, u32, u32]
     k.warpjq_set_tiling.restype = ctypes.c_int
+    k.warpjq_autotile.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(u32),
+                                  ctypes.POINTER(u32)]
+    k.warpjq_autotile.restype = ctypes.c_int
     h.warpjq_query_open.argtypes = [cp, u32, u64, ctypes.POINTER(vp), cp, sz]
     h.warpjq_query_open.restype = ctypes.c_int
     h.warpjq_query_close.argtypes = [vp]
@@ -220,6 +223,20 @@ class Query:
         k, _ = _load()
         if k.warpjq_set_tiling(self.ctx, tile_bytes, halo_bytes) != 0:
             raise ValueError("bad tiling")
+
+    def autotile(self, sample) -> tuple:
+        """Chooses the device tiling from a host sample of the input (bytes or
+        a uint8 numpy array); returns (tile_bytes, halo_bytes)."""
+        k, _ = _load()
+        if isinstance(sample, (bytes, bytearray)):
+            buf = (ctypes.c_char * len(sample)).from_buffer_copy(sample)
+            addr, n = ctypes.addressof(buf), len(sample)
+        else:
+            addr, n = sample.ctypes.data, sample.nbytes
+        t, h = ctypes.c_uint32(), ctypes.c_uint32()
+        if k.warpjq_autotile(self.ctx, ctypes.c_void_p(addr), n, ctypes.byref(t), ctypes.byref(h)) != 0:
+            raise RuntimeError("autotile failed")
+        return t.value, h.value
 
     def launch_device(self, d_ptr: int, n: int, stream: int = 0):
         """Enqueues a device-resident run (no host synchronisation)."""

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -172,8 +173,8 @@ struct warpjq_ctx {
   DevPlan plan;
   DevPlan *d_plan = nullptr;
   unsigned long long chunk_cap = 0;
-  uint32_t tile_bytes = 16384;
-  uint32_t halo_bytes = 4096;
+  uint32_t tile_bytes = 6144;
+  uint32_t halo_bytes = 2048;
   unsigned grid = 0;        // persistent CTAs for the scan kernel
   size_t scan_smem = 0;
   std::vector<Slot> slots;
@@ -332,7 +333,7 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     s.kernels++;
     CK(cudaGetLastError(), "launch scan");
     CK(cudaEventRecord(s.scan_t1, st), "event record");
-    k_reduce_tiles<<<kReduceBlocks, kThreads, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
+    k_reduce_tiles<<<kReduceBlocks, kReduceThreads, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
                                                        n_tiles, rb.block_f.p, rb.tiles.p,
                                                        rb.ctr.p, rb.block_lines.p);
     s.kernels++;
@@ -717,13 +718,60 @@ warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t h
   if (!ctx) return WARPJQ_ERR_INVALID_ARG;
   uint32_t T = tile_bytes ? tile_bytes : ctx->tile_bytes;
   uint32_t H = halo_bytes ? halo_bytes : ctx->halo_bytes;
-  if (T % (32 * kThreads) || H % 1024 || T + H > 65535 - 64) return WARPJQ_ERR_INVALID_ARG;
+  if (T % 256 || T < 1024 || H % 256 || H < 512 || T + H > 65535 - 64) return WARPJQ_ERR_INVALID_ARG;
   CK(cudaDeviceSynchronize(), "sync");
   ctx->tile_bytes = T;
   ctx->halo_bytes = H;
   for (auto &s : ctx->slots) s.rb.release();
   ctx->dev.rb.release();
   return configure_grid(ctx, err, err_len);
+}
+
+warpjq_status warpjq_autotile(warpjq_ctx *ctx, const uint8_t *sample, uint64_t len,
+                              uint32_t *tile_bytes, uint32_t *halo_bytes) {
+  if (!ctx || (!sample && len)) return WARPJQ_ERR_INVALID_ARG;
+  // Line-length statistics of the complete lines in the sample.
+  uint64_t lines = 0, longest = 0;
+  double sum = 0.0, sum2 = 0.0;
+  const uint8_t *p = sample, *end = sample + len;
+  const uint8_t *nl;
+  while (p < end && (nl = (const uint8_t *)memchr(p, '\n', (size_t)(end - p))) != nullptr) {
+    double l = (double)(nl - p) + 1.0;
+    sum += l;
+    sum2 += l * l;
+    longest = std::max<uint64_t>(longest, (uint64_t)(nl - p) + 1);
+    lines++;
+    p = nl + 1;
+  }
+  uint32_t T = ctx->tile_bytes, H = ctx->halo_bytes;
+  if (lines >= 16) {
+    const double mean = sum / (double)lines;
+    const double var = std::max(0.0, sum2 / (double)lines - mean * mean);
+    const double cv = std::sqrt(var) / mean;
+    // A tile's lines are walked in rounds of 32; each tile also costs about
+    // as much as a few lines in staging and bookkeeping.  Score = lines per
+    // walked lane slot, with the line count taken two deviations high.
+    double best = -1.0;
+    uint32_t best_T = T;
+    for (uint32_t t = 1024; t <= 8192; t += 256) {
+      double L = (double)t / mean;
+      double hi = L + 2.0 * std::sqrt(L) * cv;
+      double rounds = std::ceil(hi / 32.0);
+      double score = L / (32.0 * rounds + 4.0);
+      if (score >= best - 1e-9) {
+        best = score;
+        best_T = t;
+      }
+    }
+    T = best_T;
+    uint64_t h = (longest * 3 / 2 + 255) & ~255ull;
+    H = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(h, 512), 16384);
+    if (T + H > 65535 - 64) H = ((65535 - 64 - T) & ~255u);
+  }
+  if (tile_bytes) *tile_bytes = T;
+  if (halo_bytes) *halo_bytes = H;
+  if (T == ctx->tile_bytes && H == ctx->halo_bytes) return WARPJQ_OK;
+  return warpjq_set_tiling(ctx, T, H);
 }
 
 warpjq_status warpjq_launch_device(warpjq_ctx *ctx, const uint8_t *d_data, uint64_t n_bytes,

@@ -302,6 +302,7 @@ struct warpjq_query {
   warpjq_ctx *ctx = nullptr;
   uint64_t cap = 0;
   uint32_t n_slots = 2;
+  bool tiled = false;  // device tiling chosen from the first bytes of a run
 };
 
 namespace {
@@ -452,6 +453,13 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     return 0;
   };
 
+  // Tiles sized from the input's own line lengths (first MiB of the run).
+  if (!q->tiled && len) {
+    if (warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
+        WARPJQ_OK)
+      return fail("CUDA error in choosing the device tiling");
+    q->tiled = true;
+  }
   while (pos < len) {
     // Next newline-aligned chunk of at most `cap` bytes (chunk.rs:234-278).
     uint64_t want = std::min<uint64_t>(q->cap, len - pos);
@@ -490,6 +498,9 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
       q->cap = n;
       if (warpjq_ctx_create(&q->low.prog, q->cap, q->n_slots, &q->ctx, e, sizeof e) != WARPJQ_OK)
         return fail(std::string("CUDA error in creating the device context: ") + e);
+      if (warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
+          WARPJQ_OK)
+        return fail("CUDA error in choosing the device tiling");
       next_slot = 0;
     }
     uint32_t slot = next_slot;

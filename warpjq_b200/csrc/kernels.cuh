@@ -28,8 +28,9 @@
 
 namespace wjq {
 
-constexpr int kThreads = 128;
-constexpr uint32_t kMaxLinesPerPass = 4096;  // line-start list capacity per pass
+constexpr int kThreads = 32;                 // one warp per CTA; each warp owns its tile
+constexpr uint32_t kMaxLinesPerPass = 512;   // line-start list capacity per pass
+constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
 
 // Dynamic shared memory of k_scan for tile T and halo H (the layout is at the
 // top of k_scan).
@@ -38,10 +39,7 @@ __host__ __device__ inline size_t scan_smem_bytes(uint32_t T, uint32_t H) {
   size_t s = T + H + 32;
   s += ((nchunk_max + 3) & ~(size_t)3) * sizeof(uint32_t);
   s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
-  s += 64 * sizeof(uint32_t);
-  s = (s + 7) & ~(size_t)7;
-  s += 64 * sizeof(unsigned long long) + 8;
-  return s;
+  return (s + 15) & ~(size_t)15;
 }
 
 // Record of one selected row, staged per CTA until the look-back resolves.
@@ -119,55 +117,6 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 
 __device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Block-wide exclusive scan of (a, b) in thread order.
-__device__ __forceinline__ void block_scan2(uint32_t a, unsigned long long b, uint32_t &ea,
-                                            unsigned long long &eb, uint32_t &ta,
-                                            unsigned long long &tb, uint32_t *s_a,
-                                            unsigned long long *s_b) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t ia = a;
-  unsigned long long ib = b;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    uint32_t xa = __shfl_up_sync(0xffffffffu, ia, d);
-    unsigned long long xb = __shfl_up_sync(0xffffffffu, ib, d);
-    if (lane >= d) {
-      ia += xa;
-      ib += xb;
-    }
-  }
-  if (lane == 31) {
-    s_a[warp] = ia;
-    s_b[warp] = ib;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t wa = lane < kThreads / 32 ? s_a[lane] : 0;
-    unsigned long long wb = lane < kThreads / 32 ? s_b[lane] : 0;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      uint32_t xa = __shfl_up_sync(0xffffffffu, wa, d);
-      unsigned long long xb = __shfl_up_sync(0xffffffffu, wb, d);
-      if (lane >= d) {
-        wa += xa;
-        wb += xb;
-      }
-    }
-    if (lane < kThreads / 32) {
-      s_a[lane + 32] = wa;  // inclusive warp prefix
-      s_b[lane + 32] = wb;
-    }
-  }
-  __syncthreads();
-  uint32_t wpa = warp ? s_a[32 + warp - 1] : 0;
-  unsigned long long wpb = warp ? s_b[32 + warp - 1] : 0;
-  ea = wpa + ia - a;
-  eb = wpb + ib - b;
-  ta = s_a[32 + kThreads / 32 - 1];
-  tb = s_b[32 + kThreads / 32 - 1];
-  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -409,8 +358,44 @@ struct ThreadAgg {
   }
 };
 
-__device__ __forceinline__ bool is_line_blank_byte(uint32_t c) {
-  return c == ' ' || c == '\t' || c == '\r' || c == 0x0C;
+// 16-byte global -> shared copy that does not go through registers; bytes
+// past `src_bytes` (0..16) are zero-filled and not read.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
+  return x;
+}
+
+// Exclusive warp scan of (a, b) in lane order, with the warp totals.
+__device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uint32_t &ea,
+                                           unsigned long long &eb, uint32_t &ta,
+                                           unsigned long long &tb) {
+  const int lane = threadIdx.x & 31;
+  uint32_t ia = a;
+  unsigned long long ib = b;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t xa = __shfl_up_sync(0xffffffffu, ia, d);
+    unsigned long long xb = __shfl_up_sync(0xffffffffu, ib, d);
+    if (lane >= d) {
+      ia += xa;
+      ib += xb;
+    }
+  }
+  ea = ia - a;
+  eb = ib - b;
+  ta = __shfl_sync(0xffffffffu, ia, 31);
+  tb = __shfl_sync(0xffffffffu, ib, 31);
 }
 
 template <bool kRows>
@@ -418,28 +403,23 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
   extern __shared__ __align__(16) uint8_t smem[];
   const DevPlan &P = *sp.plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
-  // Shared layout: window bytes, per-32-byte-chunk newline masks, the
-  // line-start list, scan scratch.
+  // Shared layout: window bytes (+32 readable bytes past the end for the
+  // walker's word reads), per-32-byte-chunk newline masks, line starts.
   const uint32_t nchunk_max = (T + H) / 32 + 1;
-  uint8_t *win = smem;                                                  // T + H + 32
-  uint32_t *nlmask = (uint32_t *)(smem + T + H + 32);                   // nchunk_max (+pad)
-  uint16_t *lstart = (uint16_t *)(nlmask + ((nchunk_max + 3) & ~3u));   // kMaxLinesPerPass + 2
-  uint32_t *scan_a = (uint32_t *)(lstart + kMaxLinesPerPass + 2);       // 64
-  unsigned long long *scan_b = (unsigned long long *)(((uintptr_t)(scan_a + 64) + 7) & ~(uintptr_t)7);
-  __shared__ unsigned long long s_tile;
-  __shared__ unsigned int s_prev_nl;
-  __shared__ unsigned int s_first_invalid;
-  __shared__ unsigned int s_first_type;
-  __shared__ unsigned long long s_excl[3];
-  __shared__ double s_fsum[kThreads / 32];
+  uint8_t *win = smem;                                                 // T + H + 32
+  uint32_t *nlmask = (uint32_t *)(smem + T + H + 32);                  // nchunk_max (+pad)
+  uint16_t *lstart = (uint16_t *)(nlmask + ((nchunk_max + 3) & ~3u));  // kMaxLinesPerPass + 2
 
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int lane = threadIdx.x;
   const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
   const uint32_t rec_stride = P.rec_stride;
   uint8_t *my_recs = sp.rec_scratch + (unsigned long long)blockIdx.x * sp.rec_cap_per_cta * rec_stride;
   DeepStack deep;
   deep.words = sp.deep_words + (unsigned long long)blockIdx.x * (sp.deep_levels_per_cta / 32);
   deep.cap_levels = sp.deep_levels_per_cta;
+  // Lane l lists the newlines of tile chunks [l*K, l*K + K).
+  const uint32_t K = (T / 32 + 31) / 32;
+  const uint32_t c0 = lane * K;
 
   ThreadAgg agg;
   agg.init();
@@ -448,9 +428,9 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
   SlotVal slots[kMaxSlots];
 
   for (;;) {
-    if (tid == 0) s_tile = atomicAdd(&sp.ctr->next_tile, 1ull);
-    __syncthreads();
-    const unsigned long long tile = s_tile;
+    unsigned long long tile = 0;
+    if (lane == 0) tile = atomicAdd(&sp.ctr->next_tile, 1ull);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= sp.n_tiles) break;
     const unsigned long long ts = tile * T;
     const unsigned long long te = min(ts + T, sp.n);
@@ -458,31 +438,22 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
     const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, sp.n - ts);
     const bool win_reaches_end = ts + wlen == sp.n;
 
-    // 1. Stage tile + halo, 32 bytes per thread per step, and mark its
-    //    newlines.  The newline flags of the eight words are gathered
-    //    in a permuted order (bit 8j+k = byte 4k+j), which costs one shift
-    //    per word, and put in byte order only for chunks that hold one.
-    //    When the window ends at the data end, a '\n' stored after the last
-    //    byte ends the last line for the walker (it is not in the masks).
+    // 1. Stage tile + halo with asynchronous 16-byte copies.
+    const uint32_t n16 = (wlen + 15) >> 4;
+    for (uint32_t k = lane; k < n16; k += 32)
+      cp_async16(win + k * 16, sp.data + ts + k * 16, min(16u, wlen - k * 16));
+    const uint32_t prev_nl = (ts == 0 || sp.data[ts - 1] == '\n') ? 1u : 0u;
+    cp_async_wait_all();
+    __syncwarp();
+
+    // 2. Newline masks per 32-byte chunk.  The flags of the eight words
+    //    are gathered in a permuted order (bit 8j+k = byte 4k+j), one shift
+    //    per word, and put in byte order only for chunks holding one.
     const uint32_t nchunks = (wlen + 31) >> 5;
-    for (uint32_t c = tid; c < nchunks; c += kThreads) {
-      uint32_t w[8];
-      const bool full = c * 32 + 32 <= wlen;
-      if (full) {
-        uint4 a = __ldg((const uint4 *)(sp.data + ts) + 2 * c);
-        uint4 b = __ldg((const uint4 *)(sp.data + ts) + 2 * c + 1);
-        w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
-        w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
-      } else {
-        for (int k = 0; k < 8; k++) {
-          uint32_t x = 0;
-          for (int t = 0; t < 4; t++) {
-            uint32_t at = c * 32 + k * 4 + t;
-            if (at < wlen) x |= (uint32_t)sp.data[ts + at] << (8 * t);
-          }
-          w[k] = x;
-        }
-      }
+    for (uint32_t c = lane; c < nchunks; c += 32) {
+      const uint4 a = ((const uint4 *)win)[2 * c];
+      const uint4 b = ((const uint4 *)win)[2 * c + 1];
+      const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
       uint32_t nl = 0;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
@@ -497,28 +468,20 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           nat |= 1u << (((bit & 7u) << 2) | (bit >> 3));
         }
         nl = nat;
+        if (wlen - c * 32 < 32) nl &= (1u << (wlen - c * 32)) - 1u;  // bytes past the data
       }
       nlmask[c] = nl;
-      if (!full && win_reaches_end) {
-        uint32_t at = wlen - c * 32;
-        w[at >> 2] |= (uint32_t)'\n' << (8 * (at & 3));
-      }
-      ((uint4 *)win)[2 * c] = make_uint4(w[0], w[1], w[2], w[3]);
-      ((uint4 *)win)[2 * c + 1] = make_uint4(w[4], w[5], w[6], w[7]);
     }
-    if (tid == 0) {
+    if (lane == 0) {
       nlmask[nchunks] = 0;
-      if (win_reaches_end && (wlen & 31u) == 0) win[wlen] = '\n';
-      s_prev_nl = (ts == 0 || sp.data[ts - 1] == '\n') ? 1u : 0u;
-      s_first_invalid = 0xFFFFFFFFu;
-      s_first_type = 0xFFFFFFFFu;
+      // A '\n' after the last byte ends the last line for the walker.
+      if (win_reaches_end) win[wlen] = '\n';
     }
-    __syncthreads();
+    __syncwarp();
 
-    // 2. Line starts: ts itself (after a newline) and q+1 for every newline
-    //    q in [ts, te-1).  Thread t owns chunks [t*K, (t+1)*K) of the tile.
-    const uint32_t K = T / 32 / kThreads;
-    const uint32_t nl_limit = tlen ? tlen - 1 : 0;  // newline positions below this start lines
+    // 3. Lines starting in the tile: ts itself (after a newline) and q+1 for
+    //    every newline q in [ts, te-1).
+    const uint32_t nl_limit = tlen ? tlen - 1 : 0;
     auto nl_bits = [&](uint32_t c) -> uint32_t {
       uint32_t base = c * 32;
       if (base >= nl_limit) return 0u;
@@ -526,22 +489,22 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
       if (nl_limit - base < 32) m &= (1u << (nl_limit - base)) - 1u;
       return m;
     };
-    const uint32_t c0 = tid * K;
     uint32_t my_nl = 0;
     for (uint32_t k = 0; k < K; k++) my_nl += __popc(nl_bits(c0 + k));
     uint32_t first_nl, tot_nl;
     unsigned long long dummy_e, dummy_t;
-    block_scan2(my_nl, 0ull, first_nl, dummy_e, tot_nl, dummy_t, scan_a, scan_b);
-    const uint32_t lead = s_prev_nl;
+    warp_scan2(my_nl, 0ull, first_nl, dummy_e, tot_nl, dummy_t);
+    const uint32_t lead = prev_nl;
     const uint32_t n_lines_tile = tot_nl + lead;
 
-    // 3. walk the lines, pass by pass.
+    // 4. Walk the lines, one per lane, in passes of the list's capacity.
     unsigned long long tile_rows = 0, tile_bytes = 0;
-    double fsum_thread = 0.0;
+    double fsum_lane = 0.0;
+    uint32_t tile_first_invalid = 0xFFFFFFFFu, tile_first_type = 0xFFFFFFFFu;
     for (uint32_t base = 0; base < n_lines_tile; base += kMaxLinesPerPass) {
       const uint32_t cnt = min(n_lines_tile - base, kMaxLinesPerPass);
       // list line starts [base, base + cnt] (one extra as the end marker)
-      if (lead && tid == 0 && base == 0) lstart[0] = 0;
+      if (lead && lane == 0 && base == 0) lstart[0] = 0;
       {
         uint32_t idx = first_nl + lead;
         if (my_nl && idx <= base + cnt && idx + my_nl > base) {
@@ -556,9 +519,9 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           }
         }
       }
-      __syncthreads();
-      for (uint32_t b0 = 0; b0 < cnt; b0 += kThreads) {
-        const uint32_t li = b0 + tid;  // line index within the pass
+      __syncwarp();
+      for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
+        const uint32_t li = b0 + lane;  // line index within the pass
         int status = -1;
         uint32_t has_row = 0, row_len = 0;
         unsigned long long line_abs = 0;
@@ -594,6 +557,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           if (found) {
             lp = win + s;
             line_len = e - s;
+            status = walk_window(P, win, s, e, nv);
           } else {
             // longer than the window: walk it from global memory
             in_window = false;
@@ -601,22 +565,21 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             while (q < sp.n && sp.data[q] != '\n') q++;
             lp = sp.data + line_abs;
             line_len = (uint32_t)(q - line_abs);
+            status = walk_line(P, lp, line_len, nv, nullptr);
           }
-          status = in_window ? walk_window(P, win, s, s + line_len, nv)
-                             : walk_line(P, lp, line_len, nv, nullptr);
         }
         // Lines nesting past 64 levels share this CTA's deep stack, so they
         // are walked one at a time.
-        if (__syncthreads_or(status == LS_DEEP)) {
-          for (int t = 0; t < kThreads; t++) {
-            if (tid == t && status == LS_DEEP) {
+        if (__any_sync(0xffffffffu, status == LS_DEEP)) {
+          for (int t = 0; t < 32; t++) {
+            if (lane == t && status == LS_DEEP) {
               status = walk_line(P, lp, line_len, nv, &deep);
               if (status == LS_DEEP_FULL) {
                 atomicOr(&sp.ctr->overflow, 8u);
                 status = LS_INVALID;
               }
             }
-            __syncthreads();
+            __syncwarp();
           }
         }
         // `line_len` for output excludes a trailing '\r' (chunk.rs:433-435).
@@ -642,15 +605,15 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             status = 101;  // selected
           }
         }
-        if (status == LS_BLANK) c_blank++;
-        else if (status == LS_INVALID) {
+        if (status == LS_BLANK) {
+          c_blank++;
+        } else if (status == LS_INVALID) {
           c_invalid++;
-          atomicMin(&s_first_invalid, ordinal);
+          tile_first_invalid = min(tile_first_invalid, ordinal);
         } else if (status == LS_TYPE_ERROR) {
           c_type++;
-          atomicMin(&s_first_type, ordinal);
-        }
-        else if (status == 101) {
+          tile_first_type = min(tile_first_type, ordinal);
+        } else if (status == 101) {
           c_sel++;
           if (kRows) {
             has_row = 1;
@@ -688,7 +651,6 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
 
         // Aggregate contribution of this line.
         bool contrib = !kRows && status == 101;
-        unsigned long long v_num = 0, v_int = 0;
         long long iv = 0;
         double fv = 0.0;
         bool is_int = false, is_num = false;
@@ -700,8 +662,6 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             agg.saw = 1;
           }
         }
-        (void)v_num;
-        (void)v_int;
         if (contrib && !has_group) {
           agg.count++;
           if (is_num) {
@@ -713,12 +673,11 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
               agg.add_int(iv);
               agg.n_int++;
             } else {
-              fsum_thread += fv;
+              fsum_lane += fv;
             }
           }
         }
         if (!kRows && P.group_slot >= 0) {
-          // Group updates, aggregated per warp on the key id.
           uint32_t kid = 0xFFFFFFFFu;
           if (has_group) kid = group_find_or_insert(sp, gk, gh);
           const GroupTable &g = sp.g;
@@ -745,11 +704,9 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
         }
 
         if (kRows) {
-          uint32_t er;
-          unsigned long long eb;
-          uint32_t tr;
-          unsigned long long tb;
-          block_scan2(has_row, (unsigned long long)row_len, er, eb, tr, tb, scan_a, scan_b);
+          uint32_t er, tr;
+          unsigned long long eb, tb;
+          warp_scan2(has_row, (unsigned long long)row_len, er, eb, tr, tb);
           if (has_row) {
             unsigned long long ri = tile_rows + er;
             if (ri < sp.rec_cap_per_cta) {
@@ -774,76 +731,86 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           tile_bytes += tb;
         }
       }
-      __syncthreads();
+      __syncwarp();
     }
-    c_lines += (tid == 0) ? n_lines_tile : 0;
+    if (lane == 0) c_lines += n_lines_tile;
 
     // Per-tile bookkeeping.
-    if (tid == 0) {
+    tile_first_invalid = __reduce_min_sync(0xffffffffu, tile_first_invalid);
+    tile_first_type = __reduce_min_sync(0xffffffffu, tile_first_type);
+    if (lane == 0) {
       sp.tiles[tile].n_lines = n_lines_tile;
-      sp.tiles[tile].first_invalid = s_first_invalid;
-      sp.tiles[tile].first_type_error = s_first_type;
-      if (s_first_invalid != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_invalid_tile, tile);
-      if (s_first_type != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_type_tile, tile);
+      sp.tiles[tile].first_invalid = tile_first_invalid;
+      sp.tiles[tile].first_type_error = tile_first_type;
+      if (tile_first_invalid != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_invalid_tile, tile);
+      if (tile_first_type != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_type_tile, tile);
     }
     if (!kRows) {
-      // fixed-order tree: warp shuffle tree, then warps in order
-      double f = fsum_thread;
+      // fixed-order tree over the lanes
+      double f = fsum_lane;
 #pragma unroll
       for (int d = 16; d > 0; d >>= 1) f += __shfl_down_sync(0xffffffffu, f, d);
-      if (lane == 0) s_fsum[warp] = f;
-      __syncthreads();
-      if (tid == 0) {
-        double t = 0.0;
-        for (int w = 0; w < kThreads / 32; w++) t += s_fsum[w];
-        sp.tile_fsum[tile] = t;
-      }
-      __syncthreads();
+      if (lane == 0) sp.tile_fsum[tile] = f;
       continue;
     }
 
-    // 4. look-back for this tile's row / byte / line prefix.
-    if (tid == 0) {
-      unsigned long long mine[3] = {tile_rows, tile_bytes, (unsigned long long)n_lines_tile};
-      unsigned long long ex[3] = {0, 0, 0};
-      if (tile == 0) {
+    // 5. Look-back for this tile's row / byte / line prefix, 32 earlier
+    //    tiles per step (lane l reads tile j_hi - l).
+    const unsigned long long mine[3] = {tile_rows, tile_bytes, (unsigned long long)n_lines_tile};
+    unsigned long long ex[3] = {0, 0, 0};
+    if (tile == 0) {
+      if (lane == 0) {
         for (int k = 0; k < 3; k++) sp.lb_incl[k] = mine[k];
         __threadfence();
         st_release(&sp.lb_flag[0], 2u);
-      } else {
+      }
+    } else {
+      if (lane == 0) {
         for (int k = 0; k < 3; k++) sp.lb_agg[tile * 3 + k] = mine[k];
         __threadfence();
         st_release(&sp.lb_flag[tile], 1u);
-        long long j = (long long)tile - 1;
-        unsigned long long spins = 0;
-        while (j >= 0) {
-          unsigned f = ld_acquire(&sp.lb_flag[j]);
-          if (f == 0) {
-            if (++spins > sp.spin_limit) {
-              atomicOr(&sp.ctr->error, 1u);
-              break;
-            }
-            __nanosleep(64);
-            continue;
+      }
+      long long j_hi = (long long)tile - 1;
+      unsigned long long spins = 0;
+      bool failed = false;
+      for (;;) {
+        const long long j = j_hi - lane;
+        unsigned f = j >= 0 ? ld_acquire(&sp.lb_flag[j]) : 2u;
+        while (__any_sync(0xffffffffu, f == 0)) {
+          if (++spins > sp.spin_limit) {
+            failed = true;
+            break;
           }
-          const unsigned long long *src = f == 2 ? sp.lb_incl : sp.lb_agg;
-          for (int k = 0; k < 3; k++) ex[k] += src[j * 3 + k];
-          if (f == 2) break;
-          j--;
+          __nanosleep(64);
+          if (f == 0) f = ld_acquire(&sp.lb_flag[j]);
         }
+        if (failed) {
+          if (lane == 0) atomicOr(&sp.ctr->error, 1u);
+          break;
+        }
+        const unsigned incl_mask = __ballot_sync(0xffffffffu, f == 2);
+        const int stop = incl_mask ? __ffs(incl_mask) - 1 : 32;
+        for (int k = 0; k < 3; k++) {
+          unsigned long long v = 0;
+          if (lane < stop) v = sp.lb_agg[j * 3 + k];
+          else if (lane == stop && j >= 0) v = sp.lb_incl[j * 3 + k];
+          ex[k] += warp_sum_u64(v);
+        }
+        if (incl_mask) break;
+        j_hi -= 32;
+      }
+      if (lane == 0) {
         for (int k = 0; k < 3; k++) sp.lb_incl[tile * 3 + k] = ex[k] + mine[k];
         __threadfence();
         st_release(&sp.lb_flag[tile], 2u);
       }
-      for (int k = 0; k < 3; k++) s_excl[k] = ex[k];
     }
-    __syncthreads();
 
-    // 5. emit this tile's rows in line order, one warp per row.
+    // 6. Emit this tile's rows in line order, the whole warp on each row.
     {
-      const unsigned long long row0 = s_excl[0], byte0 = s_excl[1], line0 = s_excl[2];
+      const unsigned long long row0 = ex[0], byte0 = ex[1], line0 = ex[2];
       const unsigned long long nrec = min(tile_rows, sp.rec_cap_per_cta);
-      for (unsigned long long r = warp; r < nrec; r += kThreads / 32) {
+      for (unsigned long long r = 0; r < nrec; r++) {
         const RowRec *rr = (const RowRec *)(my_recs + r * rec_stride);
         const uint32_t *fl = (const uint32_t *)(rr + 1);
         unsigned long long dst_off = byte0 + rr->local_off;
@@ -861,19 +828,15 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
         }
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
 
   // Flush this CTA's counters.
-  auto wsum = [](unsigned long long x) {
-    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
-    return x;
-  };
-  c_lines = wsum(c_lines);
-  c_blank = wsum(c_blank);
-  c_invalid = wsum(c_invalid);
-  c_type = wsum(c_type);
-  c_sel = wsum(c_sel);
+  c_lines = warp_sum_u64(c_lines);
+  c_blank = warp_sum_u64(c_blank);
+  c_invalid = warp_sum_u64(c_invalid);
+  c_type = warp_sum_u64(c_type);
+  c_sel = warp_sum_u64(c_sel);
   if (lane == 0) {
     if (c_lines) atomicAdd(&sp.ctr->n_lines, c_lines);
     if (c_blank) atomicAdd(&sp.ctr->n_blank, c_blank);
@@ -882,7 +845,8 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
     if (c_sel) atomicAdd(&sp.ctr->n_selected, c_sel);
   }
   if (!kRows && P.group_slot < 0 && P.output_kind == 3) {
-    unsigned long long cnt = wsum(agg.count), num = wsum(agg.numeric), ni = wsum(agg.n_int);
+    unsigned long long cnt = warp_sum_u64(agg.count), num = warp_sum_u64(agg.numeric),
+                       ni = warp_sum_u64(agg.n_int);
     // 128-bit sums: reduce the low words with carry counting, per lane pair
     unsigned long long lo = agg.isum_lo, hi = agg.isum_hi;
     for (int d = 16; d > 0; d >>= 1) {
@@ -927,15 +891,15 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
 __global__ void k_reduce_tiles(const double *tile_fsum, unsigned long long n_tiles,
                                double *block_out, const TileDesc *tiles, RunCounters *ctr,
                                unsigned long long *block_lines) {
-  __shared__ double s_f[kThreads];
-  __shared__ unsigned long long s_l[kThreads], s_t[kThreads];
+  __shared__ double s_f[kReduceThreads];
+  __shared__ unsigned long long s_l[kReduceThreads], s_t[kReduceThreads];
   unsigned long long per = (n_tiles + gridDim.x - 1) / gridDim.x;
   unsigned long long b0 = blockIdx.x * per, b1 = min(b0 + per, n_tiles);
   unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
   double f = 0.0;
   unsigned long long lines = 0, lines_t = 0;
   unsigned long long chunk = (b1 > b0 ? b1 - b0 : 0);
-  unsigned long long cper = (chunk + kThreads - 1) / kThreads;
+  unsigned long long cper = (chunk + kReduceThreads - 1) / kReduceThreads;
   unsigned long long c0 = b0 + threadIdx.x * cper, c1 = min(c0 + cper, b1);
   for (unsigned long long t = c0; t < c1; t++) {
     if (tile_fsum) f += tile_fsum[t];
@@ -946,7 +910,7 @@ __global__ void k_reduce_tiles(const double *tile_fsum, unsigned long long n_til
   s_l[threadIdx.x] = lines;
   s_t[threadIdx.x] = lines_t;
   __syncthreads();
-  for (int d = kThreads / 2; d > 0; d >>= 1) {
+  for (int d = kReduceThreads / 2; d > 0; d >>= 1) {
     if (threadIdx.x < d) {
       s_f[threadIdx.x] += s_f[threadIdx.x + d];
       s_l[threadIdx.x] += s_l[threadIdx.x + d];

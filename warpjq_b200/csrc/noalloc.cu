@@ -50,11 +50,11 @@ using namespace wjq;
 namespace {
 
 constexpr uint64_t kNoAllocMaxInput = 4ull << 30;
-constexpr uint32_t kNoAllocTile = 32768;
-constexpr uint32_t kNoAllocHalo = 8192;
+constexpr uint32_t kNoAllocTile = 16384;
+constexpr uint32_t kNoAllocHalo = 2048;
 constexpr uint64_t kNoAllocMaxTiles = kNoAllocMaxInput / kNoAllocTile;
-constexpr uint32_t kNoAllocMaxGrid = 512;
-constexpr uint64_t kNoAllocDeepLevels = 1u << 16;  // per CTA, beyond the 64 in registers
+constexpr uint32_t kNoAllocMaxGrid = 2048;
+constexpr uint64_t kNoAllocDeepLevels = 1u << 14;  // per CTA, beyond the 64 in registers
 constexpr unsigned kNoAllocReduceBlocks = 256;
 
 constexpr uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
@@ -234,7 +234,7 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     sp.spin_limit = 1ull << 24;
     unsigned grid = (unsigned)(n_tiles < s->grid ? n_tiles : s->grid);
     k_scan<false><<<grid, kThreads, s->smem, st>>>(sp);
-    k_reduce_tiles<<<kNoAllocReduceBlocks, kThreads, 0, st>>>(tile_fsum, n_tiles, block_f, tiles, ctr,
+    k_reduce_tiles<<<kNoAllocReduceBlocks, kReduceThreads, 0, st>>>(tile_fsum, n_tiles, block_f, tiles, ctr,
                                                              block_lines);
     k_finalize<<<1, 32, 0, st>>>(block_f, block_lines, kNoAllocReduceBlocks, tiles, ctr, nullptr,
                                  n_tiles, nullptr, 0);
