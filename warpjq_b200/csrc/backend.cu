@@ -66,8 +66,8 @@ struct DevBuf {
 struct RunBufs {
   DevBuf<RunCounters> ctr;
   DevBuf<TileDesc> tiles;
-  DevBuf<unsigned int> lb_flag;
-  DevBuf<unsigned long long> lb_agg, lb_incl;
+  DevBuf<RowTile> row_tiles;
+  DevBuf<unsigned long long> row_bsum;
   DevBuf<uint8_t> recs;
   DevBuf<uint8_t> out;
   DevBuf<unsigned long long> row_off, line_idx;
@@ -92,7 +92,7 @@ struct RunBufs {
   unsigned long long deep_levels = 0;
 
   void release() {
-    ctr.release(); tiles.release(); lb_flag.release(); lb_agg.release(); lb_incl.release();
+    ctr.release(); tiles.release(); row_tiles.release(); row_bsum.release();
     recs.release(); out.release(); row_off.release(); line_idx.release(); tile_fsum.release();
     block_f.release(); block_lines.release(); deep.release(); g_slots.release();
     g_key_off.release(); g_count.release(); g_numeric.release(); g_isum_lo.release();
@@ -104,8 +104,7 @@ struct RunBufs {
 
 constexpr unsigned kReduceBlocks = 256;
 
-__global__ void k_reset_run(RunCounters *ctr, unsigned int *lb_flag, unsigned long long n_tiles,
-                            GroupTable g, uint32_t g_cap, uint32_t key_cap) {
+__global__ void k_reset_run(RunCounters *ctr, GroupTable g, uint32_t g_cap, uint32_t key_cap) {
   unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
   unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   if (tid == 0) {
@@ -118,8 +117,6 @@ __global__ void k_reset_run(RunCounters *ctr, unsigned int *lb_flag, unsigned lo
     z.first_invalid = ~0ull;
     *ctr = z;
   }
-  if (lb_flag)
-    for (unsigned long long i = tid; i < n_tiles; i += stride) lb_flag[i] = 0;
   if (g.slots) {
     for (unsigned long long i = tid; i < g_cap; i += stride) g.slots[i] = 0;
     for (unsigned long long i = tid; i < key_cap; i += stride) {
@@ -223,10 +220,11 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n, char *er
   if (!rb.deep_levels) rb.deep_levels = 1u << 16;
   CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32)), "alloc deep stack");
   if (P.needs_rows) {
-    CK(rb.lb_flag.ensure(n_tiles), "alloc look-back");
-    CK(rb.lb_agg.ensure(n_tiles * 3), "alloc look-back");
-    CK(rb.lb_incl.ensure(n_tiles * 3), "alloc look-back");
-    if (!rb.rec_cap_per_cta) rb.rec_cap_per_cta = std::max<unsigned long long>(c->tile_bytes / 64, 256);
+    CK(rb.row_tiles.ensure(n_tiles), "alloc row tiles");
+    CK(rb.row_bsum.ensure(3 * ((n_tiles + kEmitTiles - 1) / kEmitTiles)), "alloc row prefixes");
+    // Records accumulate over all of a CTA's tiles: start with room for a
+    // row per KiB of input, grown on overflow.
+    if (!rb.rec_cap_per_cta) rb.rec_cap_per_cta = n / 1024 / std::max(1u, c->grid) + 1024;
     CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * P.rec_stride), "alloc records");
     if (!rb.out_cap) rb.out_cap = n + n / 4 + (1u << 20);
     CK(rb.out.ensure(rb.out_cap), "alloc output");
@@ -291,8 +289,7 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
   unsigned long long n_tiles = (n + c->tile_bytes - 1) / c->tile_bytes;
   GroupTable g = group_view(rb, groups);
   s.kernels = 0;
-  k_reset_run<<<256, 256, 0, st>>>(rb.ctr.p, P.needs_rows ? rb.lb_flag.p : nullptr, n_tiles, g,
-                                   groups ? rb.g_cap : 0, groups ? rb.g_key_cap : 0);
+  k_reset_run<<<256, 256, 0, st>>>(rb.ctr.p, g, groups ? rb.g_cap : 0, groups ? rb.g_key_cap : 0);
   s.kernels++;
   CK(cudaGetLastError(), "launch reset");
   if (n > 0) {
@@ -305,21 +302,13 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.n_tiles = n_tiles;
     sp.ctr = rb.ctr.p;
     sp.tiles = rb.tiles.p;
-    sp.lb_flag = rb.lb_flag.p;
-    sp.lb_agg = rb.lb_agg.p;
-    sp.lb_incl = rb.lb_incl.p;
+    sp.row_tiles = rb.row_tiles.p;
     sp.rec_scratch = rb.recs.p;
     sp.rec_cap_per_cta = rb.rec_cap_per_cta;
-    sp.out = rb.out.p;
-    sp.out_cap = rb.out_cap;
-    sp.row_off = rb.row_off.p;
-    sp.line_idx = rb.line_idx.p;
-    sp.rows_cap = rb.rows_cap;
     sp.tile_fsum = rb.tile_fsum.p;
     sp.g = g;
     sp.deep_words = rb.deep.p;
     sp.deep_levels_per_cta = rb.deep_levels;
-    sp.spin_limit = 1ull << 24;
     unsigned grid = (unsigned)std::min<unsigned long long>(c->grid, n_tiles);
     if (!s.scan_t0) {
       CK(cudaEventCreate(&s.scan_t0), "event");
@@ -333,14 +322,37 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     s.kernels++;
     CK(cudaGetLastError(), "launch scan");
     CK(cudaEventRecord(s.scan_t1, st), "event record");
+    if (P.needs_rows) {
+      const unsigned nb = (unsigned)((n_tiles + kEmitTiles - 1) / kEmitTiles);
+      k_rows_block_sums<<<nb, kEmitThreads, 0, st>>>(rb.row_tiles.p, rb.tiles.p, n_tiles,
+                                                      rb.row_bsum.p);
+      k_rows_block_prefix<<<1, kEmitThreads, 0, st>>>(rb.row_bsum.p, nb, rb.ctr.p, rb.row_off.p,
+                                                      rb.rows_cap, rb.out_cap);
+      EmitParams ep{};
+      ep.data = d_data;
+      ep.plan = c->d_plan;
+      ep.row_tiles = rb.row_tiles.p;
+      ep.tiles = rb.tiles.p;
+      ep.n_tiles = n_tiles;
+      ep.block_prefix = rb.row_bsum.p;
+      ep.recs = rb.recs.p;
+      ep.out = rb.out.p;
+      ep.out_cap = rb.out_cap;
+      ep.row_off = rb.row_off.p;
+      ep.line_idx = rb.line_idx.p;
+      ep.rows_cap = rb.rows_cap;
+      ep.ctr = rb.ctr.p;
+      k_rows_emit<<<nb, kEmitThreads, 0, st>>>(ep);
+      s.kernels += 3;
+      CK(cudaGetLastError(), "launch rows");
+    }
     k_reduce_tiles<<<kReduceBlocks, kReduceThreads, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
                                                        n_tiles, rb.block_f.p, rb.tiles.p,
                                                        rb.ctr.p, rb.block_lines.p);
     s.kernels++;
     CK(cudaGetLastError(), "launch reduce");
     k_finalize<<<1, 32, 0, st>>>(rb.block_f.p, rb.block_lines.p, kReduceBlocks, rb.tiles.p,
-                                 rb.ctr.p, P.needs_rows ? rb.lb_incl.p : nullptr, n_tiles,
-                                 P.needs_rows ? rb.row_off.p : nullptr, rb.rows_cap);
+                                 rb.ctr.p);
     s.kernels++;
     CK(cudaGetLastError(), "launch finalize");
   }
@@ -353,8 +365,8 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
 bool grow_after_overflow(warpjq_ctx *c, Slot &s, const RunCounters &h, unsigned long long n) {
   RunBufs &rb = s.rb;
   bool again = false;
-  if (h.overflow & 1u) {  // records per tile
-    rb.rec_cap_per_cta = std::min<unsigned long long>(rb.rec_cap_per_cta * 4, c->tile_bytes);
+  if (h.overflow & 1u) {  // records per CTA
+    rb.rec_cap_per_cta *= 4;
     rb.recs.release();
     again = true;
   }
@@ -404,7 +416,7 @@ warpjq_status run_to_completion(warpjq_ctx *c, Slot &s, const uint8_t *d_data,
        "D2H counters");
     CK(cudaStreamSynchronize(st), "stream sync");
     if (h.error) {
-      set_err(err, err_len, "a device-side wait gave up (look-back did not complete)");
+      set_err(err, err_len, "the scan kernel raised its error flag");
       return WARPJQ_ERR_CUDA;
     }
     if (!h.overflow) return WARPJQ_OK;

@@ -1,22 +1,22 @@
 // The sm_100a scan kernels.
 //
-// One persistent kernel does the whole hot path of the reference's
-// k_nl_count / k_nl_write / k_build_lines / k_eval / DeviceSelect / k_row_len
-// / k_emit chain (warpjq_kernels.cu:1117-1849) in a single pass over the
-// input:
+// The hot path of the reference's k_nl_count / k_nl_write / k_build_lines /
+// k_eval / DeviceSelect / k_row_len / k_emit chain (warpjq_kernels.cu:
+// 1117-1849) as one scan pass plus, for row output, two small passes:
 //
-//   1. A CTA takes the next tile from a work ticket and stages tile + halo
-//      into shared memory with 16-byte loads, recording the newline mask.
-//   2. It lists the lines that start in the tile, in order.
-//   3. Each thread walks one line (walker.cuh), evaluates the filter and
-//      computes the row it will emit, or folds the line into the aggregate.
-//   4. Rows: the tile's row count and byte count are published and the
-//      exclusive prefix over all earlier tiles is obtained by decoupled
-//      look-back (tiles are taken in ticket order, so every earlier tile is
-//      owned by a running CTA); the CTA then writes its rows, in line order,
-//      straight from shared memory to the output.
+//   k_scan      One warp per CTA.  A warp takes the next tile from a work
+//               ticket, stages tile + halo into shared memory with
+//               asynchronous 16-byte copies, marks its newlines, lists the
+//               lines that start in the tile, and walks them one line per
+//               lane (walker.cuh): validation, path resolution, the filter,
+//               and either the aggregate or a compact record per selected
+//               row (line offset, row length, field spans).
+//   k_rows_*    Rows only: block sums and an exclusive prefix over the
+//               per-tile (rows, bytes, lines) totals, then the rows are
+//               copied in line order from the input to the output.
 //
-// No host synchronisation happens inside a run; every wait is bounded.
+// No host synchronisation happens inside a run and no kernel waits on
+// another CTA.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -49,8 +49,7 @@ struct RowRec {
   uint32_t ordinal;               // line index within the tile
   uint32_t local_off;             // row offset within the tile's output
   uint32_t row_len;
-  uint32_t in_window;             // line bytes are in the shared window
-  uint32_t pad;
+  uint32_t pad[2];
   // followed by n_fields x {uint32 off (relative to line), uint32 len|kind<<28|esc<<27}
 };
 static_assert(sizeof(RowRec) == kRowRecBytes, "row record header size");
@@ -74,6 +73,14 @@ struct GroupTable {
   unsigned int *saw_non_numeric;
 };
 
+// Per-tile totals of a rows run.
+struct RowTile {
+  unsigned long long rec_begin;  // the tile's first record in the record arena
+  unsigned long long bytes;      // output bytes of the tile's rows
+  uint32_t rows;
+  uint32_t pad;
+};
+
 struct ScanParams {
   const uint8_t *data;
   unsigned long long n;
@@ -83,41 +90,35 @@ struct ScanParams {
   unsigned long long n_tiles;
   RunCounters *ctr;
   TileDesc *tiles;
-  // look-back state, rows mode: per tile flag + aggregate + inclusive values
-  unsigned int *lb_flag;
-  unsigned long long *lb_agg;   // 3 per tile: rows, bytes, lines
-  unsigned long long *lb_incl;  // 3 per tile
-  // per-CTA record scratch
+  // rows mode: per-tile totals and the record arena (rec_cap_per_cta
+  // records per CTA, appended over all the CTA's tiles)
+  RowTile *row_tiles;
   uint8_t *rec_scratch;
-  unsigned long long rec_cap_per_cta;  // records
-  // outputs
-  uint8_t *out;
-  unsigned long long out_cap;
-  unsigned long long *row_off;    // rows_cap + 1
-  unsigned long long *line_idx;   // rows_cap
-  unsigned long long rows_cap;
+  unsigned long long rec_cap_per_cta;
   // per-tile FP partial sums (fixed-order reduction)
   double *tile_fsum;
   GroupTable g;
   // deep-nesting scratch, per CTA
   uint32_t *deep_words;
   unsigned long long deep_levels_per_cta;
-  unsigned long long spin_limit;
 };
 
-// ---------------------------------------------------------------------------
-// Small block utilities
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
+// Rows emission.
+struct EmitParams {
+  const uint8_t *data;
+  const DevPlan *plan;
+  const RowTile *row_tiles;
+  const TileDesc *tiles;
+  unsigned long long n_tiles;
+  const unsigned long long *block_prefix;  // 3 per block of kEmitTiles tiles
+  const uint8_t *recs;
+  uint8_t *out;
+  unsigned long long out_cap;
+  unsigned long long *row_off;   // rows_cap + 1
+  unsigned long long *line_idx;  // rows_cap
+  unsigned long long rows_cap;
+  RunCounters *ctr;
+};
 
 // ---------------------------------------------------------------------------
 // Group table (open addressing; the key is published with one 64-bit CAS
@@ -424,6 +425,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
   ThreadAgg agg;
   agg.init();
   unsigned long long c_lines = 0, c_blank = 0, c_invalid = 0, c_type = 0, c_sel = 0;
+  unsigned long long cta_recs = 0;  // records this CTA has appended (rows mode)
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
@@ -499,6 +501,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
 
     // 4. Walk the lines, one per lane, in passes of the list's capacity.
     unsigned long long tile_rows = 0, tile_bytes = 0;
+    const unsigned long long tile_rec0 = cta_recs;
     double fsum_lane = 0.0;
     uint32_t tile_first_invalid = 0xFFFFFFFFu, tile_first_type = 0xFFFFFFFFu;
     for (uint32_t base = 0; base < n_lines_tile; base += kMaxLinesPerPass) {
@@ -526,7 +529,6 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
         uint32_t has_row = 0, row_len = 0;
         unsigned long long line_abs = 0;
         uint32_t line_len = 0, ordinal = base + li;
-        bool in_window = true;
         const uint8_t *lp = nullptr;
         bool has_group = false;
         KeyRef gk;
@@ -560,7 +562,6 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             status = walk_window(P, win, s, e, nv);
           } else {
             // longer than the window: walk it from global memory
-            in_window = false;
             unsigned long long q = ts + wlen;
             while (q < sp.n && sp.data[q] != '\n') q++;
             lp = sp.data + line_abs;
@@ -708,7 +709,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           unsigned long long eb, tb;
           warp_scan2(has_row, (unsigned long long)row_len, er, eb, tr, tb);
           if (has_row) {
-            unsigned long long ri = tile_rows + er;
+            unsigned long long ri = cta_recs + er;
             if (ri < sp.rec_cap_per_cta) {
               RowRec *r = (RowRec *)(my_recs + ri * rec_stride);
               r->line_start = line_abs;
@@ -716,7 +717,6 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
               r->ordinal = ordinal;
               r->local_off = (uint32_t)(tile_bytes + eb);
               r->row_len = row_len;
-              r->in_window = in_window;
               uint32_t *fl = (uint32_t *)(r + 1);
               for (uint32_t f = 0; f < nf; f++) {
                 const SlotVal &s = slots[P.output_kind == 1 ? P.out_slot : P.field_slot[f]];
@@ -729,6 +729,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
           }
           tile_rows += tr;
           tile_bytes += tb;
+          cta_recs += tr;
         }
       }
       __syncwarp();
@@ -745,90 +746,22 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
       if (tile_first_invalid != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_invalid_tile, tile);
       if (tile_first_type != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_type_tile, tile);
     }
-    if (!kRows) {
+    if (kRows) {
+      if (lane == 0) {
+        RowTile rt;
+        rt.rec_begin = (unsigned long long)blockIdx.x * sp.rec_cap_per_cta + tile_rec0;
+        rt.bytes = tile_bytes;
+        rt.rows = (uint32_t)tile_rows;
+        rt.pad = 0;
+        sp.row_tiles[tile] = rt;
+      }
+    } else {
       // fixed-order tree over the lanes
       double f = fsum_lane;
 #pragma unroll
       for (int d = 16; d > 0; d >>= 1) f += __shfl_down_sync(0xffffffffu, f, d);
       if (lane == 0) sp.tile_fsum[tile] = f;
-      continue;
     }
-
-    // 5. Look-back for this tile's row / byte / line prefix, 32 earlier
-    //    tiles per step (lane l reads tile j_hi - l).
-    const unsigned long long mine[3] = {tile_rows, tile_bytes, (unsigned long long)n_lines_tile};
-    unsigned long long ex[3] = {0, 0, 0};
-    if (tile == 0) {
-      if (lane == 0) {
-        for (int k = 0; k < 3; k++) sp.lb_incl[k] = mine[k];
-        __threadfence();
-        st_release(&sp.lb_flag[0], 2u);
-      }
-    } else {
-      if (lane == 0) {
-        for (int k = 0; k < 3; k++) sp.lb_agg[tile * 3 + k] = mine[k];
-        __threadfence();
-        st_release(&sp.lb_flag[tile], 1u);
-      }
-      long long j_hi = (long long)tile - 1;
-      unsigned long long spins = 0;
-      bool failed = false;
-      for (;;) {
-        const long long j = j_hi - lane;
-        unsigned f = j >= 0 ? ld_acquire(&sp.lb_flag[j]) : 2u;
-        while (__any_sync(0xffffffffu, f == 0)) {
-          if (++spins > sp.spin_limit) {
-            failed = true;
-            break;
-          }
-          __nanosleep(64);
-          if (f == 0) f = ld_acquire(&sp.lb_flag[j]);
-        }
-        if (failed) {
-          if (lane == 0) atomicOr(&sp.ctr->error, 1u);
-          break;
-        }
-        const unsigned incl_mask = __ballot_sync(0xffffffffu, f == 2);
-        const int stop = incl_mask ? __ffs(incl_mask) - 1 : 32;
-        for (int k = 0; k < 3; k++) {
-          unsigned long long v = 0;
-          if (lane < stop) v = sp.lb_agg[j * 3 + k];
-          else if (lane == stop && j >= 0) v = sp.lb_incl[j * 3 + k];
-          ex[k] += warp_sum_u64(v);
-        }
-        if (incl_mask) break;
-        j_hi -= 32;
-      }
-      if (lane == 0) {
-        for (int k = 0; k < 3; k++) sp.lb_incl[tile * 3 + k] = ex[k] + mine[k];
-        __threadfence();
-        st_release(&sp.lb_flag[tile], 2u);
-      }
-    }
-
-    // 6. Emit this tile's rows in line order, the whole warp on each row.
-    {
-      const unsigned long long row0 = ex[0], byte0 = ex[1], line0 = ex[2];
-      const unsigned long long nrec = min(tile_rows, sp.rec_cap_per_cta);
-      for (unsigned long long r = 0; r < nrec; r++) {
-        const RowRec *rr = (const RowRec *)(my_recs + r * rec_stride);
-        const uint32_t *fl = (const uint32_t *)(rr + 1);
-        unsigned long long dst_off = byte0 + rr->local_off;
-        unsigned long long ri = row0 + r;
-        if (dst_off + rr->row_len > sp.out_cap || ri >= sp.rows_cap) {
-          if (lane == 0) atomicOr(&sp.ctr->overflow, 2u);
-          continue;
-        }
-        const uint8_t *line =
-            rr->in_window ? win + (uint32_t)(rr->line_start - ts) : sp.data + rr->line_start;
-        emit_row(P, line, *rr, fl, sp.out + dst_off, lane);
-        if (lane == 0) {
-          sp.row_off[ri] = dst_off;
-          sp.line_idx[ri] = line0 + rr->ordinal;
-        }
-      }
-    }
-    __syncwarp();
   }
 
   // Flush this CTA's counters.
@@ -926,9 +859,7 @@ __global__ void k_reduce_tiles(const double *tile_fsum, unsigned long long n_til
 }
 
 __global__ void k_finalize(const double *block_f, const unsigned long long *block_lines,
-                           unsigned nblocks, const TileDesc *tiles, RunCounters *ctr,
-                           const unsigned long long *lb_incl, unsigned long long n_tiles,
-                           unsigned long long *row_off, unsigned long long rows_cap) {
+                           unsigned nblocks, const TileDesc *tiles, RunCounters *ctr) {
   if (threadIdx.x != 0) return;
   double f = 0.0;
   unsigned long long lines = 0, lines_t = 0;
@@ -941,12 +872,142 @@ __global__ void k_finalize(const double *block_f, const unsigned long long *bloc
   unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
   ctr->first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
   ctr->first_type_error = cut_t == ~0ull ? ~0ull : lines_t + tiles[cut_t].first_type_error;
-  if (row_off && n_tiles > 0) {
-    // The last tile's inclusive prefix holds the totals.
-    unsigned long long rows = lb_incl[(n_tiles - 1) * 3 + 0];
-    unsigned long long bytes = lb_incl[(n_tiles - 1) * 3 + 1];
-    ctr->out_len = bytes;
-    if (rows <= rows_cap) row_off[rows] = bytes;
+}
+
+// ---------------------------------------------------------------------------
+// Rows: prefix over the per-tile totals, then emission in line order.
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t kEmitTiles = 1024;  // tiles per block of the rows passes
+constexpr int kEmitThreads = 256;
+
+// Exclusive block scan of three u64 values in thread order, with totals.
+__device__ __forceinline__ void block_scan3(const unsigned long long v[3], unsigned long long ex[3],
+                                            unsigned long long tot[3],
+                                            unsigned long long (*s_w)[kEmitThreads / 32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long inc[3] = {v[0], v[1], v[2]};
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      unsigned long long x = __shfl_up_sync(0xffffffffu, inc[k], d);
+      if (lane >= d) inc[k] += x;
+    }
+  }
+  if (lane == 31)
+    for (int k = 0; k < 3; k++) s_w[k][warp] = inc[k];
+  __syncthreads();
+  for (int k = 0; k < 3; k++) {
+    unsigned long long before = 0, all = 0;
+    for (int w = 0; w < kEmitThreads / 32; w++) {
+      if (w < warp) before += s_w[k][w];
+      all += s_w[k][w];
+    }
+    ex[k] = before + inc[k] - v[k];
+    tot[k] = all;
+  }
+  __syncthreads();
+}
+
+// Pass 1: (rows, bytes, lines) summed per block of kEmitTiles tiles.
+__global__ void __launch_bounds__(kEmitThreads)
+    k_rows_block_sums(const RowTile *rt, const TileDesc *td, unsigned long long n_tiles,
+                      unsigned long long *bsum) {
+  __shared__ unsigned long long s_w[3][kEmitThreads / 32];
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * kEmitTiles;
+  unsigned long long v[3] = {0, 0, 0};
+  for (uint32_t k = threadIdx.x; k < kEmitTiles; k += kEmitThreads) {
+    unsigned long long t = t0 + k;
+    if (t < n_tiles) {
+      v[0] += rt[t].rows;
+      v[1] += rt[t].bytes;
+      v[2] += td[t].n_lines;
+    }
+  }
+  unsigned long long ex[3], tot[3];
+  block_scan3(v, ex, tot, s_w);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) bsum[blockIdx.x * 3 + k] = tot[k];
+}
+
+// Pass 2 (one block): block sums -> exclusive block prefixes, in place; the
+// totals give the output length and the closing row offset.  Output that
+// does not fit raises the overflow flag (the run is repeated with room).
+__global__ void __launch_bounds__(kEmitThreads)
+    k_rows_block_prefix(unsigned long long *bsum, unsigned nblocks, RunCounters *ctr,
+                        unsigned long long *row_off, unsigned long long rows_cap,
+                        unsigned long long out_cap) {
+  __shared__ unsigned long long s_w[3][kEmitThreads / 32];
+  const unsigned per = (nblocks + kEmitThreads - 1) / kEmitThreads;
+  const unsigned b0 = threadIdx.x * per, b1 = min(b0 + per, nblocks);
+  unsigned long long v[3] = {0, 0, 0};
+  for (unsigned b = b0; b < b1; b++)
+    for (int k = 0; k < 3; k++) v[k] += bsum[b * 3 + k];
+  unsigned long long ex[3], tot[3];
+  block_scan3(v, ex, tot, s_w);
+  for (unsigned b = b0; b < b1; b++)
+    for (int k = 0; k < 3; k++) {
+      unsigned long long x = bsum[b * 3 + k];
+      bsum[b * 3 + k] = ex[k];
+      ex[k] += x;
+    }
+  if (threadIdx.x == 0) {
+    ctr->out_len = tot[1];
+    if (tot[0] > rows_cap || tot[1] > out_cap) atomicOr(&ctr->overflow, 2u);
+    else row_off[tot[0]] = tot[1];
+  }
+}
+
+// Pass 3: each block takes its kEmitTiles tiles kEmitThreads at a time:
+// per-tile prefixes by a block scan, then each warp copies whole tiles'
+// rows, one row at a time, from the input to the output.
+__global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
+  __shared__ unsigned long long s_w[3][kEmitThreads / 32];
+  __shared__ unsigned long long s_pre[3][kEmitThreads];
+  __shared__ unsigned long long s_rec[kEmitThreads];
+  __shared__ uint32_t s_rows[kEmitThreads];
+  if (ep.ctr->overflow & 3u) return;  // the run is repeated with bigger buffers
+  const DevPlan &P = *ep.plan;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t rec_stride = P.rec_stride;
+  unsigned long long carry[3];
+  for (int k = 0; k < 3; k++) carry[k] = ep.block_prefix[blockIdx.x * 3 + k];
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * kEmitTiles;
+  for (uint32_t sub = 0; sub < kEmitTiles; sub += kEmitThreads) {
+    if (t0 + sub >= ep.n_tiles) break;
+    const unsigned long long t = t0 + sub + threadIdx.x;
+    unsigned long long v[3] = {0, 0, 0};
+    unsigned long long rec = 0;
+    if (t < ep.n_tiles) {
+      const RowTile rt = ep.row_tiles[t];
+      v[0] = rt.rows;
+      v[1] = rt.bytes;
+      v[2] = ep.tiles[t].n_lines;
+      rec = rt.rec_begin;
+    }
+    unsigned long long ex[3], tot[3];
+    block_scan3(v, ex, tot, s_w);
+    for (int k = 0; k < 3; k++) s_pre[k][threadIdx.x] = carry[k] + ex[k];
+    s_rec[threadIdx.x] = rec;
+    s_rows[threadIdx.x] = (uint32_t)v[0];
+    __syncthreads();
+    for (int i = warp; i < kEmitThreads; i += kEmitThreads / 32) {
+      const uint32_t rows = s_rows[i];
+      const unsigned long long row0 = s_pre[0][i], byte0 = s_pre[1][i], line0 = s_pre[2][i];
+      for (uint32_t r = 0; r < rows; r++) {
+        const RowRec *rr = (const RowRec *)(ep.recs + (s_rec[i] + r) * rec_stride);
+        const uint32_t *fl = (const uint32_t *)(rr + 1);
+        const unsigned long long dst_off = byte0 + rr->local_off;
+        emit_row(P, ep.data + rr->line_start, *rr, fl, ep.out + dst_off, lane);
+        if (lane == 0) {
+          ep.row_off[row0 + r] = dst_off;
+          ep.line_idx[row0 + r] = line0 + rr->ordinal;
+        }
+      }
+    }
+    for (int k = 0; k < 3; k++) carry[k] += tot[k];
+    __syncthreads();
   }
 }
 

@@ -231,13 +231,11 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     sp.tile_fsum = tile_fsum;
     sp.deep_words = deep;
     sp.deep_levels_per_cta = kNoAllocDeepLevels;
-    sp.spin_limit = 1ull << 24;
     unsigned grid = (unsigned)(n_tiles < s->grid ? n_tiles : s->grid);
     k_scan<false><<<grid, kThreads, s->smem, st>>>(sp);
-    k_reduce_tiles<<<kNoAllocReduceBlocks, kReduceThreads, 0, st>>>(tile_fsum, n_tiles, block_f, tiles, ctr,
-                                                             block_lines);
-    k_finalize<<<1, 32, 0, st>>>(block_f, block_lines, kNoAllocReduceBlocks, tiles, ctr, nullptr,
-                                 n_tiles, nullptr, 0);
+    k_reduce_tiles<<<kNoAllocReduceBlocks, kReduceThreads, 0, st>>>(tile_fsum, n_tiles, block_f,
+                                                                    tiles, ctr, block_lines);
+    k_finalize<<<1, 32, 0, st>>>(block_f, block_lines, kNoAllocReduceBlocks, tiles, ctr);
   }
   k_noalloc_result<<<1, 32, 0, st>>>(ctr, d_result);
   e = cudaGetLastError();
