@@ -436,6 +436,20 @@ __device__ __noinline__ double slow_decimal_to_double(const uint8_t *p, uint32_t
 // holds its exact value.
 __device__ __forceinline__ double parse_number(const uint8_t *p, uint32_t n, bool &is_int,
                                                long long &iv) {
+  if (n <= 9) {  // short non-negative integers: exact in 32 bits
+    uint32_t v = 0;
+    uint32_t k = 0;
+    for (; k < n; k++) {
+      uint32_t dgt = (uint32_t)p[k] - '0';
+      if (dgt > 9) break;
+      v = v * 10 + dgt;
+    }
+    if (k == n) {
+      is_int = true;
+      iv = (long long)v;
+      return (double)v;
+    }
+  }
   bool neg = p[0] == '-';
   uint32_t i = neg ? 1 : 0;
   unsigned long long mant = 0;

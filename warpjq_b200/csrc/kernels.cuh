@@ -31,6 +31,7 @@ namespace wjq {
 constexpr int kThreads = 32;                 // one warp per CTA; each warp owns its tile
 constexpr uint32_t kMaxLinesPerPass = 512;   // line-start list capacity per pass
 constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
+constexpr int kScanBlocksPerSM = 24;         // register budget of k_scan: 24 warps per SM
 
 // Dynamic shared memory of k_scan for tile T and halo H (the layout is at the
 // top of k_scan).
@@ -399,8 +400,40 @@ __device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uin
   tb = __shfl_sync(0xffffffffu, ib, 31);
 }
 
+// Natural-order newline mask of window chunk c (bytes 32c .. 32c+31); bytes
+// at or past `wlen` do not count.  A cheap has-a-newline test runs first;
+// the exact per-byte flags are worked out only for chunks holding one.
+__device__ __forceinline__ uint32_t chunk_newlines(const uint8_t *win, uint32_t c, uint32_t wlen) {
+  const uint4 a = ((const uint4 *)win)[2 * c];
+  const uint4 b = ((const uint4 *)win)[2 * c + 1];
+  const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  uint32_t any = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    uint32_t t = w[k] ^ 0x0A0A0A0Au;
+    any |= (t - 0x01010101u) & ~t;  // nonzero iff a byte of t is zero (flags above it may be spurious)
+  }
+  if (!(any & 0x80808080u)) return 0;
+  // Exact flags, gathered in a permuted order (bit 8j+k = byte 4k+j), then
+  // put in byte order.
+  uint32_t nl = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    uint32_t t = w[k] ^ 0x0A0A0A0Au;
+    nl |= (~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u) >> (7 - k);
+  }
+  uint32_t nat = 0;
+  while (nl) {
+    uint32_t bit = (uint32_t)__ffs(nl) - 1u;
+    nl &= nl - 1u;
+    nat |= 1u << (((bit & 7u) << 2) | (bit >> 3));
+  }
+  if (wlen - c * 32 < 32) nat &= (1u << (wlen - c * 32)) - 1u;
+  return nat;
+}
+
 template <bool kRows>
-__global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
+__global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams sp) {
   extern __shared__ __align__(16) uint8_t smem[];
   const DevPlan &P = *sp.plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
@@ -429,11 +462,14 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
+  // Tickets are taken one tile ahead, so the atomic's latency overlaps a
+  // tile's work.
+  unsigned long long next_ticket = 0;
+  if (lane == 0) next_ticket = atomicAdd(&sp.ctr->next_tile, 1ull);
   for (;;) {
-    unsigned long long tile = 0;
-    if (lane == 0) tile = atomicAdd(&sp.ctr->next_tile, 1ull);
-    tile = __shfl_sync(0xffffffffu, tile, 0);
+    const unsigned long long tile = __shfl_sync(0xffffffffu, next_ticket, 0);
     if (tile >= sp.n_tiles) break;
+    if (lane == 0) next_ticket = atomicAdd(&sp.ctr->next_tile, 1ull);
     const unsigned long long ts = tile * T;
     const unsigned long long te = min(ts + T, sp.n);
     const uint32_t tlen = (uint32_t)(te - ts);
@@ -448,51 +484,36 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
     cp_async_wait_all();
     __syncwarp();
 
-    // 2. Newline masks per 32-byte chunk.  The flags of the eight words
-    //    are gathered in a permuted order (bit 8j+k = byte 4k+j), one shift
-    //    per word, and put in byte order only for chunks holding one.
-    const uint32_t nchunks = (wlen + 31) >> 5;
-    for (uint32_t c = lane; c < nchunks; c += 32) {
-      const uint4 a = ((const uint4 *)win)[2 * c];
-      const uint4 b = ((const uint4 *)win)[2 * c + 1];
-      const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-      uint32_t nl = 0;
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        uint32_t t = w[k] ^ 0x0A0A0A0Au;
-        nl |= (~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u) >> (7 - k);
-      }
-      if (nl) {
-        uint32_t nat = 0;
-        while (nl) {
-          uint32_t bit = (uint32_t)__ffs(nl) - 1u;
-          nl &= nl - 1u;
-          nat |= 1u << (((bit & 7u) << 2) | (bit >> 3));
-        }
-        nl = nat;
-        if (wlen - c * 32 < 32) nl &= (1u << (wlen - c * 32)) - 1u;  // bytes past the data
-      }
-      nlmask[c] = nl;
-    }
-    if (lane == 0) {
-      nlmask[nchunks] = 0;
-      // A '\n' after the last byte ends the last line for the walker.
-      if (win_reaches_end) win[wlen] = '\n';
-    }
-    __syncwarp();
+    if (lane == 0 && win_reaches_end) win[wlen] = '\n';  // ends the last line for the walker
 
-    // 3. Lines starting in the tile: ts itself (after a newline) and q+1 for
-    //    every newline q in [ts, te-1).
-    const uint32_t nl_limit = tlen ? tlen - 1 : 0;
-    auto nl_bits = [&](uint32_t c) -> uint32_t {
-      uint32_t base = c * 32;
+    // 2. Newline masks of the tile's chunks (lane l owns [l*K, l*K + K)),
+    //    counted as they are made; chunks past the tile are classified only
+    //    when the tile's last line is looked for there.
+    const uint32_t nchunks = (wlen + 31) >> 5;
+    const uint32_t tchunks = (tlen + 31) >> 5;
+    const uint32_t nl_limit = tlen ? tlen - 1 : 0;  // newlines below this start a line in the tile
+    auto listed = [&](uint32_t c, uint32_t m) -> uint32_t {
+      const uint32_t base = c * 32;
       if (base >= nl_limit) return 0u;
-      uint32_t m = nlmask[c];
       if (nl_limit - base < 32) m &= (1u << (nl_limit - base)) - 1u;
       return m;
     };
     uint32_t my_nl = 0;
-    for (uint32_t k = 0; k < K; k++) my_nl += __popc(nl_bits(c0 + k));
+    unsigned long long nz = 0;  // bit k: chunk c0 + k lists a line start
+    for (uint32_t k = 0; k < K; k++) {
+      const uint32_t c = c0 + k;
+      if (c >= tchunks) break;
+      const uint32_t m = chunk_newlines(win, c, wlen);
+      nlmask[c] = m;
+      const uint32_t lm = listed(c, m);
+      if (lm) {
+        my_nl += __popc(lm);
+        nz |= 1ull << k;
+      }
+    }
+
+    // 3. Lines starting in the tile: ts itself (after a newline) and q+1 for
+    //    every newline q in [ts, te-1).
     uint32_t first_nl, tot_nl;
     unsigned long long dummy_e, dummy_t;
     warp_scan2(my_nl, 0ull, first_nl, dummy_e, tot_nl, dummy_t);
@@ -511,8 +532,9 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
       {
         uint32_t idx = first_nl + lead;
         if (my_nl && idx <= base + cnt && idx + my_nl > base) {
-          for (uint32_t k = 0; k < K; k++) {
-            uint32_t m = nl_bits(c0 + k);
+          for (unsigned long long z = nz; z; z &= z - 1) {
+            const uint32_t k = (uint32_t)__ffsll((long long)z) - 1u;
+            uint32_t m = listed(c0 + k, nlmask[c0 + k]);
             while (m) {
               uint32_t b = (c0 + k) * 32 + (uint32_t)__ffs(m) - 1;
               m &= m - 1;
@@ -548,8 +570,9 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanParams sp) {
             uint32_t q = tlen ? tlen - 1 : 0;
             if (q < s) q = s;
             uint32_t c = q >> 5;
-            uint32_t m = nlmask[c] & (0xFFFFFFFFu << (q & 31));
-            while (!m && ++c < nchunks) m = nlmask[c];
+            uint32_t m = (c < tchunks ? nlmask[c] : chunk_newlines(win, c, wlen)) &
+                         (0xFFFFFFFFu << (q & 31));
+            while (!m && ++c < nchunks) m = c < tchunks ? nlmask[c] : chunk_newlines(win, c, wlen);
             q = m ? c * 32 + (uint32_t)__ffs(m) - 1 : wlen;
             if (q < wlen) e = q;
             else if (win_reaches_end) e = wlen;

@@ -34,6 +34,9 @@ enum JKind : uint8_t {
 };
 
 struct PlanNode {
+  // Bit L set when a key child's key is L bytes long (bit 63: 63 or more);
+  // a key of any other length cannot match and is skipped without compare.
+  unsigned long long key_len_mask;
   uint32_t index;        // array index, for an index step
   uint16_t key_off;      // decoded key bytes in blob, for a key step
   uint16_t key_len;
@@ -120,7 +123,7 @@ struct RunCounters {
   // group table
   unsigned int n_keys;
   unsigned int overflow;     // bit0 records, bit1 output, bit2 groups, bit3 deep stack
-  unsigned int error;        // nonzero: a bounded wait gave up (device state suspect)
+  unsigned int error;        // nonzero: a kernel found its own state inconsistent
   double fsum_total;         // written by the finalize kernel
   unsigned long long first_invalid;     // written by the finalize kernel
   unsigned long long first_type_error;  // written by the finalize kernel

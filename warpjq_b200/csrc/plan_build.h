@@ -137,10 +137,15 @@ inline warpjq_status build_plan(const warpjq_program *p, DevPlan &P, char *err, 
     d.next_sibling = kNoNode;
     d.subtree_end = (uint8_t)subtree_end[order[i]];
     d.key_first = (!x.is_index && x.key_len) ? p->blob[x.key_off] : 0;
+    d.key_len_mask = 0;
     for (size_t k = 0; k < x.kids.size(); k++) {
       const TmpNode &c = tn[x.kids[k]];
-      if (c.is_index) d.has_index_children = 1;
-      else d.has_key_children = 1;
+      if (c.is_index) {
+        d.has_index_children = 1;
+      } else {
+        d.has_key_children = 1;
+        d.key_len_mask |= 1ull << (c.key_len < 63 ? c.key_len : 63);
+      }
     }
   }
   // Sibling links last: filling a node above resets its own link.

@@ -346,14 +346,19 @@ __device__ __forceinline__ uint32_t str_special(uint32_t x) {
          0x80808080u;
 }
 
-// Number of ASCII digits starting at w[j].
-__device__ __forceinline__ uint32_t digit_run(const uint8_t *w, uint32_t j) {
+// Number of ASCII digits starting at w[j]; `term` receives the byte after
+// them.
+__device__ __forceinline__ uint32_t digit_run(const uint8_t *w, uint32_t j, uint32_t &term) {
   uint32_t n = 0;
   for (;;) {
     uint32_t x = load4(w, j + n);
     // a byte is a digit when its high nibble is 3 and its low nibble is <= 9
     uint32_t nd = ((x & 0xF0F0F0F0u) ^ 0x30303030u) | (((x & 0x0F0F0F0Fu) + 0x06060606u) & 0x10101010u);
-    if (nd) return n + (((uint32_t)__ffs(nd) - 1u) >> 3);
+    if (nd) {
+      const uint32_t sh = ((uint32_t)__ffs(nd) - 1u) & ~7u;
+      term = (x >> sh) & 0xFFu;
+      return n + (sh >> 3);
+    }
     n += 4;
   }
 }
@@ -365,44 +370,59 @@ __device__ __forceinline__ bool simple_escape(uint32_t e) {
 
 // Closing quote of the string opened at w[i], or 0 when the string is
 // malformed (a bad escape, a raw control byte) or reaches the newline.
-// `esc` reports whether the body holds a backslash.
+// `esc` reports whether the body holds a backslash.  Ordinary bytes are
+// skipped four at a time up to a 16-byte boundary, then 32 at a time; the
+// byte that stops a step is taken from the loaded word.
 __device__ __forceinline__ uint32_t win_string(const uint8_t *w, uint32_t i, bool &esc) {
   uint32_t p = i + 1;
   esc = false;
   for (;;) {
     uint32_t wa = p & ~3u;
-    uint32_t f = str_special(*(const uint32_t *)(w + wa)) & (0xFFFFFFFFu << ((p & 3u) * 8u));
+    uint32_t x = *(const uint32_t *)(w + wa);
+    uint32_t f = str_special(x) & (0xFFFFFFFFu << ((p & 3u) * 8u));
     if (!f) {
       wa += 4;
       while (wa & 15u) {
-        f = str_special(*(const uint32_t *)(w + wa));
+        x = *(const uint32_t *)(w + wa);
+        f = str_special(x);
         if (f) break;
         wa += 4;
       }
       while (!f) {
-        uint4 x = *(const uint4 *)(w + wa);
-        uint32_t f0 = str_special(x.x), f1 = str_special(x.y), f2 = str_special(x.z),
-                 f3 = str_special(x.w);
+        const uint4 u = *(const uint4 *)(w + wa);
+        const uint4 v = *(const uint4 *)(w + wa + 16);
+        const uint32_t f0 = str_special(u.x), f1 = str_special(u.y), f2 = str_special(u.z),
+                       f3 = str_special(u.w);
+        const uint32_t f4 = str_special(v.x), f5 = str_special(v.y), f6 = str_special(v.z),
+                       f7 = str_special(v.w);
         if (f0 | f1 | f2 | f3) {
           if (f0) {
-            f = f0;
+            f = f0; x = u.x;
           } else if (f1) {
-            f = f1;
-            wa += 4;
+            f = f1; x = u.y; wa += 4;
           } else if (f2) {
-            f = f2;
-            wa += 8;
+            f = f2; x = u.z; wa += 8;
           } else {
-            f = f3;
-            wa += 12;
+            f = f3; x = u.w; wa += 12;
+          }
+        } else if (f4 | f5 | f6 | f7) {
+          if (f4) {
+            f = f4; x = v.x; wa += 16;
+          } else if (f5) {
+            f = f5; x = v.y; wa += 20;
+          } else if (f6) {
+            f = f6; x = v.z; wa += 24;
+          } else {
+            f = f7; x = v.w; wa += 28;
           }
         } else {
-          wa += 16;
+          wa += 32;
         }
       }
     }
-    p = wa + (((uint32_t)__ffs(f) - 1u) >> 3);
-    uint32_t c = w[p];
+    const uint32_t sh = ((uint32_t)__ffs(f) - 1u) & ~7u;
+    p = wa + (sh >> 3);
+    const uint32_t c = (x >> sh) & 0xFFu;
     if (c == '"') return p;
     if (c == '\\') {
       esc = true;
@@ -433,20 +453,19 @@ __device__ __forceinline__ uint32_t win_atom(const uint8_t *w, uint32_t i, uint3
   uint32_t j = i;
   if (c == '-') c = w[++j];
   if (c - '0' >= 10u) return 0;
-  uint32_t d = digit_run(w, j);
+  uint32_t t;
+  uint32_t d = digit_run(w, j, t);
   if (c == '0' && d > 1) return 0;
   j += d;
-  c = w[j];
-  if (c == '.') {
-    d = digit_run(w, j + 1);
+  if (t == '.') {
+    d = digit_run(w, j + 1, t);
     if (!d) return 0;
     j += 1 + d;
-    c = w[j];
   }
-  if ((c | 0x20u) == 'e') {
-    c = w[++j];
-    if (c == '+' || c == '-') j++;
-    d = digit_run(w, j);
+  if ((t | 0x20u) == 'e') {
+    uint32_t sgn = w[++j];
+    if (sgn == '+' || sgn == '-') j++;
+    d = digit_run(w, j, t);
     if (!d) return 0;
     j += d;
   }
@@ -456,7 +475,7 @@ __device__ __forceinline__ uint32_t win_atom(const uint8_t *w, uint32_t i, uint3
 }  // namespace detail
 
 // Walks the line w[s, e) of a window.  w must be 4-byte aligned, w[e] must
-// be '\n' and the 16 bytes after it readable.  Offsets recorded in `v` are
+// be '\n' and the 32 bytes after it readable.  Offsets recorded in `v` are
 // relative to s.  Lines nesting past 64 levels return LS_DEEP.
 __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, uint32_t s,
                                            uint32_t e, NodeVals &v) {
@@ -482,6 +501,7 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
   uint64_t arrs = 0;  // bit d: the container open at depth d is an array
   uint32_t depth = 0;
   uint32_t cur = kNoNode, idx = 0;  // trie node and element index of the innermost container
+  unsigned long long cur_lm = 0;    // key_len_mask of cur (0: no key is looked up)
   uint8_t stk_node[kMaxDepthFast];
   uint32_t stk_idx[kMaxDepthFast];
   uint32_t vn = n_nodes ? 0u : kNoNode;  // node the next value lands on
@@ -491,19 +511,24 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
     if (want_key) {
       if (c != '"') return LS_INVALID;
       bool esc;
-      uint32_t q = win_string(w, i, esc);
+      const uint32_t q = win_string(w, i, esc);
       if (!q) return LS_INVALID;
       vn = kNoNode;
-      if (cur != kNoNode && P.nodes[cur].has_key_children)
-        vn = match_key(P, (uint8_t)cur, w + i + 1, q - i - 1, esc);
-      i = q + 1;
-      c = w[i];
-      if (c != ':') {
-        if (!is_ws3(c)) return LS_INVALID;
-        i = skip_ws3(w, i);
-        if (w[i] != ':') return LS_INVALID;
+      if (cur_lm) {
+        const uint32_t kl = q - i - 1;
+        if (esc || ((cur_lm >> (kl < 63u ? kl : 63u)) & 1ull))
+          vn = match_key(P, (uint8_t)cur, w + i + 1, kl, esc);
       }
-      c = w[++i];
+      // ':' and the value's first byte, usually in one read
+      const uint32_t la = load4(w, q + 1);
+      if ((la & 0xFFu) == ':') {
+        i = q + 2;
+        c = (la >> 8) & 0xFFu;
+      } else {
+        i = skip_ws3(w, q + 1);
+        if (w[i] != ':') return LS_INVALID;
+        c = w[++i];
+      }
       if (is_ws3(c)) {
         i = skip_ws3(w, i);
         c = w[i];
@@ -526,6 +551,7 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
       depth++;
       cur = vn;
       idx = 0;
+      cur_lm = (!arr && vn != kNoNode) ? P.nodes[vn].key_len_mask : 0ull;
       c = w[++i];
       if (is_ws3(c)) {
         i = skip_ws3(w, i);
@@ -551,18 +577,22 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
       }
       if (vn != kNoNode) v.len[vn] = j - i;
       i = j;
-      c = w[i];
+    }
+    // After a value: commas and closing brackets, with the next bytes read
+    // four at a time.
+    uint32_t la = load4(w, i);
+    for (;;) {
+      c = la & 0xFFu;
       if (is_ws3(c)) {
         i = skip_ws3(w, i);
-        c = w[i];
+        la = load4(w, i);
+        c = la & 0xFFu;
       }
-    }
-    // After a value: commas and closing brackets.
-    for (;;) {
       if (depth == 0) return c == '\n' ? LS_OK : LS_INVALID;
       const bool arr = (arrs >> (depth - 1)) & 1;
       if (c == ',') {
-        c = w[++i];
+        i++;
+        c = (la >> 8) & 0xFFu;
         if (is_ws3(c)) {
           i = skip_ws3(w, i);
           c = w[i];
@@ -579,11 +609,10 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
       depth--;
       cur = stk_node[depth];
       idx = stk_idx[depth];
-      c = w[++i];
-      if (is_ws3(c)) {
-        i = skip_ws3(w, i);
-        c = w[i];
-      }
+      const bool parent_obj = depth > 0 && !((arrs >> (depth - 1)) & 1);
+      cur_lm = (parent_obj && cur != kNoNode) ? P.nodes[cur].key_len_mask : 0ull;
+      i++;
+      la = load4(w, i);
     }
   }
 }
