@@ -98,6 +98,19 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
 warpjq_status warpjq_slot_first_errors(warpjq_ctx *ctx, uint32_t slot, uint64_t *first_invalid,
                                        uint64_t *first_type_error);
 
+/* warpjq_submit with the chunk copied to the device straight from `src`
+ * (n_bytes <= the slot capacity) instead of from the slot's pinned buffer.
+ * For host memory that is already page-locked (cudaHostAlloc'd or
+ * registered), this skips the staging copy; `src` must stay valid and
+ * unmodified until warpjq_wait on this slot returns.  Errors as
+ * warpjq_submit.  No reference counterpart. */
+warpjq_status warpjq_submit_host(warpjq_ctx *ctx, uint32_t slot, const uint8_t *src,
+                                 uint64_t n_bytes, char *err, size_t err_len);
+
+/* 1 when `p` points into page-locked host memory the device can read by DMA,
+ * else 0.  No reference counterpart. */
+int warpjq_host_is_pinned(const void *p);
+
 /* Device-resident scan tunables: bytes per tile (one warp walks the lines
  * starting in a tile, one line per lane) and the halo staged after it (a line
  * that runs past tile + halo is walked from global memory, more slowly).

@@ -34,7 +34,7 @@ ABI_SYMBOLS = [
 ]
 EXT_SYMBOLS = [
     "warpjq_launch_device", "warpjq_collect_device", "warpjq_slot_first_errors",
-    "warpjq_set_tiling", "warpjq_autotile",
+    "warpjq_set_tiling", "warpjq_autotile", "warpjq_submit_host", "warpjq_host_is_pinned",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",

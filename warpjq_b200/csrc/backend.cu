@@ -76,12 +76,9 @@ struct RunBufs {
   DevBuf<unsigned long long> block_lines;
   DevBuf<uint32_t> deep;
   // group table
-  DevBuf<unsigned long long> g_slots, g_key_off, g_count, g_numeric, g_isum_lo, g_isum_hi, g_n_int,
-      g_min, g_max;
-  DevBuf<uint32_t> g_key_len;
-  DevBuf<uint8_t> g_key_kind, g_key_esc;
-  DevBuf<double> g_fsum;
-  DevBuf<unsigned int> g_saw;
+  DevBuf<unsigned long long> g_slots;
+  DevBuf<GroupKeyDesc> g_keys;
+  DevBuf<GroupAcc> g_acc;
 
   // current capacities
   unsigned long long rec_cap_per_cta = 0;
@@ -95,10 +92,7 @@ struct RunBufs {
     ctr.release(); tiles.release(); row_tiles.release(); row_bsum.release();
     recs.release(); out.release(); row_off.release(); line_idx.release(); tile_fsum.release();
     block_f.release(); block_lines.release(); deep.release(); g_slots.release();
-    g_key_off.release(); g_count.release(); g_numeric.release(); g_isum_lo.release();
-    g_isum_hi.release(); g_n_int.release(); g_min.release(); g_max.release();
-    g_key_len.release(); g_key_kind.release(); g_key_esc.release(); g_fsum.release();
-    g_saw.release();
+    g_keys.release(); g_acc.release();
   }
 };
 
@@ -120,15 +114,12 @@ __global__ void k_reset_run(RunCounters *ctr, GroupTable g, uint32_t g_cap, uint
   if (g.slots) {
     for (unsigned long long i = tid; i < g_cap; i += stride) g.slots[i] = 0;
     for (unsigned long long i = tid; i < key_cap; i += stride) {
-      g.count[i] = 0;
-      g.numeric[i] = 0;
-      g.isum_lo[i] = 0;
-      g.isum_hi[i] = 0;
-      g.n_int[i] = 0;
-      g.min_bits[i] = ~0ull;
-      g.max_bits[i] = 0;
-      g.fsum[i] = 0.0;
-      g.saw_non_numeric[i] = 0;
+      GroupAcc a;
+      a.count = a.numeric = a.isum_lo = a.isum_hi = a.n_int = 0;
+      a.min_bits = ~0ull;
+      a.max_bits = 0;
+      a.fsum = 0.0;
+      g.acc[i] = a;
     }
   }
 }
@@ -238,20 +229,8 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n, char *er
       rb.g_key_cap = 1u << 16;
     }
     CK(rb.g_slots.ensure(rb.g_cap), "alloc group table");
-    size_t k = rb.g_key_cap;
-    CK(rb.g_key_off.ensure(k), "alloc groups");
-    CK(rb.g_key_len.ensure(k), "alloc groups");
-    CK(rb.g_key_kind.ensure(k), "alloc groups");
-    CK(rb.g_key_esc.ensure(k), "alloc groups");
-    CK(rb.g_count.ensure(k), "alloc groups");
-    CK(rb.g_numeric.ensure(k), "alloc groups");
-    CK(rb.g_isum_lo.ensure(k), "alloc groups");
-    CK(rb.g_isum_hi.ensure(k), "alloc groups");
-    CK(rb.g_n_int.ensure(k), "alloc groups");
-    CK(rb.g_min.ensure(k), "alloc groups");
-    CK(rb.g_max.ensure(k), "alloc groups");
-    CK(rb.g_fsum.ensure(k), "alloc groups");
-    CK(rb.g_saw.ensure(k), "alloc groups");
+    CK(rb.g_keys.ensure(rb.g_key_cap), "alloc group keys");
+    CK(rb.g_acc.ensure(rb.g_key_cap), "alloc group accumulators");
   }
   return WARPJQ_OK;
 }
@@ -262,19 +241,8 @@ GroupTable group_view(RunBufs &rb, bool on) {
   g.slots = rb.g_slots.p;
   g.cap_mask = rb.g_cap - 1;
   g.key_cap = rb.g_key_cap;
-  g.key_off = rb.g_key_off.p;
-  g.key_len = rb.g_key_len.p;
-  g.key_kind = rb.g_key_kind.p;
-  g.key_esc = rb.g_key_esc.p;
-  g.count = rb.g_count.p;
-  g.numeric = rb.g_numeric.p;
-  g.isum_lo = rb.g_isum_lo.p;
-  g.isum_hi = rb.g_isum_hi.p;
-  g.n_int = rb.g_n_int.p;
-  g.min_bits = rb.g_min.p;
-  g.max_bits = rb.g_max.p;
-  g.fsum = rb.g_fsum.p;
-  g.saw_non_numeric = rb.g_saw.p;
+  g.keys = rb.g_keys.p;
+  g.acc = rb.g_acc.p;
   return g;
 }
 
@@ -389,10 +357,8 @@ bool grow_after_overflow(warpjq_ctx *c, Slot &s, const RunCounters &h, unsigned 
     while (rb.g_cap < rb.g_key_cap * 2u) rb.g_cap <<= 1;
     rb.g_key_cap = rb.g_cap / 2;
     rb.g_slots.release();
-    rb.g_key_off.release(); rb.g_key_len.release(); rb.g_key_kind.release(); rb.g_key_esc.release();
-    rb.g_count.release(); rb.g_numeric.release(); rb.g_isum_lo.release(); rb.g_isum_hi.release();
-    rb.g_n_int.release(); rb.g_min.release(); rb.g_max.release(); rb.g_fsum.release();
-    rb.g_saw.release();
+    rb.g_keys.release();
+    rb.g_acc.release();
     again = true;
   }
   if (h.overflow & 8u) {  // deep nesting
@@ -570,6 +536,33 @@ warpjq_status warpjq_submit(warpjq_ctx *ctx, uint32_t slot, uint64_t n_bytes, ch
   return WARPJQ_OK;
 }
 
+warpjq_status warpjq_submit_host(warpjq_ctx *ctx, uint32_t slot, const uint8_t *src,
+                                 uint64_t n_bytes, char *err, size_t err_len) {
+  if (!ctx || slot >= ctx->slots.size() || n_bytes > ctx->chunk_cap || (!src && n_bytes)) {
+    set_err(err, err_len, "submit: bad slot or source, or %llu bytes over the slot capacity",
+            (unsigned long long)n_bytes);
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  Slot &s = ctx->slots[slot];
+  s.n_bytes = n_bytes;
+  if (n_bytes)
+    CK(cudaMemcpyAsync(s.d_chunk, src, n_bytes, cudaMemcpyHostToDevice, s.stream), "H2D chunk");
+  warpjq_status rc = enqueue_run(ctx, s, s.d_chunk, n_bytes, s.stream, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  CK(cudaEventRecord(s.done, s.stream), "event record");
+  return WARPJQ_OK;
+}
+
+int warpjq_host_is_pinned(const void *p) {
+  if (!p) return 0;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the error state of the failed query
+    return 0;
+  }
+  return a.type == cudaMemoryTypeHost ? 1 : 0;
+}
+
 static warpjq_status ensure_pinned(Slot &s, size_t out_bytes, size_t rows, size_t groups,
                                    char *err, size_t err_len) {
   if (out_bytes > s.h_out_cap || !s.h_out) {
@@ -605,37 +598,29 @@ static warpjq_status fetch_groups(warpjq_ctx *ctx, Slot &s, const RunCounters &h
   out.clear();
   uint32_t nk = std::min<uint32_t>(h.n_keys, s.rb.g_key_cap);
   if (!nk) return WARPJQ_OK;
-  std::vector<unsigned long long> off(nk), cnt(nk), num(nk), lo(nk), hi(nk), ni(nk), mn(nk), mx(nk);
-  std::vector<uint32_t> len(nk);
-  std::vector<uint8_t> kind(nk);
-  std::vector<double> fs(nk);
+  std::vector<GroupKeyDesc> keys(nk);
+  std::vector<GroupAcc> acc(nk);
   RunBufs &rb = s.rb;
-  CK(cudaMemcpy(off.data(), rb.g_key_off.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(len.data(), rb.g_key_len.p, nk * 4, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(kind.data(), rb.g_key_kind.p, nk, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(cnt.data(), rb.g_count.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(num.data(), rb.g_numeric.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(lo.data(), rb.g_isum_lo.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(hi.data(), rb.g_isum_hi.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(ni.data(), rb.g_n_int.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(mn.data(), rb.g_min.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(mx.data(), rb.g_max.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
-  CK(cudaMemcpy(fs.data(), rb.g_fsum.p, nk * 8, cudaMemcpyDeviceToHost), "D2H groups");
+  CK(cudaMemcpy(keys.data(), rb.g_keys.p, nk * sizeof(GroupKeyDesc), cudaMemcpyDeviceToHost),
+     "D2H group keys");
+  CK(cudaMemcpy(acc.data(), rb.g_acc.p, nk * sizeof(GroupAcc), cudaMemcpyDeviceToHost),
+     "D2H group accumulators");
   for (uint32_t k = 0; k < nk; k++) {
-    if (cnt[k] == 0) continue;  // an id allocated by a racing insert that lost
+    const GroupAcc &a = acc[k];
+    if (a.count == 0) continue;  // an id allocated by a racing insert that lost
     warpjq_group_ext g{};
-    g.key_off = off[k];
-    g.key_len = len[k];
-    g.key_kind = kind[k];
-    g.count = cnt[k];
-    g.numeric = num[k];
-    g.isum_lo = lo[k];
-    g.isum_hi = hi[k];
-    g.n_int = ni[k];
-    g.fsum = fs[k];
-    g.min = num[k] ? from_order_bits(mn[k]) : 1.0 / 0.0;
-    g.max = num[k] ? from_order_bits(mx[k]) : -1.0 / 0.0;
-    g.sum = (ni[k] ? i128_to_double(lo[k], hi[k]) : 0.0) + fs[k];
+    g.key_off = keys[k].off;
+    g.key_len = keys[k].len;
+    g.key_kind = keys[k].kind;
+    g.count = a.count;
+    g.numeric = a.numeric;
+    g.isum_lo = a.isum_lo;
+    g.isum_hi = a.isum_hi;
+    g.n_int = a.n_int;
+    g.fsum = a.fsum;
+    g.min = a.numeric ? from_order_bits(a.min_bits) : 1.0 / 0.0;
+    g.max = a.numeric ? from_order_bits(a.max_bits) : -1.0 / 0.0;
+    g.sum = (a.n_int ? i128_to_double(a.isum_lo, a.isum_hi) : 0.0) + a.fsum;
     out.push_back(g);
   }
   (void)ctx;

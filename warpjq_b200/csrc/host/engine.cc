@@ -453,6 +453,9 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     return 0;
   };
 
+  // Page-locked input is copied to the device straight from the caller's
+  // memory; anything else is staged through the slots' pinned buffers.
+  const bool pinned = len && warpjq_host_is_pinned(data) && warpjq_host_is_pinned(data + len - 1);
   // Tiles sized from the input's own line lengths (first MiB of the run).
   if (!q->tiled && len) {
     if (warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
@@ -510,9 +513,14 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
       if (drain(flight.front())) return 1;
       flight.erase(flight.begin());
     }
-    copy_to_pinned(warpjq_slot_buffer(q->ctx, slot), data + pos, n);
-    if (warpjq_submit(q->ctx, slot, n, e, sizeof e) != WARPJQ_OK)
-      return fail(std::string("CUDA error in submitting a chunk: ") + e);
+    warpjq_status sub;
+    if (pinned) {
+      sub = warpjq_submit_host(q->ctx, slot, data + pos, n, e, sizeof e);
+    } else {
+      copy_to_pinned(warpjq_slot_buffer(q->ctx, slot), data + pos, n);
+      sub = warpjq_submit(q->ctx, slot, n, e, sizeof e);
+    }
+    if (sub != WARPJQ_OK) return fail(std::string("CUDA error in submitting a chunk: ") + e);
     flight.push_back({slot, data + pos, n});
     if (flight.size() > 1) {
       if (drain(flight.front())) return 1;

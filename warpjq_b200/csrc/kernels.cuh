@@ -55,23 +55,31 @@ struct RowRec {
 };
 static_assert(sizeof(RowRec) == kRowRecBytes, "row record header size");
 
+// One group key's accumulators: a 64-byte record, so all updates of a key
+// land on one line of memory.
+struct GroupAcc {
+  unsigned long long count, numeric, isum_lo, isum_hi, n_int, min_bits, max_bits;
+  double fsum;
+};
+static_assert(sizeof(GroupAcc) == 64, "group accumulator record");
+
+// Where a group key's bytes are (the first line that inserted it).
+struct GroupKeyDesc {
+  unsigned long long off;  // absolute input offset of the key bytes (string: body)
+  uint32_t len;
+  uint8_t kind;
+  uint8_t esc;
+  uint8_t saw_non_numeric;  // a selected line had a non-numeric, non-null value
+  uint8_t pad;
+};
+static_assert(sizeof(GroupKeyDesc) == 16, "group key descriptor");
+
 struct GroupTable {
   unsigned long long *slots;  // 0 = empty, else (hash << 32) | (key_id + 1)
   uint32_t cap_mask;
   uint32_t key_cap;
-  unsigned long long *key_off;
-  uint32_t *key_len;
-  uint8_t *key_kind;
-  uint8_t *key_esc;
-  unsigned long long *count;
-  unsigned long long *numeric;
-  unsigned long long *isum_lo;
-  unsigned long long *isum_hi;
-  unsigned long long *n_int;
-  unsigned long long *min_bits;
-  unsigned long long *max_bits;
-  double *fsum;
-  unsigned int *saw_non_numeric;
+  GroupKeyDesc *keys;
+  GroupAcc *acc;
 };
 
 // Per-tile totals of a rows run.
@@ -166,10 +174,14 @@ __device__ uint32_t group_find_or_insert(const ScanParams &sp, const KeyRef &k, 
           atomicOr(&sp.ctr->overflow, 4u);
           return 0xFFFFFFFFu;
         }
-        g.key_off[mine] = k.abs_off;
-        g.key_len[mine] = k.len;
-        g.key_kind[mine] = k.kind;
-        g.key_esc[mine] = k.esc;
+        GroupKeyDesc d;
+        d.off = k.abs_off;
+        d.len = k.len;
+        d.kind = k.kind;
+        d.esc = k.esc;
+        d.saw_non_numeric = 0;
+        d.pad = 0;
+        g.keys[mine] = d;
         __threadfence();
       }
       unsigned long long want = ((unsigned long long)h << 32) | (mine + 1ull);
@@ -180,9 +192,8 @@ __device__ uint32_t group_find_or_insert(const ScanParams &sp, const KeyRef &k, 
     if ((uint32_t)(w >> 32) == h) {
       uint32_t kid = (uint32_t)w - 1;
       __threadfence();
-      if (g.key_kind[kid] == k.kind &&
-          key_bytes_equal(k, sp.data + g.key_off[kid], g.key_len[kid], g.key_esc[kid]))
-        return kid;
+      const GroupKeyDesc d = g.keys[kid];
+      if (d.kind == k.kind && key_bytes_equal(k, sp.data + d.off, d.len, d.esc)) return kid;
     }
     pos = (pos + 1) & g.cap_mask;
   }
@@ -275,9 +286,22 @@ __device__ __forceinline__ uint32_t row_length(const DevPlan &P, const uint8_t *
   }
 }
 
-// Warp-cooperative copy of n bytes (lanes stride by 32: coalesced stores).
+// Warp-cooperative copy of n bytes: each lane loads four bytes 32 apart
+// before storing them, so one step moves 128 bytes with the loads in flight
+// together (lanes stride by 32: coalesced accesses).
 __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint32_t n, int lane) {
-  for (uint32_t k = lane; k < n; k += 32) dst[k] = src[k];
+  for (uint32_t base = 0; base < n; base += 128) {
+    const uint32_t k0 = base + lane;
+    uint8_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+    if (k0 < n) b0 = src[k0];
+    if (k0 + 32 < n) b1 = src[k0 + 32];
+    if (k0 + 64 < n) b2 = src[k0 + 64];
+    if (k0 + 96 < n) b3 = src[k0 + 96];
+    if (k0 < n) dst[k0] = b0;
+    if (k0 + 32 < n) dst[k0 + 32] = b1;
+    if (k0 + 64 < n) dst[k0 + 64] = b2;
+    if (k0 + 96 < n) dst[k0 + 96] = b3;
+  }
 }
 
 // Writes one row.  All lanes of the warp call it together.
@@ -702,28 +726,70 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
           }
         }
         if (!kRows && P.group_slot >= 0) {
+          // Lanes whose keys hash alike compare their key bytes with the
+          // lowest such lane; only lanes that differ from it look up the
+          // table themselves.
+          const uint32_t hv = has_group ? gh : 0u;
+          const unsigned peers = __match_any_sync(0xffffffffu, hv);
+          const int leader = __ffs(peers) - 1;
+          const unsigned long long lp = __shfl_sync(0xffffffffu, (unsigned long long)gk.p, leader);
+          const uint32_t llen = __shfl_sync(0xffffffffu, gk.len, leader);
+          const uint32_t lkind = __shfl_sync(0xffffffffu, (uint32_t)gk.kind, leader);
+          const uint32_t lesc = __shfl_sync(0xffffffffu, (uint32_t)gk.esc, leader);
+          const bool same = has_group && lane != leader && gk.kind == lkind &&
+                            key_bytes_equal(gk, (const uint8_t *)lp, llen, (uint8_t)lesc);
           uint32_t kid = 0xFFFFFFFFu;
-          if (has_group) kid = group_find_or_insert(sp, gk, gh);
-          const GroupTable &g = sp.g;
-          if (kid != 0xFFFFFFFFu) {
-            atomicAdd(&g.count[kid], 1ull);
-            if (is_num) {
-              atomicAdd(&g.numeric[kid], 1ull);
-              unsigned long long ob = order_bits(fv);
-              atomicMin(&g.min_bits[kid], ob);
-              atomicMax(&g.max_bits[kid], ob);
-              if (is_int) {
-                unsigned long long old = atomicAdd(&g.isum_lo[kid], (unsigned long long)iv);
-                unsigned long long carry = (old + (unsigned long long)iv) < old;
-                unsigned long long hi = (iv < 0 ? ~0ull : 0ull) + carry;
-                if (hi) atomicAdd(&g.isum_hi[kid], hi);
-                atomicAdd(&g.n_int[kid], 1ull);
-              } else {
-                atomicAdd(&g.fsum[kid], fv);
-              }
-            } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0) {
-              g.saw_non_numeric[kid] = 1;
+          if (has_group && !same) kid = group_find_or_insert(sp, gk, gh);
+          const uint32_t lkid = __shfl_sync(0xffffffffu, kid, leader);
+          if (same) kid = lkid;
+          const bool saw_here =
+              has_group && !is_num && aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0;
+          // One update per distinct key in the warp: its lanes' contributions
+          // are reduced first (a fixed lane-order tree).
+          unsigned pending = __ballot_sync(0xffffffffu, kid != 0xFFFFFFFFu);
+          while (pending) {
+            const int ld = __ffs(pending) - 1;
+            const uint32_t k = __shfl_sync(0xffffffffu, kid, ld);
+            const bool m = kid == k;
+            const unsigned grp = __ballot_sync(0xffffffffu, m);
+            const unsigned long long cnt = __popc(grp);
+            const unsigned long long num = __popc(__ballot_sync(0xffffffffu, m && is_num));
+            const unsigned long long nint = __popc(__ballot_sync(0xffffffffu, m && is_num && is_int));
+            const bool saw = __any_sync(0xffffffffu, m && saw_here);
+            const long long v = (m && is_num && is_int) ? iv : 0;
+            unsigned long long lo = (unsigned long long)v, hi = v < 0 ? ~0ull : 0ull;
+            double f = (m && is_num && !is_int) ? fv : 0.0;
+            unsigned long long mn = (m && is_num) ? order_bits(fv) : ~0ull;
+            unsigned long long mx = (m && is_num) ? order_bits(fv) : 0ull;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+              const unsigned long long olo = __shfl_xor_sync(0xffffffffu, lo, d);
+              const unsigned long long ohi = __shfl_xor_sync(0xffffffffu, hi, d);
+              const unsigned long long sum = lo + olo;
+              hi += ohi + (sum < lo ? 1ull : 0ull);
+              lo = sum;
+              f += __shfl_xor_sync(0xffffffffu, f, d);
+              mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
+              mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
             }
+            if (lane == ld) {
+              GroupAcc &a = sp.g.acc[k];
+              atomicAdd(&a.count, cnt);
+              if (num) {
+                atomicAdd(&a.numeric, num);
+                atomicMin(&a.min_bits, mn);
+                atomicMax(&a.max_bits, mx);
+              }
+              if (nint) {
+                const unsigned long long old = atomicAdd(&a.isum_lo, lo);
+                const unsigned long long carry = (old + lo) < old ? 1ull : 0ull;
+                if (hi + carry) atomicAdd(&a.isum_hi, hi + carry);
+                atomicAdd(&a.n_int, nint);
+              }
+              if (num > nint) atomicAdd(&a.fsum, f);
+              if (saw) sp.g.keys[k].saw_non_numeric = 1;
+            }
+            pending &= ~grp;
           }
         }
 
@@ -881,16 +947,25 @@ __global__ void k_reduce_tiles(const double *tile_fsum, unsigned long long n_til
   }
 }
 
+// One warp: lane l sums block partials l, l+32, ... in order, then a fixed
+// shuffle tree combines the lanes (the same order on every run).
 __global__ void k_finalize(const double *block_f, const unsigned long long *block_lines,
                            unsigned nblocks, const TileDesc *tiles, RunCounters *ctr) {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x;
   double f = 0.0;
   unsigned long long lines = 0, lines_t = 0;
-  for (unsigned b = 0; b < nblocks; b++) {
+  for (unsigned b = lane; b < nblocks; b += 32) {
     f += block_f[b];
     lines += block_lines[2 * b];
     lines_t += block_lines[2 * b + 1];
   }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    f += __shfl_down_sync(0xffffffffu, f, d);
+    lines += __shfl_down_sync(0xffffffffu, lines, d);
+    lines_t += __shfl_down_sync(0xffffffffu, lines_t, d);
+  }
+  if (lane != 0) return;
   ctr->fsum_total = f;
   unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
   ctr->first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
@@ -901,8 +976,9 @@ __global__ void k_finalize(const double *block_f, const unsigned long long *bloc
 // Rows: prefix over the per-tile totals, then emission in line order.
 // ---------------------------------------------------------------------------
 
-constexpr uint32_t kEmitTiles = 1024;  // tiles per block of the rows passes
-constexpr int kEmitThreads = 256;
+constexpr uint32_t kEmitTiles = 128;  // tiles per block of the rows passes
+constexpr int kEmitThreads = 128;     // one thread per tile in the prefix step
+static_assert(kEmitTiles % kEmitThreads == 0, "emission sub-steps cover whole blocks");
 
 // Exclusive block scan of three u64 values in thread order, with totals.
 __device__ __forceinline__ void block_scan3(const unsigned long long v[3], unsigned long long ex[3],
