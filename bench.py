@@ -293,7 +293,7 @@ def main():
         outs = 0
         for _ in range(args.e2e_steps):
             for q in host_qs:
-                r = q.run(data_np)
+                r = q.run(data_np, copy_out=False)
                 if r.rc != 0:
                     raise RuntimeError(r.err)
                 outs += len(r.out)

@@ -120,6 +120,28 @@ def _take(ptr, n) -> bytes:
     return b
 
 
+class _HostBuffer:
+    """A malloc'd result buffer of the host library, exposed to numpy
+    without a copy and freed with the last array that views it."""
+
+    def __init__(self, ptr: int, n: int):
+        self.ptr, self.n = ptr, n
+        self.__array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr or 0, False),
+                                    "version": 3}
+
+    def __del__(self):
+        if self.ptr:
+            _load()[1].warpjq_host_free(ctypes.c_void_p(self.ptr))
+            self.ptr = 0
+
+
+def _view(ptr, n):
+    import numpy as np
+    if not ptr.value:
+        return np.zeros(0, dtype=np.uint8)
+    return np.asarray(_HostBuffer(ptr.value, n.value))
+
+
 def _stats(arr):
     return dict(zip(["bytes_in", "lines_in", "lines_out", "malformed", "type_errors"], list(arr)))
 
@@ -203,8 +225,11 @@ class Query:
     def is_aggregate(self) -> bool:
         return bool(self._h.warpjq_query_is_aggregate(self._q))
 
-    def run(self, data, on_invalid: str = "skip", max_line_bytes: int = 0) -> RunResult:
-        """Runs over host memory: `data` is bytes, or a numpy uint8 array."""
+    def run(self, data, on_invalid: str = "skip", max_line_bytes: int = 0,
+            copy_out: bool = True) -> RunResult:
+        """Runs over host memory: `data` is bytes, or a numpy uint8 array.
+        With copy_out=False the output is a numpy uint8 view of the host
+        library's buffer (no copy; freed with the array)."""
         if isinstance(data, (bytes, bytearray)):
             keep = ctypes.c_char_p(bytes(data))
             addr, n_bytes = ctypes.cast(keep, ctypes.c_void_p), len(data)
@@ -217,7 +242,8 @@ class Query:
         rc = self._h.warpjq_query_run(self._q, addr, n_bytes, ON_INVALID[on_invalid],
                                       max_line_bytes, ctypes.byref(out), ctypes.byref(n), st, err,
                                       len(err))
-        return RunResult(rc, _take(out, n), _stats(st), err.value.decode(errors="replace"))
+        body = _take(out, n) if copy_out else _view(out, n)
+        return RunResult(rc, body, _stats(st), err.value.decode(errors="replace"))
 
     def set_tiling(self, tile_bytes: int = 0, halo_bytes: int = 0):
         k, _ = _load()

@@ -235,8 +235,39 @@ GroupKey device_key(const uint8_t *data, uint64_t off, uint32_t len, uint32_t ki
 // Output writer (output.rs:87-334)
 // ---------------------------------------------------------------------------
 
+// Growable malloc'd byte buffer for row output: realloc grows big blocks
+// in place (remapped pages), and the finished buffer is handed to the
+// caller without another copy.
+struct Bytes {
+  char *p = nullptr;
+  size_t n = 0, cap = 0;
+  ~Bytes() { free(p); }
+  bool reserve(size_t want) {
+    if (want <= cap) return true;
+    char *q = (char *)realloc(p, want);
+    if (!q) return false;
+    p = q;
+    cap = want;
+    return true;
+  }
+  bool append(const void *src, size_t k) {
+    if (n + k + 1 > cap && !reserve(std::max(n + k + 1, cap * 2))) return false;
+    memcpy(p + n, src, k);
+    n += k;
+    return true;
+  }
+  char *release() {
+    char *q = p;
+    p = nullptr;
+    n = cap = 0;
+    return q;
+  }
+};
+
 struct Writer {
-  std::string buf;
+  std::string buf;   // text output (header, aggregates, groups)
+  Bytes bulk_rows;   // row output, after any header text
+  bool oom = false;
   uint32_t fmt;  // WARPJQ_FMT_*
   uint64_t rows = 0;
   void header(const Program &p) {
@@ -251,7 +282,16 @@ struct Writer {
   }
   void bulk(const uint8_t *p, size_t n, uint64_t r) {
     rows += r;
-    if (fmt != WARPJQ_FMT_COUNT) buf.append((const char *)p, n);
+    if (fmt == WARPJQ_FMT_COUNT) return;
+    if (!bulk_rows.p && !buf.empty()) {
+      oom |= !bulk_rows.append(buf.data(), buf.size());
+      buf.clear();
+    }
+    oom |= !bulk_rows.append(p, n);
+  }
+  // Expected total row bytes, from the share of the input done so far.
+  void reserve_rows(size_t total) {
+    if (total > bulk_rows.cap) oom |= !bulk_rows.reserve(total + 1);
   }
   void aggregate(uint32_t kind, const Agg &a) {
     rows++;
@@ -285,9 +325,23 @@ struct Writer {
       buf += '\n';
     }
   }
-  std::string finish() {
+  // Hands the output to the caller as one malloc'd, NUL-terminated buffer.
+  char *finish(size_t &len) {
     if (fmt == WARPJQ_FMT_COUNT) buf = std::to_string(rows) + "\n";
-    return buf;
+    if (bulk_rows.p) {
+      if (!buf.empty()) oom |= !bulk_rows.append(buf.data(), buf.size());
+      oom |= !bulk_rows.reserve(bulk_rows.n + 1);
+      if (oom) return nullptr;
+      bulk_rows.p[bulk_rows.n] = 0;
+      len = bulk_rows.n;
+      return bulk_rows.release();
+    }
+    char *o = (char *)malloc(buf.size() + 1);
+    if (!o) return nullptr;
+    memcpy(o, buf.data(), buf.size());
+    o[buf.size()] = 0;
+    len = buf.size();
+    return o;
   }
 };
 
@@ -418,6 +472,7 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     return 1;
   };
 
+  bool reserved = false;
   auto drain = [&](const Flight &f) -> int {
     warpjq_chunk_result r;
     warpjq_status rc = warpjq_wait(q->ctx, f.slot, &r, e, sizeof e);
@@ -449,7 +504,14 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     } else if (r.n_selected) {
       w.bulk(r.out_bytes + r.out_row_off[0], (size_t)(r.out_row_off[r.n_selected] - r.out_row_off[0]),
              r.n_selected);
+      // Size the output once from the first chunk's share of it.
+      const uint64_t done = (uint64_t)(f.data - data) + f.n;
+      if (!reserved && done < len) {
+        w.reserve_rows((size_t)((double)w.bulk_rows.n * (double)len / (double)done * 1.05));
+        reserved = true;
+      }
     }
+    if (w.oom) return fail("out of host memory for the output");
     return 0;
   };
 
@@ -542,7 +604,9 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     }
   }
   uint64_t rows = w.rows;
-  std::string res = w.finish();
+  size_t res_len = 0;
+  char *res = w.finish(res_len);
+  if (!res) return fail("out of host memory for the output");
   if (stats) {
     stats[0] = len;
     stats[1] = st_lines;
@@ -550,11 +614,8 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     stats[3] = st_malformed;
     stats[4] = st_type;
   }
-  char *buf = (char *)malloc(res.size() + 1);
-  memcpy(buf, res.data(), res.size());
-  buf[res.size()] = 0;
-  *out = buf;
-  if (out_len) *out_len = res.size();
+  *out = res;
+  if (out_len) *out_len = res_len;
   return 0;
 }
 
@@ -598,12 +659,11 @@ int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r, c
   } else {
     w.rows = r->n_selected;
   }
-  std::string res = w.finish();
-  char *buf = (char *)malloc(res.size() + 1);
-  memcpy(buf, res.data(), res.size());
-  buf[res.size()] = 0;
-  *out = buf;
-  if (out_len) *out_len = res.size();
+  size_t res_len = 0;
+  char *res = w.finish(res_len);
+  if (!res) return 1;
+  *out = res;
+  if (out_len) *out_len = res_len;
   return 0;
 }
 

@@ -742,54 +742,26 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
           if (has_group && !same) kid = group_find_or_insert(sp, gk, gh);
           const uint32_t lkid = __shfl_sync(0xffffffffu, kid, leader);
           if (same) kid = lkid;
-          const bool saw_here =
-              has_group && !is_num && aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0;
-          // One update per distinct key in the warp: its lanes' contributions
-          // are reduced first (a fixed lane-order tree).
-          unsigned pending = __ballot_sync(0xffffffffu, kid != 0xFFFFFFFFu);
-          while (pending) {
-            const int ld = __ffs(pending) - 1;
-            const uint32_t k = __shfl_sync(0xffffffffu, kid, ld);
-            const bool m = kid == k;
-            const unsigned grp = __ballot_sync(0xffffffffu, m);
-            const unsigned long long cnt = __popc(grp);
-            const unsigned long long num = __popc(__ballot_sync(0xffffffffu, m && is_num));
-            const unsigned long long nint = __popc(__ballot_sync(0xffffffffu, m && is_num && is_int));
-            const bool saw = __any_sync(0xffffffffu, m && saw_here);
-            const long long v = (m && is_num && is_int) ? iv : 0;
-            unsigned long long lo = (unsigned long long)v, hi = v < 0 ? ~0ull : 0ull;
-            double f = (m && is_num && !is_int) ? fv : 0.0;
-            unsigned long long mn = (m && is_num) ? order_bits(fv) : ~0ull;
-            unsigned long long mx = (m && is_num) ? order_bits(fv) : 0ull;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-              const unsigned long long olo = __shfl_xor_sync(0xffffffffu, lo, d);
-              const unsigned long long ohi = __shfl_xor_sync(0xffffffffu, hi, d);
-              const unsigned long long sum = lo + olo;
-              hi += ohi + (sum < lo ? 1ull : 0ull);
-              lo = sum;
-              f += __shfl_xor_sync(0xffffffffu, f, d);
-              mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
-              mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
-            }
-            if (lane == ld) {
-              GroupAcc &a = sp.g.acc[k];
-              atomicAdd(&a.count, cnt);
-              if (num) {
-                atomicAdd(&a.numeric, num);
-                atomicMin(&a.min_bits, mn);
-                atomicMax(&a.max_bits, mx);
+          if (kid != 0xFFFFFFFFu) {
+            GroupAcc &a = sp.g.acc[kid];
+            atomicAdd(&a.count, 1ull);
+            if (is_num) {
+              atomicAdd(&a.numeric, 1ull);
+              const unsigned long long ob = order_bits(fv);
+              atomicMin(&a.min_bits, ob);
+              atomicMax(&a.max_bits, ob);
+              if (is_int) {
+                const unsigned long long old = atomicAdd(&a.isum_lo, (unsigned long long)iv);
+                const unsigned long long carry = (old + (unsigned long long)iv) < old ? 1ull : 0ull;
+                const unsigned long long hi = (iv < 0 ? ~0ull : 0ull) + carry;
+                if (hi) atomicAdd(&a.isum_hi, hi);
+                atomicAdd(&a.n_int, 1ull);
+              } else {
+                atomicAdd(&a.fsum, fv);
               }
-              if (nint) {
-                const unsigned long long old = atomicAdd(&a.isum_lo, lo);
-                const unsigned long long carry = (old + lo) < old ? 1ull : 0ull;
-                if (hi + carry) atomicAdd(&a.isum_hi, hi + carry);
-                atomicAdd(&a.n_int, nint);
-              }
-              if (num > nint) atomicAdd(&a.fsum, f);
-              if (saw) sp.g.keys[k].saw_non_numeric = 1;
+            } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0) {
+              sp.g.keys[kid].saw_non_numeric = 1;
             }
-            pending &= ~grp;
           }
         }
 
