@@ -131,7 +131,10 @@ class _HostBuffer:
 
     def __del__(self):
         if self.ptr:
-            _load()[1].warpjq_host_free(ctypes.c_void_p(self.ptr))
+            try:
+                _load()[1].warpjq_host_free(ctypes.c_void_p(self.ptr))
+            except Exception:  # interpreter shutdown: the process frees it
+                pass
             self.ptr = 0
 
 

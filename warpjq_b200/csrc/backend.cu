@@ -178,7 +178,8 @@ namespace {
 
 
 warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
-  c->scan_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes);
+  c->scan_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes,
+                                 c->plan.output_kind == WARPJQ_OUT_AGG && c->plan.group_slot >= 0);
   int per_sm = 0;
   CK(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)c->scan_smem),

@@ -33,9 +33,11 @@ constexpr uint32_t kMaxLinesPerPass = 512;   // line-start list capacity per pas
 constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
 constexpr int kScanBlocksPerSM = 24;         // register budget of k_scan: 24 warps per SM
 
+constexpr int kGroupCache = 16;  // per-CTA group accumulators kept in shared memory
+
 // Dynamic shared memory of k_scan for tile T and halo H (the layout is at the
-// top of k_scan).
-__host__ __device__ inline size_t scan_smem_bytes(uint32_t T, uint32_t H) {
+// top of k_scan), plus the group cache for grouped aggregates.
+__host__ __device__ inline size_t scan_smem_base(uint32_t T, uint32_t H) {
   size_t nchunk_max = (T + H) / 32 + 1;
   size_t s = T + H + 32;
   s += ((nchunk_max + 3) & ~(size_t)3) * sizeof(uint32_t);
@@ -73,6 +75,18 @@ struct GroupKeyDesc {
   uint8_t pad;
 };
 static_assert(sizeof(GroupKeyDesc) == 16, "group key descriptor");
+
+// A CTA's private accumulators for up to kGroupCache keys (direct-mapped by
+// key id), merged into the global records when the CTA finishes.  Hot keys
+// then cost shared-memory atomics instead of contended global ones.
+struct GroupCache {
+  uint32_t tag[kGroupCache];  // key id held by the entry, or 0xFFFFFFFF
+  GroupAcc acc[kGroupCache];
+};
+
+__host__ __device__ inline size_t scan_smem_bytes(uint32_t T, uint32_t H, bool groups) {
+  return scan_smem_base(T, H) + (groups ? sizeof(GroupCache) : 0);
+}
 
 struct GroupTable {
   unsigned long long *slots;  // 0 = empty, else (hash << 32) | (key_id + 1)
@@ -467,6 +481,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
   uint8_t *win = smem;                                                 // T + H + 32
   uint32_t *nlmask = (uint32_t *)(smem + T + H + 32);                  // nchunk_max (+pad)
   uint16_t *lstart = (uint16_t *)(nlmask + ((nchunk_max + 3) & ~3u));  // kMaxLinesPerPass + 2
+  GroupCache *gcache = (GroupCache *)(smem + scan_smem_base(T, H));     // grouped aggregates only
 
   const int lane = threadIdx.x;
   const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
@@ -485,6 +500,20 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
   unsigned long long cta_recs = 0;  // records this CTA has appended (rows mode)
   NodeVals nv;
   SlotVal slots[kMaxSlots];
+
+  const bool grouped = !kRows && P.group_slot >= 0;
+  if (grouped) {
+    for (int k = lane; k < kGroupCache; k += 32) {
+      gcache->tag[k] = 0xFFFFFFFFu;
+      GroupAcc z;
+      z.count = z.numeric = z.isum_lo = z.isum_hi = z.n_int = 0;
+      z.min_bits = ~0ull;
+      z.max_bits = 0;
+      z.fsum = 0.0;
+      gcache->acc[k] = z;
+    }
+    __syncwarp();
+  }
 
   // Tickets are taken one tile ahead, so the atomic's latency overlaps a
   // tile's work.
@@ -743,7 +772,17 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
           const uint32_t lkid = __shfl_sync(0xffffffffu, kid, leader);
           if (same) kid = lkid;
           if (kid != 0xFFFFFFFFu) {
-            GroupAcc &a = sp.g.acc[kid];
+            // This CTA's cached entry for the key if it has (or can claim)
+            // one, else the global record.
+            GroupAcc *ap = &sp.g.acc[kid];
+            const uint32_t e = kid & (kGroupCache - 1);
+            uint32_t t = *(volatile uint32_t *)&gcache->tag[e];
+            if (t == 0xFFFFFFFFu) {
+              const uint32_t prev = atomicCAS(&gcache->tag[e], 0xFFFFFFFFu, kid);
+              t = prev == 0xFFFFFFFFu ? kid : prev;
+            }
+            if (t == kid) ap = &gcache->acc[e];
+            GroupAcc &a = *ap;
             atomicAdd(&a.count, 1ull);
             if (is_num) {
               atomicAdd(&a.numeric, 1ull);
@@ -822,6 +861,30 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
 #pragma unroll
       for (int d = 16; d > 0; d >>= 1) f += __shfl_down_sync(0xffffffffu, f, d);
       if (lane == 0) sp.tile_fsum[tile] = f;
+    }
+  }
+
+  // Merge this CTA's cached group accumulators into the global records.
+  if (grouped) {
+    __syncwarp();
+    for (int k = lane; k < kGroupCache; k += 32) {
+      const uint32_t kid = gcache->tag[k];
+      if (kid == 0xFFFFFFFFu) continue;
+      const GroupAcc c = gcache->acc[k];
+      GroupAcc &a = sp.g.acc[kid];
+      if (c.count) atomicAdd(&a.count, c.count);
+      if (c.numeric) {
+        atomicAdd(&a.numeric, c.numeric);
+        atomicMin(&a.min_bits, c.min_bits);
+        atomicMax(&a.max_bits, c.max_bits);
+      }
+      if (c.n_int) {
+        const unsigned long long old = atomicAdd(&a.isum_lo, c.isum_lo);
+        const unsigned long long carry = (old + c.isum_lo) < old ? 1ull : 0ull;
+        if (c.isum_hi + carry) atomicAdd(&a.isum_hi, c.isum_hi + carry);
+        atomicAdd(&a.n_int, c.n_int);
+      }
+      if (c.numeric > c.n_int) atomicAdd(&a.fsum, c.fsum);
     }
   }
 

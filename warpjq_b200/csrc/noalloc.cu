@@ -98,7 +98,7 @@ warpjq_status noalloc_setup(int dev, DeviceSetup *&out, char *err, size_t err_le
       set_err(err, err_len, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
       return WARPJQ_ERR_CUDA;
     }
-    size_t smem = scan_smem_bytes(kNoAllocTile, kNoAllocHalo);
+    size_t smem = scan_smem_bytes(kNoAllocTile, kNoAllocHalo, false);  // grouped queries are rejected
     e = cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
       set_err(err, err_len, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
