@@ -166,3 +166,23 @@ def test_nginx_benchmark_queries():
           "group_by(.host) | sum(.bytes)", "select(.status == 500)", "sum(.bytes)", "avg(.latency_ms)",
           "max(.latency_ms)", "min(.bytes)", "group_by(.path) | count", "group_by(.status) | avg(.bytes)"]
     agree(data, qs, "nginx", chunk_bytes=1 << 22, fractional={"avg(.latency_ms)"})
+
+
+def test_contexts_with_different_tilings_interleave():
+    """Several live queries with different tile sizes and shared-memory needs
+    (a grouped aggregate keeps a per-CTA key cache) launched in turn: each
+    context's launches must stay valid after the others are configured."""
+    import numpy as np
+    buf, used, _ = wjq.gen_nginx(4 << 20, seed=5)
+    data = bytes(buf[:used])
+    qs = [wjq.Query("group_by(.host) | sum(.bytes)"), wjq.Query("select(.status == 500) | count"),
+          wjq.Query("select(.status == 500)")]
+    qs[0].autotile(np.frombuffer(data[: 1 << 20], dtype=np.uint8))
+    qs[1].set_tiling(4096, 1024)
+    qs[2].set_tiling(12288, 2048)
+    for _ in range(2):
+        for q in qs:
+            r = q.run(data)
+            assert r.rc == 0, r.err
+            c = orc.run(q.query, data)
+            assert r.out == c.out, q.query

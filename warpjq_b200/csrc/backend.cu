@@ -181,11 +181,20 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
   c->scan_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes,
                                  c->plan.output_kind == WARPJQ_OUT_AGG && c->plan.group_slot >= 0);
   int per_sm = 0;
-  CK(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)c->scan_smem),
+  // The limit is a property of the kernel, shared by every context in the
+  // process, so it is raised to the device maximum rather than to this
+  // context's need (occupancy follows each launch's own request).
+  int dev = 0, smem_max = 0;
+  CK(cudaGetDevice(&dev), "device");
+  CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "attribute");
+  if (c->scan_smem > (size_t)smem_max) {
+    set_err(err, err_len, "tiling needs %zu bytes of shared memory, over the %d available",
+            c->scan_smem, smem_max);
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  CK(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan rows)");
-  CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)c->scan_smem),
+  CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan agg)");
   int a = 0, b = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_scan<true>, kThreads, c->scan_smem),
