@@ -162,7 +162,7 @@ typedef struct {
  * aligned, at most 4 GiB, larger inputs are rejected with
  * WARPJQ_ERR_INVALID_ARG) and a warpjq_noalloc_result in device memory, which
  * is written when the work on `stream` completes.  All scratch lives in one
- * fixed array of about 7 MiB that every GPU loading this library holds
+ * fixed array of about 10 MiB that every GPU loading this library holds
  * until exit; every call shares it and it keeps the last call's contents, so
  * calls that overlap on the GPU race -- order them on one stream.  The first
  * call on each device does a one-time set-up (it looks up the array's device

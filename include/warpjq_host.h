@@ -37,6 +37,13 @@ int warpjq_query_open(const char *query, uint32_t format, uint64_t chunk_bytes,
                       warpjq_query **out, char *err, size_t err_len);
 void warpjq_query_close(warpjq_query *q);
 
+/* Parses and lowers `query` without a device context: enough to render
+ * results (warpjq_query_render_device), e.g. on the rank that merges the
+ * partial results of several GPUs; the query cannot run. */
+int warpjq_query_open_host(const char *query, uint32_t format, warpjq_query **out, char *err,
+                           size_t err_len);
+int warpjq_query_is_grouped(const warpjq_query *q);
+
 /* The device context, for device-resident runs through warpjq_ext.h. */
 warpjq_ctx *warpjq_query_ctx(warpjq_query *q);
 int warpjq_query_is_aggregate(const warpjq_query *q);

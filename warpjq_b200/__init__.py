@@ -39,7 +39,7 @@ EXT_SYMBOLS = [
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
     "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
-    "warpjq_gen_nginx", "warpjq_gen_nginx_block",
+    "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
 ]
 
 
@@ -84,6 +84,10 @@ def _load():
     h.warpjq_query_ctx.restype = vp
     h.warpjq_query_is_aggregate.argtypes = [vp]
     h.warpjq_query_is_aggregate.restype = ctypes.c_int
+    h.warpjq_query_open_host.argtypes = [cp, u32, ctypes.POINTER(vp), cp, sz]
+    h.warpjq_query_open_host.restype = ctypes.c_int
+    h.warpjq_query_is_grouped.argtypes = [vp]
+    h.warpjq_query_is_grouped.restype = ctypes.c_int
     h.warpjq_query_run.argtypes = [vp, vp, sz, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
                                    ctypes.POINTER(u64), cp, sz]
     h.warpjq_query_run.restype = ctypes.c_int
@@ -196,13 +200,19 @@ class DeviceResult(ctypes.Structure):
 class Query:
     """A compiled query with its device context (warpjq_query_open)."""
 
-    def __init__(self, query: str, fmt: str = "ndjson", chunk_bytes: int = 0):
+    def __init__(self, query: str, fmt: str = "ndjson", chunk_bytes: int = 0, device: bool = True):
+        """device=False parses and lowers only (no device context): such a
+        query renders merged results (render_device) but cannot run."""
         _, h = _load()
         self._h = h
         self._q = ctypes.c_void_p()
         err = ctypes.create_string_buffer(4096)
-        rc = h.warpjq_query_open(query.encode(), FORMATS[fmt], chunk_bytes, ctypes.byref(self._q),
-                                 err, len(err))
+        if device:
+            rc = h.warpjq_query_open(query.encode(), FORMATS[fmt], chunk_bytes, ctypes.byref(self._q),
+                                     err, len(err))
+        else:
+            rc = h.warpjq_query_open_host(query.encode(), FORMATS[fmt], ctypes.byref(self._q), err,
+                                          len(err))
         if rc:
             raise ValueError(err.value.decode(errors="replace")) if rc == 2 else \
                 RuntimeError(err.value.decode(errors="replace"))
@@ -223,6 +233,14 @@ class Query:
     @property
     def ctx(self):
         return self._h.warpjq_query_ctx(self._q)
+
+    @property
+    def is_aggregate(self) -> bool:
+        return bool(self._h.warpjq_query_is_aggregate(self._q))
+
+    @property
+    def is_grouped(self) -> bool:
+        return bool(self._h.warpjq_query_is_grouped(self._q))
 
     @property
     def is_aggregate(self) -> bool:

@@ -397,8 +397,9 @@ extern "C" {
 
 void warpjq_host_free(void *p) { free(p); }
 
-int warpjq_query_open(const char *query, uint32_t format, uint64_t chunk_bytes, warpjq_query **out,
-                      char *err, size_t err_len) {
+// Parse and lowering, shared by both opens.
+static int open_parsed(const char *query, uint32_t format, warpjq_query **out, char *err,
+                       size_t err_len) {
   *out = nullptr;
   auto *q = new warpjq_query();
   QueryError qe;
@@ -417,6 +418,23 @@ int warpjq_query_open(const char *query, uint32_t format, uint64_t chunk_bytes, 
   }
   q->fmt = format;
   q->low.build(q->prog, format == WARPJQ_FMT_CSV);
+  *out = q;
+  return 0;
+}
+
+int warpjq_query_open_host(const char *query, uint32_t format, warpjq_query **out, char *err,
+                           size_t err_len) {
+  return open_parsed(query, format, out, err, err_len);
+}
+
+int warpjq_query_is_grouped(const warpjq_query *q) { return q && q->prog.has_group; }
+
+int warpjq_query_open(const char *query, uint32_t format, uint64_t chunk_bytes, warpjq_query **out,
+                      char *err, size_t err_len) {
+  *out = nullptr;
+  warpjq_query *q = nullptr;
+  int prc = open_parsed(query, format, &q, err, err_len);
+  if (prc) return prc;
   // gpu/mod.rs:143-145: the GPU chunk is capped at 64 MiB.
   uint64_t cap = chunk_bytes ? chunk_bytes : (256ull << 20);
   cap = std::min<uint64_t>(cap, std::max<uint64_t>(64ull << 20, 1 << 20));

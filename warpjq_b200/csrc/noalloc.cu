@@ -8,7 +8,7 @@
 // ungrouped-aggregate variant of the scan (count / sum / min / max / avg,
 // with or without a select()) using only:
 //   - the input and the result struct, both in device memory the caller owns;
-//   - a fixed scratch array in this file (g_noalloc_scratch, about 7 MiB),
+//   - a fixed scratch array in this file (g_noalloc_scratch, about 10 MiB),
 //     which every GPU that loads the library holds until the process exits.
 //
 // Limits and caveats:

@@ -1,0 +1,252 @@
+"""Scans over several GPUs: one newline-aligned byte range per rank.
+
+Lines are independent, so the input shards by byte range, cut after a
+newline the way the reference cuts its chunks
+(crates/warpjq-core/src/chunk.rs:234-278).  Each rank scans its range on its
+own GPU with no collective on the data path; rank 0 then gathers the ranks'
+partial results -- the exact aggregate state (counts, 128-bit integer sums,
+the FP sum, min/max), the groups with their key bytes, or the rank's rows --
+and merges them in rank order, as the reference's host merges chunk results
+in input order (crates/warpjq-core/src/gpu/mod.rs:959-1221, agg.rs:73-84).
+The merged state is rendered by the host library's own formatter
+(warpjq_query_render_device), so output bytes are those of a one-GPU run.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+from . import DeviceResult, Query, _GroupExt
+
+KIND_NULL, KIND_STR = 1, 4
+
+
+def shard_bounds(data, world: int) -> List[Tuple[int, int]]:
+    """[start, end) of each rank's range: the input cut into `world` parts
+    of about equal size, each cut placed just after a newline (a part is
+    empty when one line spans it)."""
+    mv = memoryview(data).cast("B")
+    n = len(mv)
+    cuts = [0]
+    for r in range(1, world):
+        t = max(cuts[-1], n * r // world)
+        cut = n
+        pos = t
+        while pos < n:
+            window = bytes(mv[pos:min(n, pos + (1 << 20))])
+            k = window.find(b"\n")
+            if k >= 0:
+                cut = pos + k + 1
+                break
+            pos += len(window)
+        cuts.append(max(cut, cuts[-1]))
+    cuts.append(n)
+    return list(zip(cuts[:-1], cuts[1:]))
+
+
+def decode_key(kind: int, raw: bytes) -> bytes:
+    """Group-key identity: string keys compare by their decoded bytes (escapes
+    resolved, a lone surrogate becomes U+FFFD; json.rs:594-654), every
+    other kind by its raw bytes (agg.rs:106-212)."""
+    if kind != KIND_STR or b"\\" not in raw:
+        return raw
+    out = bytearray()
+    i, n = 0, len(raw)
+    simple = {0x22: 0x22, 0x5C: 0x5C, 0x2F: 0x2F, 0x62: 0x08, 0x66: 0x0C, 0x6E: 0x0A, 0x72: 0x0D,
+              0x74: 0x09}
+    while i < n:
+        c = raw[i]
+        if c != 0x5C:
+            out.append(c)
+            i += 1
+            continue
+        e = raw[i + 1]
+        i += 2
+        if e != 0x75:
+            out.append(simple[e])
+            continue
+        cp = int(raw[i:i + 4], 16)
+        i += 4
+        if 0xD800 <= cp < 0xDC00 and raw[i:i + 2] == b"\\u":
+            lo = int(raw[i + 2:i + 6], 16)
+            if 0xDC00 <= lo < 0xE000:
+                cp = 0x10000 + ((cp - 0xD800) << 10) + (lo - 0xDC00)
+                i += 6
+        if 0xD800 <= cp < 0xE000:
+            cp = 0xFFFD
+        out += chr(cp).encode("utf-8")
+    return bytes(out)
+
+
+@dataclass
+class GroupPart:
+    kind: int
+    raw: bytes          # key bytes as in the input (string: the body)
+    count: int = 0
+    numeric: int = 0
+    isum: int = 0       # exact sum of the integer-literal values
+    n_int: int = 0
+    fsum: float = 0.0   # sum of the other numbers, in order
+    min: float = math.inf
+    max: float = -math.inf
+
+
+@dataclass
+class Partial:
+    """One rank's result, small and portable (torch.distributed objects)."""
+    n_lines: int = 0
+    n_blank: int = 0
+    n_invalid: int = 0
+    n_type_error: int = 0
+    n_selected: int = 0
+    count: int = 0
+    numeric: int = 0
+    isum: int = 0
+    n_int: int = 0
+    fsum: float = 0.0
+    min: float = math.inf
+    max: float = -math.inf
+    saw_non_numeric: bool = False
+    groups: List[GroupPart] = field(default_factory=list)
+    rows: bytes = b""
+
+
+class _DeviceBytes:
+    """Device memory described for torch.as_tensor (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, True),
+                                         "version": 2}
+
+
+def partial_from_device(r: DeviceResult, shard_host) -> Partial:
+    """The rank's partial from a collected device-resident run; group key
+    bytes are read from the rank's host copy of its shard."""
+    p = Partial(n_lines=r.n_lines, n_blank=r.n_blank, n_invalid=r.n_invalid,
+                n_type_error=r.n_type_error, n_selected=r.n_selected, count=r.count,
+                numeric=r.numeric, isum=r.isum(), n_int=r.n_int, fsum=r.fsum, min=r.min, max=r.max,
+                saw_non_numeric=bool(r.saw_non_numeric))
+    mv = memoryview(shard_host).cast("B")
+    for k in range(r.n_groups):
+        g = r.groups[k]
+        v = (g.isum_hi << 64) | g.isum_lo
+        v = v - (1 << 128) if g.isum_hi >> 63 else v
+        p.groups.append(GroupPart(kind=g.key_kind, raw=bytes(mv[g.key_off:g.key_off + g.key_len]),
+                                  count=g.count, numeric=g.numeric, isum=v, n_int=g.n_int,
+                                  fsum=g.fsum, min=g.min, max=g.max))
+    if r.out_len and r.d_out_bytes:
+        import torch
+        t = torch.as_tensor(_DeviceBytes(r.d_out_bytes, r.out_len), device="cuda")
+        p.rows = t.cpu().numpy().tobytes()
+    return p
+
+
+def merge(parts: Sequence[Partial]) -> Partial:
+    """Rank-order merge: counts and integer sums exactly, FP sums in rank
+    order, groups by key identity (first rank's raw bytes kept)."""
+    m = Partial()
+    groups = {}
+    rows = []
+    for p in parts:
+        m.n_lines += p.n_lines
+        m.n_blank += p.n_blank
+        m.n_invalid += p.n_invalid
+        m.n_type_error += p.n_type_error
+        m.n_selected += p.n_selected
+        m.count += p.count
+        m.numeric += p.numeric
+        m.isum += p.isum
+        m.n_int += p.n_int
+        m.fsum += p.fsum
+        m.min = min(m.min, p.min)
+        m.max = max(m.max, p.max)
+        m.saw_non_numeric |= p.saw_non_numeric
+        rows.append(p.rows)
+        for g in p.groups:
+            ident = (KIND_NULL if g.kind == 0 else g.kind, decode_key(g.kind, g.raw))
+            acc = groups.get(ident)
+            if acc is None:
+                acc = groups[ident] = GroupPart(kind=g.kind, raw=g.raw)
+            acc.count += g.count
+            acc.numeric += g.numeric
+            acc.isum += g.isum
+            acc.n_int += g.n_int
+            acc.fsum += g.fsum
+            acc.min = min(acc.min, g.min)
+            acc.max = max(acc.max, g.max)
+    m.groups = list(groups.values())
+    m.rows = b"".join(rows)
+    return m
+
+
+def _sum(isum: int, n_int: int, fsum: float) -> float:
+    # the device's rounding: the exact integer sum to FP64, plus the FP sum
+    return (float(isum) if n_int else 0.0) + fsum
+
+
+def render(query: str, merged: Partial, fmt: str = "ndjson") -> bytes:
+    """Output bytes of the merged result, through the host library's
+    formatter (no device needed)."""
+    q = Query(query, fmt, device=False)
+    r = DeviceResult()
+    r.n_lines, r.n_selected = merged.n_lines, merged.n_selected
+    r.count, r.numeric, r.n_int = merged.count, merged.numeric, merged.n_int
+    r.fsum, r.min, r.max = merged.fsum, merged.min, merged.max
+    r.sum = _sum(merged.isum, merged.n_int, merged.fsum)
+    r.saw_non_numeric = int(merged.saw_non_numeric)
+    keys = bytearray()
+    garr = (_GroupExt * max(1, len(merged.groups)))()
+    for k, g in enumerate(merged.groups):
+        e = garr[k]
+        e.key_off, e.key_len, e.key_kind = len(keys), len(g.raw), g.kind
+        keys += g.raw
+        e.count, e.numeric, e.n_int = g.count, g.numeric, g.n_int
+        e.isum_lo, e.isum_hi = g.isum & ((1 << 64) - 1), (g.isum >> 64) & ((1 << 64) - 1)
+        e.fsum, e.min, e.max = g.fsum, g.min, g.max
+        e.sum = _sum(g.isum, g.n_int, g.fsum)
+    r.groups = ctypes.cast(garr, ctypes.POINTER(_GroupExt))
+    r.n_groups = len(merged.groups)
+    head = q.render_device(r, bytes(keys))
+    q.close()
+    return head + merged.rows
+
+
+def gather(partial: Partial, rank: int, world: int, group=None) -> Optional[List[Partial]]:
+    """Rank 0 receives every rank's partial, in rank order (others: None)."""
+    if world == 1:
+        return [partial]
+    import torch.distributed as dist
+    out = [None] * world if rank == 0 else None
+    dist.gather_object(partial, out, dst=0, group=group)
+    return out
+
+
+def device_partial(query: str, shard_host, fmt: str = "ndjson") -> Partial:
+    """One range's partial from a device-resident run on the current GPU."""
+    import numpy as np
+    import torch
+    shard_np = np.frombuffer(memoryview(shard_host).cast("B"), dtype=np.uint8)
+    q = Query(query, fmt)
+    dev = torch.empty(max(1, len(shard_np)) + 16, dtype=torch.uint8, device="cuda")
+    if len(shard_np):
+        dev[:len(shard_np)].copy_(torch.from_numpy(shard_np.copy()))
+        q.autotile(shard_np[: 1 << 20])
+    q.launch_device(dev.data_ptr(), len(shard_np), torch.cuda.current_stream().cuda_stream)
+    part = partial_from_device(q.collect_device(), shard_np)
+    q.close()
+    return part
+
+
+def run_sharded(query: str, host_data, rank: int, world: int, fmt: str = "ndjson",
+                group=None) -> Optional[bytes]:
+    """Runs `query` over `host_data` on `world` GPUs (this process: `rank`,
+    on the current CUDA device).  Returns the output bytes on rank 0."""
+    lo, hi = shard_bounds(host_data, world)[rank]
+    part = device_partial(query, memoryview(host_data).cast("B")[lo:hi], fmt)
+    parts = gather(part, rank, world, group)
+    if rank != 0:
+        return None
+    return render(query, merge(parts), fmt)
