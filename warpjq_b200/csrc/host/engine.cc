@@ -19,6 +19,13 @@
 
 #include "../../../include/warpjq_ext.h"
 #include "../../../include/warpjq_host.h"
+
+// The extension entry points are optional: with a backend that exports only
+// the reference ABI (warpjq_kernels.h) the driver runs without them.
+#pragma weak warpjq_autotile
+#pragma weak warpjq_submit_host
+#pragma weak warpjq_host_is_pinned
+#pragma weak warpjq_slot_first_errors
 #include "query.h"
 
 namespace wjqh {
@@ -495,6 +502,11 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     warpjq_chunk_result r;
     warpjq_status rc = warpjq_wait(q->ctx, f.slot, &r, e, sizeof e);
     if (rc != WARPJQ_OK) return fail(std::string("CUDA error in waiting for a chunk: ") + e);
+    // A backend that leaves lines or groups to the host is not supported by
+    // this driver (this project's backend never does).
+    if (r.n_fallback || r.chunk_overflow || r.group_overflow)
+      return fail("the device backend left work to the host (fallback lines or an overflow), "
+                  "which this driver does not finish");
     uint64_t first_line = lines_seen + 1;
     lines_seen += r.n_lines;
     st_lines += r.n_lines - r.n_blank;
@@ -503,7 +515,7 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     if (on_invalid == WARPJQ_ON_INVALID_ABORT && (r.n_invalid || r.n_type_error)) {
       uint64_t fi = r.first_invalid == 0xFFFFFFFFu ? ~0ull : r.first_invalid;
       uint64_t ft = ~0ull, dummy = 0;
-      warpjq_slot_first_errors(q->ctx, f.slot, &dummy, &ft);
+      if (warpjq_slot_first_errors) warpjq_slot_first_errors(q->ctx, f.slot, &dummy, &ft);
       uint64_t bad = std::min(fi, ft);
       return fail("malformed JSON on line " + std::to_string(first_line + (bad == ~0ull ? 0 : bad)) +
                   " of <memory>: " + (fi <= ft ? "line is not valid JSON" : "a path hit a value of the wrong type") +
@@ -535,10 +547,12 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
 
   // Page-locked input is copied to the device straight from the caller's
   // memory; anything else is staged through the slots' pinned buffers.
-  const bool pinned = len && warpjq_host_is_pinned(data) && warpjq_host_is_pinned(data + len - 1);
+  const bool pinned = len && warpjq_host_is_pinned && warpjq_submit_host &&
+                      warpjq_host_is_pinned(data) && warpjq_host_is_pinned(data + len - 1);
   // Tiles sized from the input's own line lengths (first MiB of the run).
   if (!q->tiled && len) {
-    if (warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
+    if (warpjq_autotile &&
+        warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
         WARPJQ_OK)
       return fail("CUDA error in choosing the device tiling");
     q->tiled = true;
@@ -581,7 +595,8 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
       q->cap = n;
       if (warpjq_ctx_create(&q->low.prog, q->cap, q->n_slots, &q->ctx, e, sizeof e) != WARPJQ_OK)
         return fail(std::string("CUDA error in creating the device context: ") + e);
-      if (warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
+      if (warpjq_autotile &&
+          warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
           WARPJQ_OK)
         return fail("CUDA error in choosing the device tiling");
       next_slot = 0;
