@@ -118,7 +118,8 @@ class _DeviceBytes:
     """Device memory described for torch.as_tensor (no copy)."""
 
     def __init__(self, ptr: int, n: int):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, True),
+        # torch accepts only writable descriptions; the view is only read
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False),
                                          "version": 2}
 
 
