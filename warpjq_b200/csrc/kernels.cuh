@@ -1011,9 +1011,10 @@ __global__ void k_finalize(const double *block_f, const unsigned long long *bloc
 // Rows: prefix over the per-tile totals, then emission in line order.
 // ---------------------------------------------------------------------------
 
-constexpr uint32_t kEmitTiles = 128;  // tiles per block of the rows passes
-constexpr int kEmitThreads = 128;     // one thread per tile in the prefix step
-static_assert(kEmitTiles % kEmitThreads == 0, "emission sub-steps cover whole blocks");
+// Tiles per block of the rows passes: small, so a run of a few thousand
+// tiles still spreads its row copies over hundreds of blocks.
+constexpr uint32_t kEmitTiles = 32;
+constexpr int kEmitThreads = 128;
 
 // Exclusive block scan of three u64 values in thread order, with totals.
 __device__ __forceinline__ void block_scan3(const unsigned long long v[3], unsigned long long ex[3],
@@ -1113,7 +1114,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
     const unsigned long long t = t0 + sub + threadIdx.x;
     unsigned long long v[3] = {0, 0, 0};
     unsigned long long rec = 0;
-    if (t < ep.n_tiles) {
+    if (sub + threadIdx.x < kEmitTiles && t < ep.n_tiles) {
       const RowTile rt = ep.row_tiles[t];
       v[0] = rt.rows;
       v[1] = rt.bytes;
@@ -1126,7 +1127,8 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
     s_rec[threadIdx.x] = rec;
     s_rows[threadIdx.x] = (uint32_t)v[0];
     __syncthreads();
-    for (int i = warp; i < kEmitThreads; i += kEmitThreads / 32) {
+    const int n_here = (int)min((uint32_t)kEmitThreads, kEmitTiles - sub);
+    for (int i = warp; i < n_here; i += kEmitThreads / 32) {
       const uint32_t rows = s_rows[i];
       const unsigned long long row0 = s_pre[0][i], byte0 = s_pre[1][i], line0 = s_pre[2][i];
       for (uint32_t r = 0; r < rows; r++) {
