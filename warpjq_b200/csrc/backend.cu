@@ -304,7 +304,7 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       const unsigned nb = (unsigned)((n_tiles + kEmitTiles - 1) / kEmitTiles);
       k_rows_block_sums<<<nb, kEmitThreads, 0, st>>>(rb.row_tiles.p, rb.tiles.p, n_tiles,
                                                       rb.row_bsum.p);
-      k_rows_block_prefix<<<1, kEmitThreads, 0, st>>>(rb.row_bsum.p, nb, rb.ctr.p, rb.row_off.p,
+      k_rows_block_prefix<<<1, kPrefixThreads, 0, st>>>(rb.row_bsum.p, nb, rb.ctr.p, rb.row_off.p,
                                                       rb.rows_cap, rb.out_cap);
       EmitParams ep{};
       ep.data = d_data;

@@ -318,6 +318,36 @@ __device__ __forceinline__ void warp_copy(uint8_t *dst, const uint8_t *src, uint
   }
 }
 
+// Segment s of a value or projection row (JSON output): the value of the
+// single path, or prefix 0, value 0, prefix 1, value 1, ..., then the
+// suffix; the last segment is the newline.
+__device__ __forceinline__ const uint8_t *row_segment(const DevPlan &P, const uint8_t *line,
+                                                      const uint32_t *fields, uint32_t nf,
+                                                      uint32_t s, uint32_t &len) {
+  const bool proj = P.output_kind == 2;
+  const uint32_t n_before_suffix = proj ? 2 * nf : nf;
+  if (s < n_before_suffix) {
+    const uint32_t f = proj ? s >> 1 : s;
+    if (proj && !(s & 1)) {
+      len = P.prefix_len[f];
+      return P.blob + P.prefix_off[f];
+    }
+    const uint32_t off = fields[2 * f], lk = fields[2 * f + 1];
+    if ((lk >> 28) == JK_MISSING) {
+      len = 4;
+      return (const uint8_t *)"null";
+    }
+    len = lk & 0x07FFFFFFu;
+    return line + off;
+  }
+  if (proj && s == n_before_suffix) {
+    len = P.suffix_len;
+    return P.blob + P.suffix_off;
+  }
+  len = 1;
+  return (const uint8_t *)"\n";
+}
+
 // Writes one row.  All lanes of the warp call it together.
 __device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
                          const uint32_t *fields, uint8_t *dst, int lane) {
@@ -354,27 +384,34 @@ __device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
     dst[w] = '\n';
     return;
   }
-  uint32_t w = 0;
-  for (uint32_t f = 0; f < nf; f++) {
-    if (P.output_kind == 2) {
-      warp_copy(dst + w, P.blob + P.prefix_off[f], P.prefix_len[f], lane);
-      w += P.prefix_len[f];
+  // The row as a list of segments (value, or prefix/value pairs then the
+  // suffix, then the newline); lane l writes output bytes l, l+32, ...,
+  // finding each byte's segment with a cursor that only moves forward, and
+  // loads four bytes before storing them.
+  (void)kNull;
+  const uint32_t L = r.row_len;
+  uint32_t s = 0, soff = 0, slen;
+  const uint8_t *sp = row_segment(P, line, fields, nf, 0, slen);
+  for (uint32_t base = 0; base < L; base += 128) {
+    uint8_t bb[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t b = base + lane + 32 * k;
+      bb[k] = 0;
+      if (b < L) {
+        while (b >= soff + slen) {
+          soff += slen;
+          sp = row_segment(P, line, fields, nf, ++s, slen);
+        }
+        bb[k] = sp[b - soff];
+      }
     }
-    uint32_t off = fields[2 * f], lk = fields[2 * f + 1];
-    uint32_t kind = lk >> 28, len = lk & 0x07FFFFFFu;
-    if (kind == JK_MISSING) {
-      warp_copy(dst + w, kNull, 4, lane);
-      w += 4;
-    } else {
-      warp_copy(dst + w, line + off, len, lane);
-      w += len;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t b = base + lane + 32 * k;
+      if (b < L) dst[b] = bb[k];
     }
   }
-  if (P.output_kind == 2) {
-    warp_copy(dst + w, P.blob + P.suffix_off, P.suffix_len, lane);
-    w += P.suffix_len;
-  }
-  if (lane == 0) dst[w] = '\n';
 }
 
 // ---------------------------------------------------------------------------
@@ -1015,11 +1052,13 @@ __global__ void k_finalize(const double *block_f, const unsigned long long *bloc
 // tiles still spreads its row copies over hundreds of blocks.
 constexpr uint32_t kEmitTiles = 32;
 constexpr int kEmitThreads = 128;
+constexpr int kPrefixThreads = 1024;  // the one block that scans the block sums
 
 // Exclusive block scan of three u64 values in thread order, with totals.
+template <int NT>
 __device__ __forceinline__ void block_scan3(const unsigned long long v[3], unsigned long long ex[3],
                                             unsigned long long tot[3],
-                                            unsigned long long (*s_w)[kEmitThreads / 32]) {
+                                            unsigned long long (*s_w)[NT / 32]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long inc[3] = {v[0], v[1], v[2]};
 #pragma unroll
@@ -1035,7 +1074,7 @@ __device__ __forceinline__ void block_scan3(const unsigned long long v[3], unsig
   __syncthreads();
   for (int k = 0; k < 3; k++) {
     unsigned long long before = 0, all = 0;
-    for (int w = 0; w < kEmitThreads / 32; w++) {
+    for (int w = 0; w < NT / 32; w++) {
       if (w < warp) before += s_w[k][w];
       all += s_w[k][w];
     }
@@ -1061,7 +1100,7 @@ __global__ void __launch_bounds__(kEmitThreads)
     }
   }
   unsigned long long ex[3], tot[3];
-  block_scan3(v, ex, tot, s_w);
+  block_scan3<kEmitThreads>(v, ex, tot, s_w);
   if (threadIdx.x == 0)
     for (int k = 0; k < 3; k++) bsum[blockIdx.x * 3 + k] = tot[k];
 }
@@ -1069,18 +1108,18 @@ __global__ void __launch_bounds__(kEmitThreads)
 // Pass 2 (one block): block sums -> exclusive block prefixes, in place; the
 // totals give the output length and the closing row offset.  Output that
 // does not fit raises the overflow flag (the run is repeated with room).
-__global__ void __launch_bounds__(kEmitThreads)
+__global__ void __launch_bounds__(kPrefixThreads)
     k_rows_block_prefix(unsigned long long *bsum, unsigned nblocks, RunCounters *ctr,
                         unsigned long long *row_off, unsigned long long rows_cap,
                         unsigned long long out_cap) {
-  __shared__ unsigned long long s_w[3][kEmitThreads / 32];
-  const unsigned per = (nblocks + kEmitThreads - 1) / kEmitThreads;
+  __shared__ unsigned long long s_w[3][kPrefixThreads / 32];
+  const unsigned per = (nblocks + kPrefixThreads - 1) / kPrefixThreads;
   const unsigned b0 = threadIdx.x * per, b1 = min(b0 + per, nblocks);
   unsigned long long v[3] = {0, 0, 0};
   for (unsigned b = b0; b < b1; b++)
     for (int k = 0; k < 3; k++) v[k] += bsum[b * 3 + k];
   unsigned long long ex[3], tot[3];
-  block_scan3(v, ex, tot, s_w);
+  block_scan3<kPrefixThreads>(v, ex, tot, s_w);
   for (unsigned b = b0; b < b1; b++)
     for (int k = 0; k < 3; k++) {
       unsigned long long x = bsum[b * 3 + k];
@@ -1122,7 +1161,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
       rec = rt.rec_begin;
     }
     unsigned long long ex[3], tot[3];
-    block_scan3(v, ex, tot, s_w);
+    block_scan3<kEmitThreads>(v, ex, tot, s_w);
     for (int k = 0; k < 3; k++) s_pre[k][threadIdx.x] = carry[k] + ex[k];
     s_rec[threadIdx.x] = rec;
     s_rows[threadIdx.x] = (uint32_t)v[0];
