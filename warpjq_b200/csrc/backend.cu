@@ -222,7 +222,7 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n, char *er
   CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32)), "alloc deep stack");
   if (P.needs_rows) {
     CK(rb.row_tiles.ensure(n_tiles), "alloc row tiles");
-    CK(rb.row_bsum.ensure(3 * ((n_tiles + kEmitTiles - 1) / kEmitTiles)), "alloc row prefixes");
+    CK(rb.row_bsum.ensure(3 * ((n_tiles + 31) / 32)), "alloc row prefixes");
     // Records accumulate over all of a CTA's tiles: start with room for a
     // row per KiB of input, grown on overflow.
     if (!rb.rec_cap_per_cta) rb.rec_cap_per_cta = n / 1024 / std::max(1u, c->grid) + 1024;
@@ -301,8 +301,9 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     CK(cudaGetLastError(), "launch scan");
     CK(cudaEventRecord(s.scan_t1, st), "event record");
     if (P.needs_rows) {
-      const unsigned nb = (unsigned)((n_tiles + kEmitTiles - 1) / kEmitTiles);
-      k_rows_block_sums<<<nb, kEmitThreads, 0, st>>>(rb.row_tiles.p, rb.tiles.p, n_tiles,
+      const uint32_t tpb = rows_tiles_per_block(n_tiles);
+      const unsigned nb = (unsigned)((n_tiles + tpb - 1) / tpb);
+      k_rows_block_sums<<<nb, kEmitThreads, 0, st>>>(rb.row_tiles.p, rb.tiles.p, n_tiles, tpb,
                                                       rb.row_bsum.p);
       k_rows_block_prefix<<<1, kPrefixThreads, 0, st>>>(rb.row_bsum.p, nb, rb.ctr.p, rb.row_off.p,
                                                       rb.rows_cap, rb.out_cap);
@@ -313,6 +314,7 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       ep.tiles = rb.tiles.p;
       ep.n_tiles = n_tiles;
       ep.block_prefix = rb.row_bsum.p;
+      ep.tiles_per_block = tpb;
       ep.recs = rb.recs.p;
       ep.out = rb.out.p;
       ep.out_cap = rb.out_cap;

@@ -133,7 +133,8 @@ struct EmitParams {
   const RowTile *row_tiles;
   const TileDesc *tiles;
   unsigned long long n_tiles;
-  const unsigned long long *block_prefix;  // 3 per block of kEmitTiles tiles
+  const unsigned long long *block_prefix;  // 3 per block of tiles_per_block tiles
+  uint32_t tiles_per_block;
   const uint8_t *recs;
   uint8_t *out;
   unsigned long long out_cap;
@@ -351,7 +352,6 @@ __device__ __forceinline__ const uint8_t *row_segment(const DevPlan &P, const ui
 // Writes one row.  All lanes of the warp call it together.
 __device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
                          const uint32_t *fields, uint8_t *dst, int lane) {
-  const uint8_t *kNull = (const uint8_t *)"null";
   if (P.output_kind == 0) {
     if (!P.csv_mode) {
       warp_copy(dst, line, r.line_len, lane);
@@ -388,7 +388,6 @@ __device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
   // suffix, then the newline); lane l writes output bytes l, l+32, ...,
   // finding each byte's segment with a cursor that only moves forward, and
   // loads four bytes before storing them.
-  (void)kNull;
   const uint32_t L = r.row_len;
   uint32_t s = 0, soff = 0, slen;
   const uint8_t *sp = row_segment(P, line, fields, nf, 0, slen);
@@ -1048,10 +1047,13 @@ __global__ void k_finalize(const double *block_f, const unsigned long long *bloc
 // Rows: prefix over the per-tile totals, then emission in line order.
 // ---------------------------------------------------------------------------
 
-// Tiles per block of the rows passes: small, so a run of a few thousand
-// tiles still spreads its row copies over hundreds of blocks.
-constexpr uint32_t kEmitTiles = 32;
+// Tiles per block of the rows passes (a multiple of 32, chosen per run by
+// rows_tiles_per_block): small runs take 32 so their row copies still spread
+// over hundreds of blocks, large ones 128 for fewer, fuller blocks.
 constexpr int kEmitThreads = 128;
+__host__ __device__ inline uint32_t rows_tiles_per_block(unsigned long long n_tiles) {
+  return n_tiles < 148ull * 128 ? 32u : 128u;
+}
 constexpr int kPrefixThreads = 1024;  // the one block that scans the block sums
 
 // Exclusive block scan of three u64 values in thread order, with totals.
@@ -1084,14 +1086,14 @@ __device__ __forceinline__ void block_scan3(const unsigned long long v[3], unsig
   __syncthreads();
 }
 
-// Pass 1: (rows, bytes, lines) summed per block of kEmitTiles tiles.
+// Pass 1: (rows, bytes, lines) summed per block of `tpb` tiles.
 __global__ void __launch_bounds__(kEmitThreads)
     k_rows_block_sums(const RowTile *rt, const TileDesc *td, unsigned long long n_tiles,
-                      unsigned long long *bsum) {
+                      uint32_t tpb, unsigned long long *bsum) {
   __shared__ unsigned long long s_w[3][kEmitThreads / 32];
-  const unsigned long long t0 = (unsigned long long)blockIdx.x * kEmitTiles;
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * tpb;
   unsigned long long v[3] = {0, 0, 0};
-  for (uint32_t k = threadIdx.x; k < kEmitTiles; k += kEmitThreads) {
+  for (uint32_t k = threadIdx.x; k < tpb; k += kEmitThreads) {
     unsigned long long t = t0 + k;
     if (t < n_tiles) {
       v[0] += rt[t].rows;
@@ -1133,7 +1135,7 @@ __global__ void __launch_bounds__(kPrefixThreads)
   }
 }
 
-// Pass 3: each block takes its kEmitTiles tiles kEmitThreads at a time:
+// Pass 3: each block takes its `tiles_per_block` tiles kEmitThreads at a time:
 // per-tile prefixes by a block scan, then each warp copies whole tiles'
 // rows, one row at a time, from the input to the output.
 __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
@@ -1147,13 +1149,14 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
   const uint32_t rec_stride = P.rec_stride;
   unsigned long long carry[3];
   for (int k = 0; k < 3; k++) carry[k] = ep.block_prefix[blockIdx.x * 3 + k];
-  const unsigned long long t0 = (unsigned long long)blockIdx.x * kEmitTiles;
-  for (uint32_t sub = 0; sub < kEmitTiles; sub += kEmitThreads) {
+  const uint32_t tpb = ep.tiles_per_block;
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * tpb;
+  for (uint32_t sub = 0; sub < tpb; sub += kEmitThreads) {
     if (t0 + sub >= ep.n_tiles) break;
     const unsigned long long t = t0 + sub + threadIdx.x;
     unsigned long long v[3] = {0, 0, 0};
     unsigned long long rec = 0;
-    if (sub + threadIdx.x < kEmitTiles && t < ep.n_tiles) {
+    if (sub + threadIdx.x < tpb && t < ep.n_tiles) {
       const RowTile rt = ep.row_tiles[t];
       v[0] = rt.rows;
       v[1] = rt.bytes;
@@ -1166,7 +1169,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
     s_rec[threadIdx.x] = rec;
     s_rows[threadIdx.x] = (uint32_t)v[0];
     __syncthreads();
-    const int n_here = (int)min((uint32_t)kEmitThreads, kEmitTiles - sub);
+    const int n_here = (int)min((uint32_t)kEmitThreads, tpb - sub);
     for (int i = warp; i < n_here; i += kEmitThreads / 32) {
       const uint32_t rows = s_rows[i];
       const unsigned long long row0 = s_pre[0][i], byte0 = s_pre[1][i], line0 = s_pre[2][i];
