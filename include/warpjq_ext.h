@@ -111,6 +111,59 @@ warpjq_status warpjq_submit_host(warpjq_ctx *ctx, uint32_t slot, const uint8_t *
  * else 0.  No reference counterpart. */
 int warpjq_host_is_pinned(const void *p);
 
+/* One input's result within a batch (warpjq_batch_collect).  Line indexes
+ * are relative to the input. */
+typedef struct {
+  uint64_t n_lines;
+  uint64_t n_blank;
+  uint64_t n_invalid;
+  uint64_t n_type_error;
+  uint64_t n_selected;
+  uint64_t first_invalid;    /* lowest invalid line of the input, or UINT64_MAX */
+  uint64_t first_type_error; /* lowest line with a type error, or UINT64_MAX */
+  uint64_t row_begin;  /* the input's rows are rows [row_begin, row_begin + n_selected) of
+                        * the batch's rows (see warpjq_batch_collect's `all`) */
+  uint64_t line_begin; /* lines of the earlier inputs: subtract from the batch's line
+                        * indexes to get the input's own */
+  /* aggregate, as in warpjq_device_result */
+  uint64_t count;
+  uint64_t numeric;
+  uint64_t isum_lo;
+  uint64_t isum_hi;
+  uint64_t n_int;
+  double fsum;
+  double min;
+  double max;
+  double sum;
+  uint32_t saw_non_numeric;
+  uint32_t group_begin; /* the input's groups: all->groups[group_begin, + n_groups) */
+  uint32_t n_groups;
+  uint32_t _pad;
+} warpjq_batch_item;
+
+/* Batched device-resident run: the context's query over n_inputs separate
+ * inputs that are already in device memory, input i being
+ * d_data[offsets[i], offsets[i] + lengths[i]) (each start 16-byte aligned),
+ * in one launch sequence on `stream` with no host synchronisation.  Every
+ * input gets exactly the result a run over it alone would give; lines never
+ * continue from one input into the next.  Use it when many small inputs
+ * would each pay a run's fixed cost (launches, host round trip).  The
+ * inputs must stay in place until warpjq_batch_collect returns.  No
+ * reference counterpart. */
+warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const uint64_t *offsets,
+                                  const uint64_t *lengths, uint32_t n_inputs, void *stream,
+                                  char *err, size_t err_len);
+
+/* Waits for the batch (repeating it once with larger buffers if one
+ * overflowed) and fills items[0 .. n_inputs).  `all` (may be null) describes
+ * the whole batch: its rows in input order in device memory (d_out_bytes,
+ * d_out_row_off with n_selected + 1 entries, d_out_line_idx as batch line
+ * numbers), and every input's groups, ordered by input (key_off is an offset
+ * from d_data).  Pointers stay valid until the context's next device-resident
+ * run or batch.  No reference counterpart. */
+warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
+                                   warpjq_device_result *all, char *err, size_t err_len);
+
 /* Device-resident scan tunables: bytes per tile (one warp walks the lines
  * starting in a tile, one line per lane) and the halo staged after it (a line
  * that runs past tile + halo is walked from global memory, more slowly).

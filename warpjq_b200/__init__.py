@@ -35,6 +35,7 @@ ABI_SYMBOLS = [
 EXT_SYMBOLS = [
     "warpjq_launch_device", "warpjq_collect_device", "warpjq_slot_first_errors",
     "warpjq_set_tiling", "warpjq_autotile", "warpjq_submit_host", "warpjq_host_is_pinned",
+    "warpjq_batch_launch", "warpjq_batch_collect",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
@@ -77,6 +78,10 @@ def _load():
     k.warpjq_autotile.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(u32),
                                   ctypes.POINTER(u32)]
     k.warpjq_autotile.restype = ctypes.c_int
+    k.warpjq_batch_launch.argtypes = [vp, vp, ctypes.POINTER(u64), ctypes.POINTER(u64), u32, vp, cp, sz]
+    k.warpjq_batch_launch.restype = ctypes.c_int
+    k.warpjq_batch_collect.argtypes = [vp, vp, vp, cp, sz]
+    k.warpjq_batch_collect.restype = ctypes.c_int
     h.warpjq_query_open.argtypes = [cp, u32, u64, ctypes.POINTER(vp), cp, sz]
     h.warpjq_query_open.restype = ctypes.c_int
     h.warpjq_query_close.argtypes = [vp]
@@ -94,7 +99,7 @@ def _load():
     h.warpjq_run_bytes.argtypes = [cp, cp, sz, u32, u32, u64, u64, ctypes.POINTER(vp),
                                    ctypes.POINTER(sz), ctypes.POINTER(u64), cp, sz]
     h.warpjq_run_bytes.restype = ctypes.c_int
-    h.warpjq_query_render_device.argtypes = [vp, vp, cp, ctypes.POINTER(vp), ctypes.POINTER(sz)]
+    h.warpjq_query_render_device.argtypes = [vp, vp, vp, ctypes.POINTER(vp), ctypes.POINTER(sz)]
     h.warpjq_query_render_device.restype = ctypes.c_int
     h.warpjq_host_free.argtypes = [vp]
     h.warpjq_gen_nginx.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
@@ -195,6 +200,20 @@ class DeviceResult(ctypes.Structure):
     def isum(self) -> int:
         v = (self.isum_hi << 64) | self.isum_lo
         return v - (1 << 128) if self.isum_hi >> 63 else v
+
+
+class BatchItem(ctypes.Structure):
+    """Mirror of warpjq_batch_item (include/warpjq_ext.h)."""
+    _fields_ = [("n_lines", ctypes.c_uint64), ("n_blank", ctypes.c_uint64),
+                ("n_invalid", ctypes.c_uint64), ("n_type_error", ctypes.c_uint64),
+                ("n_selected", ctypes.c_uint64), ("first_invalid", ctypes.c_uint64),
+                ("first_type_error", ctypes.c_uint64), ("row_begin", ctypes.c_uint64),
+                ("line_begin", ctypes.c_uint64), ("count", ctypes.c_uint64),
+                ("numeric", ctypes.c_uint64), ("isum_lo", ctypes.c_uint64),
+                ("isum_hi", ctypes.c_uint64), ("n_int", ctypes.c_uint64), ("fsum", ctypes.c_double),
+                ("min", ctypes.c_double), ("max", ctypes.c_double), ("sum", ctypes.c_double),
+                ("saw_non_numeric", ctypes.c_uint32), ("group_begin", ctypes.c_uint32),
+                ("n_groups", ctypes.c_uint32), ("_pad", ctypes.c_uint32)]
 
 
 class Query:
@@ -303,10 +322,75 @@ class Query:
             raise RuntimeError(err.value.decode(errors="replace"))
         return r
 
-    def render_device(self, r: DeviceResult, host_data: bytes) -> bytes:
+    def batch_launch(self, d_ptr: int, offsets, lengths, stream: int = 0):
+        """Enqueues one batched run over the device inputs
+        d_ptr[offsets[i], offsets[i] + lengths[i]) (16-byte aligned starts)."""
+        k, _ = _load()
+        n = len(offsets)
+        self._b_off = (ctypes.c_uint64 * max(1, n))(*offsets)
+        self._b_len = (ctypes.c_uint64 * max(1, n))(*lengths)
+        self._b_n = n
+        err = ctypes.create_string_buffer(1024)
+        rc = k.warpjq_batch_launch(self.ctx, ctypes.c_void_p(d_ptr), self._b_off, self._b_len, n,
+                                   ctypes.c_void_p(stream), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+
+    def batch_collect(self):
+        """(items, all): one BatchItem per input, and the batch's
+        DeviceResult (rows and groups of every input)."""
+        k, _ = _load()
+        items = (BatchItem * max(1, self._b_n))()
+        all_ = DeviceResult()
+        err = ctypes.create_string_buffer(1024)
+        rc = k.warpjq_batch_collect(self.ctx, items, ctypes.byref(all_), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+        return list(items)[: self._b_n], all_
+
+    def batch_outputs(self, items, all_: DeviceResult, host_data) -> list:
+        """Each input's output bytes (what a run over it alone prints):
+        rows are cut from one copy of the batch's rows, aggregates and groups
+        rendered by the host formatter; `host_data` is the host copy of the
+        batch buffer (group keys are read from it)."""
+        import numpy as np
+        rows = b""
+        row_off = None
+        if all_.n_selected:
+            import torch
+            from .shard import _DeviceBytes
+            nsel = all_.n_selected
+            rows = torch.as_tensor(_DeviceBytes(all_.d_out_bytes, all_.out_len), device="cuda").cpu().numpy().tobytes()
+            ro = torch.as_tensor(_DeviceBytes(all_.d_out_row_off, (nsel + 1) * 8), device="cuda").cpu()
+            row_off = np.frombuffer(ro.numpy().tobytes(), dtype=np.uint64)
+        outs = []
+        for it in items:
+            r = DeviceResult()
+            for f in ("n_lines", "n_blank", "n_invalid", "n_type_error", "n_selected", "count", "numeric",
+                      "isum_lo", "isum_hi", "n_int", "fsum", "min", "max", "sum", "saw_non_numeric"):
+                setattr(r, f, getattr(it, f))
+            if it.n_groups:
+                r.groups = ctypes.cast(ctypes.byref(all_.groups[it.group_begin]), ctypes.POINTER(_GroupExt))
+                r.n_groups = it.n_groups
+            head = self.render_device(r, host_data)
+            body = b""
+            if it.n_selected and row_off is not None:
+                a, b = int(row_off[it.row_begin]), int(row_off[it.row_begin + it.n_selected])
+                body = rows[a:b]
+            outs.append(head + body)
+        return outs
+
+    def render_device(self, r: DeviceResult, host_data) -> bytes:
+        """Formats a device-resident result; `host_data` (bytes or a numpy
+        uint8 array) is the host copy of the input, for group keys."""
         out = ctypes.c_void_p()
         n = ctypes.c_size_t()
-        self._h.warpjq_query_render_device(self._q, ctypes.byref(r), host_data, ctypes.byref(out),
+        if isinstance(host_data, (bytes, bytearray)):
+            keep = ctypes.c_char_p(bytes(host_data))
+            addr = ctypes.cast(keep, ctypes.c_void_p)
+        else:
+            addr = ctypes.c_void_p(host_data.ctypes.data)
+        self._h.warpjq_query_render_device(self._q, ctypes.byref(r), addr, ctypes.byref(out),
                                            ctypes.byref(n))
         return _take(out, n)
 

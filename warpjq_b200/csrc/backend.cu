@@ -68,6 +68,11 @@ struct RunBufs {
   DevBuf<TileDesc> tiles;
   DevBuf<RowTile> row_tiles;
   DevBuf<unsigned long long> row_bsum;
+  // batched runs: tile -> input table, inputs' extents and first tiles, and
+  // one counter record per input
+  DevBuf<uint32_t> b_tile_input;
+  DevBuf<unsigned long long> b_in_start, b_in_end, b_in_tile0;
+  DevBuf<RunCounters> b_in_ctr;
   DevBuf<uint8_t> recs;
   DevBuf<uint8_t> out;
   DevBuf<unsigned long long> row_off, line_idx;
@@ -90,6 +95,8 @@ struct RunBufs {
 
   void release() {
     ctr.release(); tiles.release(); row_tiles.release(); row_bsum.release();
+    b_tile_input.release(); b_in_start.release(); b_in_end.release(); b_in_tile0.release();
+    b_in_ctr.release();
     recs.release(); out.release(); row_off.release(); line_idx.release(); tile_fsum.release();
     block_f.release(); block_lines.release(); deep.release(); g_slots.release();
     g_keys.release(); g_acc.release();
@@ -172,6 +179,18 @@ struct warpjq_ctx {
   unsigned long long dev_n = 0;
   cudaStream_t dev_stream = nullptr;
   std::vector<warpjq_group_ext> dev_groups;
+  // batched runs (warpjq_batch_launch): host copies of the tables
+  struct Batch {
+    bool active = false;
+    const uint8_t *d_data = nullptr;
+    cudaStream_t stream = nullptr;
+    unsigned long long n_tiles = 0, total = 0;
+    std::vector<unsigned long long> start, end, tile0;
+    std::vector<uint32_t> tile_input;
+    std::vector<RunCounters> h_ctr;
+    std::vector<warpjq_group_ext> groups;
+    std::vector<uint32_t> group_input;
+  } batch;
 };
 
 namespace {
@@ -207,11 +226,10 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
 }
 
 // Sizes the buffers of `s` for an input of n bytes (first use, or growth).
-warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n, char *err,
-                          size_t err_len) {
+warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
+                          unsigned long long n_tiles, char *err, size_t err_len) {
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
-  unsigned long long n_tiles = (n + c->tile_bytes - 1) / c->tile_bytes;
   if (n_tiles == 0) n_tiles = 1;
   CK(rb.ctr.ensure(1), "alloc counters");
   CK(rb.tiles.ensure(n_tiles), "alloc tiles");
@@ -257,20 +275,44 @@ GroupTable group_view(RunBufs &rb, bool on) {
 }
 
 // Enqueues one run over n bytes at d_data on `st`.  No host synchronisation.
+// With `b`, the run is a batch: n is the inputs' total size and the tiles
+// come from the batch's tables.
 warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigned long long n,
-                          cudaStream_t st, char *err, size_t err_len) {
-  warpjq_status rc = ensure_bufs(c, s, n, err, err_len);
+                          cudaStream_t st, char *err, size_t err_len,
+                          const warpjq_ctx::Batch *b = nullptr) {
+  const unsigned long long n_tiles = b ? b->n_tiles : (n + c->tile_bytes - 1) / c->tile_bytes;
+  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, err, err_len);
   if (rc != WARPJQ_OK) return rc;
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
   bool groups = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
-  unsigned long long n_tiles = (n + c->tile_bytes - 1) / c->tile_bytes;
+  const uint32_t n_inputs = b ? (uint32_t)b->start.size() : 0;
+  if (b) {
+    CK(rb.b_in_start.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
+    CK(rb.b_in_end.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
+    CK(rb.b_in_tile0.ensure(n_inputs + 1), "alloc batch tables");
+    CK(rb.b_in_ctr.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
+    CK(rb.b_tile_input.ensure(std::max<unsigned long long>(n_tiles, 1)), "alloc batch tables");
+    // pageable sources: staged by the driver before the calls return
+    CK(cudaMemcpyAsync(rb.b_in_start.p, b->start.data(), n_inputs * 8ull, cudaMemcpyHostToDevice, st),
+       "H2D batch tables");
+    CK(cudaMemcpyAsync(rb.b_in_end.p, b->end.data(), n_inputs * 8ull, cudaMemcpyHostToDevice, st),
+       "H2D batch tables");
+    CK(cudaMemcpyAsync(rb.b_in_tile0.p, b->tile0.data(), (n_inputs + 1) * 8ull,
+                       cudaMemcpyHostToDevice, st),
+       "H2D batch tables");
+    if (n_tiles)
+      CK(cudaMemcpyAsync(rb.b_tile_input.p, b->tile_input.data(), n_tiles * 4ull,
+                         cudaMemcpyHostToDevice, st),
+         "H2D batch tables");
+    if (n_inputs) k_batch_reset<<<(n_inputs + 255) / 256, 256, 0, st>>>(rb.b_in_ctr.p, n_inputs);
+  }
   GroupTable g = group_view(rb, groups);
   s.kernels = 0;
   k_reset_run<<<256, 256, 0, st>>>(rb.ctr.p, g, groups ? rb.g_cap : 0, groups ? rb.g_key_cap : 0);
   s.kernels++;
   CK(cudaGetLastError(), "launch reset");
-  if (n > 0) {
+  if (n > 0 && n_tiles > 0) {
     ScanParams sp{};
     sp.data = d_data;
     sp.n = n;
@@ -287,6 +329,13 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.g = g;
     sp.deep_words = rb.deep.p;
     sp.deep_levels_per_cta = rb.deep_levels;
+    if (b) {
+      sp.tile_input = rb.b_tile_input.p;
+      sp.in_start = rb.b_in_start.p;
+      sp.in_end = rb.b_in_end.p;
+      sp.in_tile0 = rb.b_in_tile0.p;
+      sp.in_ctr = rb.b_in_ctr.p;
+    }
     unsigned grid = (unsigned)std::min<unsigned long long>(c->grid, n_tiles);
     if (!s.scan_t0) {
       CK(cudaEventCreate(&s.scan_t0), "event");
@@ -335,6 +384,13 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
                                  rb.ctr.p);
     s.kernels++;
     CK(cudaGetLastError(), "launch finalize");
+    if (b && n_inputs) {
+      k_batch_finalize<<<(n_inputs + 7) / 8, 256, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
+                                                          rb.tiles.p, rb.b_in_tile0.p, rb.b_in_ctr.p,
+                                                          n_inputs);
+      s.kernels++;
+      CK(cudaGetLastError(), "launch batch finalize");
+    }
   }
   s.launched = true;
   return WARPJQ_OK;
@@ -384,10 +440,11 @@ bool grow_after_overflow(warpjq_ctx *c, Slot &s, const RunCounters &h, unsigned 
 // Runs synchronously until the result is complete; leaves counters in h.
 warpjq_status run_to_completion(warpjq_ctx *c, Slot &s, const uint8_t *d_data,
                                 unsigned long long n, cudaStream_t st, RunCounters &h,
-                                bool already_enqueued, char *err, size_t err_len) {
+                                bool already_enqueued, char *err, size_t err_len,
+                                const warpjq_ctx::Batch *b = nullptr) {
   for (int attempt = 0; attempt < 16; attempt++) {
     if (!already_enqueued || attempt > 0) {
-      warpjq_status rc = enqueue_run(c, s, d_data, n, st, err, err_len);
+      warpjq_status rc = enqueue_run(c, s, d_data, n, st, err, err_len, b);
       if (rc != WARPJQ_OK) return rc;
     }
     CK(cudaMemcpyAsync(&h, s.rb.ctr.p, sizeof(RunCounters), cudaMemcpyDeviceToHost, st),
@@ -485,7 +542,8 @@ warpjq_status warpjq_ctx_create(const warpjq_program *prog, uint64_t max_chunk_b
     CK(cudaMalloc((void **)&s.d_chunk, max_chunk_bytes + 16), "device chunk");
     CK(cudaHostAlloc((void **)&s.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
     if (max_chunk_bytes) {
-      rc = ensure_bufs(c.get(), s, max_chunk_bytes, err, err_len);
+      rc = ensure_bufs(c.get(), s, max_chunk_bytes,
+                       (max_chunk_bytes + c->tile_bytes - 1) / c->tile_bytes, err, err_len);
       if (rc != WARPJQ_OK) return rc;
     }
   }
@@ -606,8 +664,10 @@ static warpjq_status ensure_pinned(Slot &s, size_t out_bytes, size_t rows, size_
 
 // Copies the compacted group table of a finished run to the host.
 static warpjq_status fetch_groups(warpjq_ctx *ctx, Slot &s, const RunCounters &h,
-                                  std::vector<warpjq_group_ext> &out, char *err, size_t err_len) {
+                                  std::vector<warpjq_group_ext> &out, char *err, size_t err_len,
+                                  std::vector<uint32_t> *inputs = nullptr) {
   out.clear();
+  if (inputs) inputs->clear();
   uint32_t nk = std::min<uint32_t>(h.n_keys, s.rb.g_key_cap);
   if (!nk) return WARPJQ_OK;
   std::vector<GroupKeyDesc> keys(nk);
@@ -634,6 +694,7 @@ static warpjq_status fetch_groups(warpjq_ctx *ctx, Slot &s, const RunCounters &h
     g.max = a.numeric ? from_order_bits(a.max_bits) : -1.0 / 0.0;
     g.sum = (a.n_int ? i128_to_double(a.isum_lo, a.isum_hi) : 0.0) + a.fsum;
     out.push_back(g);
+    if (inputs) inputs->push_back(keys[k].input);
   }
   (void)ctx;
   return WARPJQ_OK;
@@ -841,6 +902,127 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
   if (s.scan_t0 && ctx->dev_n) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, s.scan_t0, s.scan_t1) == cudaSuccess) out->scan_ms = ms;
+  }
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const uint64_t *offsets,
+                                  const uint64_t *lengths, uint32_t n_inputs, void *stream,
+                                  char *err, size_t err_len) {
+  if (!ctx || (n_inputs && (!d_data || !offsets || !lengths))) return WARPJQ_ERR_INVALID_ARG;
+  warpjq_ctx::Batch &b = ctx->batch;
+  b.active = false;
+  b.d_data = d_data;
+  b.stream = (cudaStream_t)stream;
+  b.start.resize(n_inputs);
+  b.end.resize(n_inputs);
+  b.tile0.resize(n_inputs + 1);
+  b.tile_input.clear();
+  b.total = 0;
+  const unsigned long long T = ctx->tile_bytes;
+  unsigned long long tiles = 0;
+  for (uint32_t i = 0; i < n_inputs; i++) {
+    if (((uintptr_t)(d_data + offsets[i]) & 15u) != 0) {
+      set_err(err, err_len, "batch input %u does not start on a 16-byte boundary", i);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+    b.start[i] = offsets[i];
+    b.end[i] = offsets[i] + lengths[i];
+    b.tile0[i] = tiles;
+    const unsigned long long nt = (lengths[i] + T - 1) / T;
+    b.tile_input.insert(b.tile_input.end(), nt, i);
+    tiles += nt;
+    b.total += lengths[i];
+  }
+  b.tile0[n_inputs] = tiles;
+  b.n_tiles = tiles;
+  warpjq_status rc = enqueue_run(ctx, ctx->dev, d_data, b.total, b.stream, err, err_len, &b);
+  if (rc == WARPJQ_OK) b.active = true;
+  return rc;
+}
+
+warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
+                                   warpjq_device_result *all, char *err, size_t err_len) {
+  if (!ctx || !ctx->batch.active) return WARPJQ_ERR_INVALID_ARG;
+  warpjq_ctx::Batch &b = ctx->batch;
+  Slot &s = ctx->dev;
+  RunCounters h;
+  warpjq_status rc =
+      run_to_completion(ctx, s, b.d_data, b.total, b.stream, h, true, err, err_len, &b);
+  if (rc != WARPJQ_OK) return rc;
+  const uint32_t n = (uint32_t)b.start.size();
+  b.h_ctr.resize(std::max<uint32_t>(n, 1));
+  if (n)
+    CK(cudaMemcpy(b.h_ctr.data(), s.rb.b_in_ctr.p, n * sizeof(RunCounters), cudaMemcpyDeviceToHost),
+       "D2H batch counters");
+  const DevPlan &P = ctx->plan;
+  const bool grouped = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
+  // Groups ordered by input (stable within an input).
+  std::vector<uint32_t> first(n + 1, 0);
+  if (grouped) {
+    std::vector<warpjq_group_ext> gs;
+    std::vector<uint32_t> gin;
+    rc = fetch_groups(ctx, s, h, gs, err, err_len, &gin);
+    if (rc != WARPJQ_OK) return rc;
+    for (uint32_t in : gin) first[in + 1]++;
+    for (uint32_t i = 0; i < n; i++) first[i + 1] += first[i];
+    b.groups.assign(gs.size(), warpjq_group_ext{});
+    std::vector<uint32_t> fill(first.begin(), first.end() - 1);
+    for (size_t k = 0; k < gs.size(); k++) b.groups[fill[gin[k]]++] = gs[k];
+  } else {
+    b.groups.clear();
+  }
+  unsigned long long rows = 0, lines = 0;
+  for (uint32_t i = 0; i < n && items; i++) {
+    const RunCounters &c = b.h_ctr[i];
+    warpjq_batch_item &it = items[i];
+    std::memset(&it, 0, sizeof(it));
+    it.n_lines = c.n_lines;
+    it.n_blank = c.n_blank;
+    it.n_invalid = c.n_invalid;
+    it.n_type_error = c.n_type_error;
+    it.n_selected = P.output_kind == WARPJQ_OUT_AGG ? 0 : c.n_selected;
+    it.first_invalid = c.first_invalid;
+    it.first_type_error = c.first_type_error;
+    it.row_begin = rows;
+    it.line_begin = lines;
+    rows += it.n_selected;
+    lines += c.n_lines;
+    it.count = c.agg_count;
+    it.numeric = c.agg_numeric;
+    it.isum_lo = c.agg_isum_lo;
+    it.isum_hi = c.agg_isum_hi;
+    it.n_int = c.agg_n_int;
+    it.fsum = c.fsum_total;
+    it.min = c.agg_numeric ? from_order_bits(c.agg_min_bits) : 1.0 / 0.0;
+    it.max = c.agg_numeric ? from_order_bits(c.agg_max_bits) : -1.0 / 0.0;
+    it.sum = (c.agg_n_int ? i128_to_double(c.agg_isum_lo, c.agg_isum_hi) : 0.0) + c.fsum_total;
+    it.saw_non_numeric = c.agg_saw_non_numeric;
+    it.group_begin = first[i];
+    it.n_groups = first[i + 1] - first[i];
+  }
+  if (all) {
+    std::memset(all, 0, sizeof(*all));
+    all->n_lines = h.n_lines;
+    all->n_blank = h.n_blank;
+    all->n_invalid = h.n_invalid;
+    all->n_type_error = h.n_type_error;
+    all->n_selected = h.n_selected;
+    all->first_invalid = ~0ull;
+    all->first_type_error = ~0ull;
+    if (P.needs_rows) {
+      all->d_out_bytes = s.rb.out.p;
+      all->out_len = h.out_len;
+      all->d_out_line_idx = (const uint64_t *)s.rb.line_idx.p;
+      all->d_out_row_off = (const uint64_t *)s.rb.row_off.p;
+    }
+    all->groups = b.groups.data();
+    all->n_groups = (uint32_t)b.groups.size();
+    all->kernels_launched = s.kernels;
+    if (s.scan_t0 && b.total) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, s.scan_t0, s.scan_t1) == cudaSuccess) all->scan_ms = ms;
+    }
   }
   return WARPJQ_OK;
 }

@@ -69,12 +69,13 @@ static_assert(sizeof(GroupAcc) == 64, "group accumulator record");
 struct GroupKeyDesc {
   unsigned long long off;  // absolute input offset of the key bytes (string: body)
   uint32_t len;
+  uint32_t input;           // batch input the key belongs to (0 for one input)
   uint8_t kind;
   uint8_t esc;
   uint8_t saw_non_numeric;  // a selected line had a non-numeric, non-null value
-  uint8_t pad;
+  uint8_t pad[5];
 };
-static_assert(sizeof(GroupKeyDesc) == 16, "group key descriptor");
+static_assert(sizeof(GroupKeyDesc) == 24, "group key descriptor");
 
 // A CTA's private accumulators for up to kGroupCache keys (direct-mapped by
 // key id), merged into the global records when the CTA finishes.  Hot keys
@@ -124,6 +125,14 @@ struct ScanParams {
   // deep-nesting scratch, per CTA
   uint32_t *deep_words;
   unsigned long long deep_levels_per_cta;
+  // Batched runs (tile_input null for one input): input i is
+  // data[in_start[i], in_end[i]) and owns tiles [in_tile0[i], in_tile0[i+1]);
+  // its counters and aggregate go to in_ctr[i].
+  const uint32_t *tile_input;
+  const unsigned long long *in_start;
+  const unsigned long long *in_end;
+  const unsigned long long *in_tile0;
+  RunCounters *in_ctr;
 };
 
 // Rows emission.
@@ -155,6 +164,7 @@ struct KeyRef {
   uint32_t len;
   uint8_t kind;      // JK_NULL for missing/null keys
   uint8_t esc;
+  uint32_t input;    // batch input of the line (keys of different inputs differ)
   unsigned long long abs_off;
 };
 
@@ -189,13 +199,12 @@ __device__ uint32_t group_find_or_insert(const ScanParams &sp, const KeyRef &k, 
           atomicOr(&sp.ctr->overflow, 4u);
           return 0xFFFFFFFFu;
         }
-        GroupKeyDesc d;
+        GroupKeyDesc d = {};
         d.off = k.abs_off;
         d.len = k.len;
+        d.input = k.input;
         d.kind = k.kind;
         d.esc = k.esc;
-        d.saw_non_numeric = 0;
-        d.pad = 0;
         g.keys[mine] = d;
         __threadfence();
       }
@@ -208,7 +217,8 @@ __device__ uint32_t group_find_or_insert(const ScanParams &sp, const KeyRef &k, 
       uint32_t kid = (uint32_t)w - 1;
       __threadfence();
       const GroupKeyDesc d = g.keys[kid];
-      if (d.kind == k.kind && key_bytes_equal(k, sp.data + d.off, d.len, d.esc)) return kid;
+      if (d.kind == k.kind && d.input == k.input && key_bytes_equal(k, sp.data + d.off, d.len, d.esc))
+        return kid;
     }
     pos = (pos + 1) & g.cap_mask;
   }
@@ -474,6 +484,64 @@ __device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uin
   tb = __shfl_sync(0xffffffffu, ib, 31);
 }
 
+// Adds the warp's counts and (ungrouped) aggregate to `dst` and clears them.
+__device__ __noinline__ void flush_counts(RunCounters *dst, const DevPlan &P, bool rows, int lane,
+                                             unsigned long long &c_lines, unsigned long long &c_blank,
+                                             unsigned long long &c_invalid, unsigned long long &c_type,
+                                             unsigned long long &c_sel, ThreadAgg &agg) {
+  const unsigned long long nl = warp_sum_u64(c_lines), nb = warp_sum_u64(c_blank),
+                           ni = warp_sum_u64(c_invalid), nt = warp_sum_u64(c_type),
+                           ns = warp_sum_u64(c_sel);
+  if (lane == 0) {
+    if (nl) atomicAdd(&dst->n_lines, nl);
+    if (nb) atomicAdd(&dst->n_blank, nb);
+    if (ni) atomicAdd(&dst->n_invalid, ni);
+    if (nt) atomicAdd(&dst->n_type_error, nt);
+    if (ns) atomicAdd(&dst->n_selected, ns);
+  }
+  c_lines = c_blank = c_invalid = c_type = c_sel = 0;
+  if (!rows && P.group_slot < 0 && P.output_kind == 3) {
+    const unsigned long long cnt = warp_sum_u64(agg.count), num = warp_sum_u64(agg.numeric),
+                             nint = warp_sum_u64(agg.n_int);
+    // 128-bit sums: reduce the low words with carry counting, per lane pair
+    unsigned long long lo = agg.isum_lo, hi = agg.isum_hi;
+    for (int d = 16; d > 0; d >>= 1) {
+      const unsigned long long olo = __shfl_down_sync(0xffffffffu, lo, d);
+      const unsigned long long ohi = __shfl_down_sync(0xffffffffu, hi, d);
+      if (lane + d < 32) {
+        const unsigned long long sum = lo + olo;
+        hi += ohi + (sum < lo);
+        lo = sum;
+      }
+    }
+    unsigned long long mn = agg.min_bits, mx = agg.max_bits;
+    for (int d = 16; d > 0; d >>= 1) {
+      mn = min(mn, __shfl_down_sync(0xffffffffu, mn, d));
+      mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
+    }
+    const unsigned int saw = __any_sync(0xffffffffu, agg.saw);
+    if (lane == 0) {
+      if (cnt) atomicAdd(&dst->agg_count, cnt);
+      if (num) atomicAdd(&dst->agg_numeric, num);
+      if (nint) atomicAdd(&dst->agg_n_int, nint);
+      if (lo || hi) {
+        const unsigned long long old = atomicAdd(&dst->agg_isum_lo, lo);
+        const unsigned long long carry = (old + lo) < old;
+        if (hi + carry) atomicAdd(&dst->agg_isum_hi, hi + carry);
+      }
+      if (num) {
+        atomicMin(&dst->agg_min_bits, mn);
+        atomicMax(&dst->agg_max_bits, mx);
+      }
+      if (saw) atomicOr(&dst->agg_saw_non_numeric, 1u);
+    }
+  } else if (!rows) {
+    const unsigned int saw = __any_sync(0xffffffffu, agg.saw);
+    if (lane == 0 && saw) atomicOr(&dst->agg_saw_non_numeric, 1u);
+  }
+  agg.init();
+}
+
 // Natural-order newline mask of window chunk c (bytes 32c .. 32c+31); bytes
 // at or past `wlen` do not count.  A cheap has-a-newline test runs first;
 // the exact per-byte flags are worked out only for chunks holding one.
@@ -559,17 +627,28 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
     const unsigned long long tile = __shfl_sync(0xffffffffu, next_ticket, 0);
     if (tile >= sp.n_tiles) break;
     if (lane == 0) next_ticket = atomicAdd(&sp.ctr->next_tile, 1ull);
-    const unsigned long long ts = tile * T;
-    const unsigned long long te = min(ts + T, sp.n);
+    // The tile's input: the whole data, or one input of a batch (a window
+    // never reaches past its input's end).
+    uint32_t input = 0;
+    unsigned long long data_start = 0, data_end = sp.n, ts = tile * T;
+    RunCounters *ctr_in = sp.ctr;
+    if (sp.tile_input) {
+      input = sp.tile_input[tile];
+      data_start = sp.in_start[input];
+      data_end = sp.in_end[input];
+      ts = data_start + (tile - sp.in_tile0[input]) * T;
+      ctr_in = sp.in_ctr + input;
+    }
+    const unsigned long long te = min(ts + T, data_end);
     const uint32_t tlen = (uint32_t)(te - ts);
-    const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, sp.n - ts);
-    const bool win_reaches_end = ts + wlen == sp.n;
+    const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, data_end - ts);
+    const bool win_reaches_end = ts + wlen == data_end;
 
     // 1. Stage tile + halo with asynchronous 16-byte copies.
     const uint32_t n16 = (wlen + 15) >> 4;
     for (uint32_t k = lane; k < n16; k += 32)
       cp_async16(win + k * 16, sp.data + ts + k * 16, min(16u, wlen - k * 16));
-    const uint32_t prev_nl = (ts == 0 || sp.data[ts - 1] == '\n') ? 1u : 0u;
+    const uint32_t prev_nl = (ts == data_start || sp.data[ts - 1] == '\n') ? 1u : 0u;
     cp_async_wait_all();
     __syncwarp();
 
@@ -675,7 +754,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
           } else {
             // longer than the window: walk it from global memory
             unsigned long long q = ts + wlen;
-            while (q < sp.n && sp.data[q] != '\n') q++;
+            while (q < data_end && sp.data[q] != '\n') q++;
             lp = sp.data + line_abs;
             line_len = (uint32_t)(q - line_abs);
             status = walk_line(P, lp, line_len, nv, nullptr);
@@ -738,6 +817,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
               const SlotVal &g = slots[P.group_slot];
               has_group = true;
               gk.esc = 0;
+              gk.input = input;
               if (g.kind == JK_MISSING || g.kind == JK_NULL) {
                 gk.kind = JK_NULL;
                 gk.p = lp;
@@ -756,7 +836,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
                 gk.abs_off = line_abs + g.off;
               }
               gh = (gk.kind == JK_STR ? hash_str_body(gk.p, gk.len, gk.esc) : hash_raw(gk.p, gk.len)) ^
-                   (gk.kind * 0x9E3779B9u);
+                   (gk.kind * 0x9E3779B9u) ^ (input * 0x85EBCA6Bu);
               if (gh == 0) gh = 1;
             }
           }
@@ -801,7 +881,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
           const uint32_t llen = __shfl_sync(0xffffffffu, gk.len, leader);
           const uint32_t lkind = __shfl_sync(0xffffffffu, (uint32_t)gk.kind, leader);
           const uint32_t lesc = __shfl_sync(0xffffffffu, (uint32_t)gk.esc, leader);
-          const bool same = has_group && lane != leader && gk.kind == lkind &&
+          const uint32_t linput = __shfl_sync(0xffffffffu, input, leader);
+          const bool same = has_group && lane != leader && gk.kind == lkind && input == linput &&
                             key_bytes_equal(gk, (const uint8_t *)lp, llen, (uint8_t)lesc);
           uint32_t kid = 0xFFFFFFFFu;
           if (has_group && !same) kid = group_find_or_insert(sp, gk, gh);
@@ -879,8 +960,14 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
       sp.tiles[tile].n_lines = n_lines_tile;
       sp.tiles[tile].first_invalid = tile_first_invalid;
       sp.tiles[tile].first_type_error = tile_first_type;
-      if (tile_first_invalid != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_invalid_tile, tile);
-      if (tile_first_type != 0xFFFFFFFFu) atomicMin(&sp.ctr->first_type_tile, tile);
+      if (tile_first_invalid != 0xFFFFFFFFu) {
+        atomicMin(&sp.ctr->first_invalid_tile, tile);
+        if (sp.tile_input) atomicMin(&ctr_in->first_invalid_tile, tile);
+      }
+      if (tile_first_type != 0xFFFFFFFFu) {
+        atomicMin(&sp.ctr->first_type_tile, tile);
+        if (sp.tile_input) atomicMin(&ctr_in->first_type_tile, tile);
+      }
     }
     if (kRows) {
       if (lane == 0) {
@@ -898,6 +985,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
       for (int d = 16; d > 0; d >>= 1) f += __shfl_down_sync(0xffffffffu, f, d);
       if (lane == 0) sp.tile_fsum[tile] = f;
     }
+    // A batch input's counts and aggregate go to its own record, tile by tile.
+    if (sp.tile_input) flush_counts(ctr_in, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
@@ -924,58 +1013,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
     }
   }
 
-  // Flush this CTA's counters.
-  c_lines = warp_sum_u64(c_lines);
-  c_blank = warp_sum_u64(c_blank);
-  c_invalid = warp_sum_u64(c_invalid);
-  c_type = warp_sum_u64(c_type);
-  c_sel = warp_sum_u64(c_sel);
-  if (lane == 0) {
-    if (c_lines) atomicAdd(&sp.ctr->n_lines, c_lines);
-    if (c_blank) atomicAdd(&sp.ctr->n_blank, c_blank);
-    if (c_invalid) atomicAdd(&sp.ctr->n_invalid, c_invalid);
-    if (c_type) atomicAdd(&sp.ctr->n_type_error, c_type);
-    if (c_sel) atomicAdd(&sp.ctr->n_selected, c_sel);
-  }
-  if (!kRows && P.group_slot < 0 && P.output_kind == 3) {
-    unsigned long long cnt = warp_sum_u64(agg.count), num = warp_sum_u64(agg.numeric),
-                       ni = warp_sum_u64(agg.n_int);
-    // 128-bit sums: reduce the low words with carry counting, per lane pair
-    unsigned long long lo = agg.isum_lo, hi = agg.isum_hi;
-    for (int d = 16; d > 0; d >>= 1) {
-      unsigned long long olo = __shfl_down_sync(0xffffffffu, lo, d);
-      unsigned long long ohi = __shfl_down_sync(0xffffffffu, hi, d);
-      if (lane + d < 32) {
-        unsigned long long s = lo + olo;
-        hi += ohi + (s < lo);
-        lo = s;
-      }
-    }
-    unsigned long long mn = agg.min_bits, mx = agg.max_bits;
-    for (int d = 16; d > 0; d >>= 1) {
-      mn = min(mn, __shfl_down_sync(0xffffffffu, mn, d));
-      mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
-    }
-    unsigned int saw = __any_sync(0xffffffffu, agg.saw);
-    if (lane == 0) {
-      if (cnt) atomicAdd(&sp.ctr->agg_count, cnt);
-      if (num) atomicAdd(&sp.ctr->agg_numeric, num);
-      if (ni) atomicAdd(&sp.ctr->agg_n_int, ni);
-      if (lo || hi) {
-        unsigned long long old = atomicAdd(&sp.ctr->agg_isum_lo, lo);
-        unsigned long long carry = (old + lo) < old;
-        if (hi + carry) atomicAdd(&sp.ctr->agg_isum_hi, hi + carry);
-      }
-      if (num) {
-        atomicMin(&sp.ctr->agg_min_bits, mn);
-        atomicMax(&sp.ctr->agg_max_bits, mx);
-      }
-      if (saw) atomicOr(&sp.ctr->agg_saw_non_numeric, 1u);
-    }
-  } else if (!kRows) {
-    unsigned int saw = __any_sync(0xffffffffu, agg.saw);
-    if (lane == 0 && saw) atomicOr(&sp.ctr->agg_saw_non_numeric, 1u);
-  }
+  // Flush this CTA's counters (a batch's were flushed per tile).
+  flush_counts(sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
 }
 
 // Fixed-order reduction of the per-tile FP partials (pass 1: contiguous
@@ -1041,6 +1080,53 @@ __global__ void k_finalize(const double *block_f, const unsigned long long *bloc
   unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
   ctr->first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
   ctr->first_type_error = cut_t == ~0ull ? ~0ull : lines_t + tiles[cut_t].first_type_error;
+}
+
+// Batched runs: every input's record starts like a fresh run's.
+__global__ void k_batch_reset(RunCounters *in_ctr, uint32_t n_inputs) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_inputs; i += gridDim.x * blockDim.x) {
+    RunCounters z;
+    memset(&z, 0, sizeof(z));
+    z.first_invalid_tile = ~0ull;
+    z.first_type_tile = ~0ull;
+    z.agg_min_bits = ~0ull;
+    z.first_invalid = ~0ull;
+    z.first_type_error = ~0ull;
+    in_ctr[i] = z;
+  }
+}
+
+// Batched runs, one warp per input: the input's FP sum over its tiles (lane l
+// sums a contiguous slice in order, then a fixed shuffle tree) and its first
+// invalid / type-error line.
+__global__ void k_batch_finalize(const double *tile_fsum, const TileDesc *tiles,
+                                 const unsigned long long *in_tile0, RunCounters *in_ctr,
+                                 uint32_t n_inputs) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long i = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n_inputs) return;  // uniform per warp
+  const unsigned long long t0 = in_tile0[i], t1 = in_tile0[i + 1];
+  RunCounters &c = in_ctr[i];
+  const unsigned long long cut = c.first_invalid_tile, cut_t = c.first_type_tile;
+  const unsigned long long per = (t1 - t0 + 31) / 32;
+  const unsigned long long a = min(t0 + lane * per, t1), b = min(a + per, t1);
+  double f = 0.0;
+  unsigned long long lines = 0, lines_t = 0;
+  for (unsigned long long t = a; t < b; t++) {
+    if (tile_fsum) f += tile_fsum[t];
+    if (t < cut) lines += tiles[t].n_lines;
+    if (t < cut_t) lines_t += tiles[t].n_lines;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    f += __shfl_down_sync(0xffffffffu, f, d);
+    lines += __shfl_down_sync(0xffffffffu, lines, d);
+    lines_t += __shfl_down_sync(0xffffffffu, lines_t, d);
+  }
+  if (lane != 0) return;
+  c.fsum_total = f;
+  c.first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
+  c.first_type_error = cut_t == ~0ull ? ~0ull : lines_t + tiles[cut_t].first_type_error;
 }
 
 // ---------------------------------------------------------------------------
