@@ -484,8 +484,10 @@ __device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uin
   tb = __shfl_sync(0xffffffffu, ib, 31);
 }
 
-// Adds the warp's counts and (ungrouped) aggregate to `dst` and clears them.
-__device__ __noinline__ void flush_counts(RunCounters *dst, const DevPlan &P, bool rows, int lane,
+// Adds the warp's counts and (ungrouped) aggregate to `dst` and clears them;
+// `also` (a batch's totals, may be null) receives the line counts too.
+__device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, const DevPlan &P,
+                                          bool rows, int lane,
                                              unsigned long long &c_lines, unsigned long long &c_blank,
                                              unsigned long long &c_invalid, unsigned long long &c_type,
                                              unsigned long long &c_sel, ThreadAgg &agg) {
@@ -493,11 +495,14 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, const DevPlan &P, bo
                            ni = warp_sum_u64(c_invalid), nt = warp_sum_u64(c_type),
                            ns = warp_sum_u64(c_sel);
   if (lane == 0) {
-    if (nl) atomicAdd(&dst->n_lines, nl);
-    if (nb) atomicAdd(&dst->n_blank, nb);
-    if (ni) atomicAdd(&dst->n_invalid, ni);
-    if (nt) atomicAdd(&dst->n_type_error, nt);
-    if (ns) atomicAdd(&dst->n_selected, ns);
+    for (RunCounters *c : {dst, also}) {
+      if (!c) continue;
+      if (nl) atomicAdd(&c->n_lines, nl);
+      if (nb) atomicAdd(&c->n_blank, nb);
+      if (ni) atomicAdd(&c->n_invalid, ni);
+      if (nt) atomicAdd(&c->n_type_error, nt);
+      if (ns) atomicAdd(&c->n_selected, ns);
+    }
   }
   c_lines = c_blank = c_invalid = c_type = c_sel = 0;
   if (!rows && P.group_slot < 0 && P.output_kind == 3) {
@@ -986,7 +991,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
       if (lane == 0) sp.tile_fsum[tile] = f;
     }
     // A batch input's counts and aggregate go to its own record, tile by tile.
-    if (sp.tile_input) flush_counts(ctr_in, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
+    if (sp.tile_input)
+      flush_counts(ctr_in, sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
@@ -1014,7 +1020,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams 
   }
 
   // Flush this CTA's counters (a batch's were flushed per tile).
-  flush_counts(sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
+  flush_counts(sp.ctr, nullptr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
 }
 
 // Fixed-order reduction of the per-tile FP partials (pass 1: contiguous
