@@ -356,7 +356,7 @@ class Query:
         import numpy as np
         rows = b""
         row_off = None
-        if all_.n_selected:
+        if all_.n_selected and all_.d_out_bytes:  # row queries only
             import torch
             from .shard import _DeviceBytes
             nsel = all_.n_selected
