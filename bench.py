@@ -16,6 +16,12 @@ roofline -- the scan kernel: (input + output bytes) per launch / its
            CUDA-event duration, against the measured HBM copy bandwidth.
 cpu_baseline -- the oracle (a C++ restatement of the reference CPU engine) on
            all host cores over a bounded sample of the same input.
+batch   -- many small device-resident inputs, one of 8 queries each: one run
+           per input with a host round trip each ("plain") against one
+           batched run per query (warpjq_batch_launch), aggregate GB/s.
+serve   -- open-loop Poisson arrivals of those inputs: a server that batches
+           whatever has arrived, against one that serves requests one at a
+           time; p50 / p99 / p999 latency and sustained GB/s.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -41,6 +47,11 @@ QUERIES = [
     "select(.status == 500)",
 ]
 METRIC = "GB/s scanned per query (8 GB, device-resident); batched vs plain GB/s; p99 ms"
+BATCH_QUERIES = [
+    "select(.status == 500) | count", "sum(.bytes)", "max(.latency_ms)", "avg(.latency_ms)",
+    "group_by(.host) | sum(.bytes)", "group_by(.path) | count",
+    "select(.status >= 500) | {p: .path, b: .bytes}", "select(.status == 500)",
+]
 WORKLOAD = ("nginx-style NDJSON (ts, host, method, path, status, bytes, latency_ms, ua), "
             "8 GB device-resident, 4 queries per step")
 
@@ -130,6 +141,140 @@ def cpu_baseline(data: bytes, queries, threads=0):
     return time.perf_counter() - t
 
 
+def batch_workload(hnp, n, n_inputs=4096, lo=4096, hi=4 << 20, seed=7):
+    """Device-resident batch inputs: newline-aligned slices of the bench
+    input with log-uniform sizes, packed at 16-byte aligned offsets, and a
+    query index per input drawn uniformly from BATCH_QUERIES."""
+    import math
+    import random
+    import numpy as np
+    import torch
+    rng = random.Random(seed)
+    spans, pos = [], 0
+    for _ in range(n_inputs):
+        sz = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+        if pos + sz >= n:
+            pos = 0
+        end = pos + sz
+        k = bytes(hnp[end - 1:min(n, end + 4096)]).find(b"\n")
+        end = end + k if k >= 0 else end
+        spans.append((pos, end))
+        pos = end
+    qidx = [rng.randrange(len(BATCH_QUERIES)) for _ in range(n_inputs)]
+    offs, total = [], 0
+    for a, b in spans:
+        total = (total + 15) & ~15
+        offs.append(total)
+        total += b - a
+    packed = torch.empty(total + 16, dtype=torch.uint8).pin_memory()
+    pn = packed.numpy()
+    for (a, b), o in zip(spans, offs):
+        pn[o:o + (b - a)] = hnp[a:b]
+    dev = torch.empty(total + 16, dtype=torch.uint8, device="cuda")
+    dev.copy_(packed)
+    torch.cuda.synchronize()
+    return dev, offs, [b - a for a, b in spans], qidx
+
+
+def measure_batch(wjq, dev, offs, lens, qidx):
+    """Aggregate GB/s over all inputs: plain (one run and host round trip
+    per input) and batched (one batched run per query, collected at the
+    end); wall clock, results on the host in both."""
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    ptr = dev.data_ptr()
+    plain_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
+    batch_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
+    groups = [[i for i in range(len(offs)) if qidx[i] == k] for k in range(len(BATCH_QUERIES))]
+    total = sum(lens)
+
+    def plain():
+        for i in range(len(offs)):
+            q = plain_q[qidx[i]]
+            q.launch_device(ptr + offs[i], lens[i], stream)
+            q.collect_device()
+
+    def batched():
+        for k, g in enumerate(groups):
+            batch_q[k].batch_launch(ptr, [offs[i] for i in g], [lens[i] for i in g], stream)
+        for k in range(len(groups)):
+            batch_q[k].batch_collect()
+
+    out = {}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        fn()  # warm: buffers reach their sizes
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        out[name] = time.perf_counter() - t0
+    return {"inputs": len(offs), "bytes": total,
+            "sizes": "log-uniform 4 KiB - 4 MiB (rescaled from 4 KB - 64 MB, whose ~28 GB does not "
+                     "fit the bench's time budget)",
+            "queries": len(BATCH_QUERIES), "residency": "device",
+            "plain_gbs": round(total / out["plain"] / 1e9, 3),
+            "batched_gbs": round(total / out["batched"] / 1e9, 3),
+            "plain_s": round(out["plain"], 4), "batched_s": round(out["batched"], 4),
+            "speedup": round(out["plain"] / out["batched"], 2)}
+
+
+def measure_serving(wjq, dev, offs, lens, qidx, rate=2000.0, n_req=4096, seed=11):
+    """Open-loop Poisson arrivals at `rate` req/s over the batch inputs.
+    "batched": at each step the server takes every request that has arrived
+    and runs one batch per query among them; "one-at-a-time": one run per
+    request.  Latency = completion - arrival (wall clock)."""
+    import random
+    import torch
+    rng = random.Random(seed)
+    stream = torch.cuda.current_stream().cuda_stream
+    ptr = dev.data_ptr()
+    reqs = [rng.randrange(len(offs)) for _ in range(n_req)]
+    gaps = [rng.expovariate(rate) for _ in range(n_req)]
+    qs = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
+    for q in qs:  # warm
+        q.batch_launch(ptr, offs[:64], lens[:64], stream)
+        q.batch_collect()
+
+    def run(mode):
+        t0 = time.perf_counter() + 0.01
+        arrive, t = [], t0
+        for g in gaps:
+            t += g
+            arrive.append(t)
+        lat = [0.0] * n_req
+        nxt = 0
+        while nxt < n_req:
+            now = time.perf_counter()
+            if arrive[nxt] > now:
+                continue  # open loop: wait for the next arrival
+            k = nxt
+            while k < n_req and arrive[k] <= now:
+                k += 1
+            if mode == "one":
+                k = nxt + 1
+            todo = list(range(nxt, k))
+            by_q = {}
+            for r in todo:
+                by_q.setdefault(qidx[reqs[r]], []).append(reqs[r])
+            for qi, ins in by_q.items():
+                qs[qi].batch_launch(ptr, [offs[i] for i in ins], [lens[i] for i in ins], stream)
+            for qi in by_q:
+                qs[qi].batch_collect()
+            done = time.perf_counter()
+            for r in todo:
+                lat[r] = done - arrive[r]
+            nxt = k
+        span = time.perf_counter() - t0
+        lat.sort()
+        pick = lambda f: round(lat[min(n_req - 1, int(f * n_req))] * 1e3, 3)
+        return {"p50_ms": pick(0.50), "p99_ms": pick(0.99), "p999_ms": pick(0.999),
+                "sustained_gbs": round(sum(lens[i] for i in reqs) / span / 1e9, 3)}
+
+    return {"offered_req_per_s": rate, "requests": n_req, "residency": "device",
+            "sizes": "the batch inputs (log-uniform 4 KiB - 4 MiB, rescaled from 1 KB - 256 MB)",
+            "batched": run("batched"), "one_at_a_time": run("one")}
+
+
 def run_reference(args, rank):
     """The reference arm: the reference's CPU engine, as restated by the
     oracle (the Rust crate cannot be built here), on all host cores."""
@@ -178,6 +323,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch and serving legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -306,6 +452,13 @@ def main():
         h2d = n * len(QUERIES)
         d2h = outs // args.e2e_steps
 
+    batch = serve = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        bdev, boffs, blens, bq = batch_workload(hnp, n)
+        batch = measure_batch(wjq, bdev, boffs, blens, bq)
+        serve = measure_serving(wjq, bdev, boffs, blens, bq)
+        del bdev
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = bytes(hnp[: min(args.cpu_sample, n)])
@@ -342,6 +495,8 @@ def main():
             "gpu_launches": kernels_per_step * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "batch": batch,
+            "serve": serve,
         }
         print(json.dumps(line), flush=True)
     if dist:
