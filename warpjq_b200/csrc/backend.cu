@@ -316,7 +316,6 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     ScanParams sp{};
     sp.data = d_data;
     sp.n = n;
-    sp.plan = c->d_plan;
     sp.tile_bytes = c->tile_bytes;
     sp.halo_bytes = c->halo_bytes;
     sp.n_tiles = n_tiles;
@@ -343,9 +342,9 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     }
     CK(cudaEventRecord(s.scan_t0, st), "event record");
     if (P.needs_rows)
-      k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp);
+      k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     else
-      k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp);
+      k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     s.kernels++;
     CK(cudaGetLastError(), "launch scan");
     CK(cudaEventRecord(s.scan_t1, st), "event record");

@@ -108,7 +108,6 @@ struct RowTile {
 struct ScanParams {
   const uint8_t *data;
   unsigned long long n;
-  const DevPlan *plan;
   uint32_t tile_bytes;
   uint32_t halo_bytes;
   unsigned long long n_tiles;
@@ -579,10 +578,13 @@ __device__ __forceinline__ uint32_t chunk_newlines(const uint8_t *win, uint32_t 
   return nat;
 }
 
+// The plan is a kernel parameter (constant bank): fields at fixed offsets
+// are instruction operands, and no plan read goes through global memory.
 template <bool kRows>
-__global__ void __launch_bounds__(kThreads, kScanBlocksPerSM) k_scan(ScanParams sp) {
+__global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
+    k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
-  const DevPlan &P = *sp.plan;
+  const DevPlan &P = plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
   // Shared layout: window bytes (+32 readable bytes past the end for the
   // walker's word reads), per-32-byte-chunk newline masks, line starts.

@@ -59,8 +59,7 @@ constexpr unsigned kNoAllocReduceBlocks = 256;
 
 constexpr uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
 constexpr uint64_t kOffCtr = 0;
-constexpr uint64_t kOffPlan = align256(kOffCtr + sizeof(RunCounters));
-constexpr uint64_t kOffTiles = align256(kOffPlan + sizeof(DevPlan));
+constexpr uint64_t kOffTiles = align256(kOffCtr + sizeof(RunCounters));
 constexpr uint64_t kOffFsum = align256(kOffTiles + kNoAllocMaxTiles * sizeof(TileDesc));
 constexpr uint64_t kOffBlockF = align256(kOffFsum + kNoAllocMaxTiles * sizeof(double));
 constexpr uint64_t kOffBlockLines = align256(kOffBlockF + kNoAllocReduceBlocks * sizeof(double));
@@ -201,20 +200,12 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
   cudaStream_t st = (cudaStream_t)stream;
   unsigned char *base = s->scratch;
   RunCounters *ctr = (RunCounters *)(base + kOffCtr);
-  DevPlan *d_plan = (DevPlan *)(base + kOffPlan);
   TileDesc *tiles = (TileDesc *)(base + kOffTiles);
   double *tile_fsum = (double *)(base + kOffFsum);
   double *block_f = (double *)(base + kOffBlockF);
   unsigned long long *block_lines = (unsigned long long *)(base + kOffBlockLines);
   uint32_t *deep = (uint32_t *)(base + kOffDeep);
 
-  // The plan is copied from this stack frame; for a pageable source the copy
-  // is staged before cudaMemcpyAsync returns.
-  e = cudaMemcpyAsync(d_plan, &plan, sizeof(DevPlan), cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    set_err(err, err_len, "plan upload: %s", cudaGetErrorString(e));
-    return WARPJQ_ERR_CUDA;
-  }
   k_noalloc_reset<<<1, 32, 0, st>>>(ctr);
   unsigned long long n_tiles = (n_bytes + kNoAllocTile - 1) / kNoAllocTile;
   if (n_bytes > 0) {
@@ -222,7 +213,6 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     memset(&sp, 0, sizeof(sp));
     sp.data = d_data;
     sp.n = n_bytes;
-    sp.plan = d_plan;
     sp.tile_bytes = kNoAllocTile;
     sp.halo_bytes = kNoAllocHalo;
     sp.n_tiles = n_tiles;
@@ -232,7 +222,7 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     sp.deep_words = deep;
     sp.deep_levels_per_cta = kNoAllocDeepLevels;
     unsigned grid = (unsigned)(n_tiles < s->grid ? n_tiles : s->grid);
-    k_scan<false><<<grid, kThreads, s->smem, st>>>(sp);
+    k_scan<false><<<grid, kThreads, s->smem, st>>>(sp, plan);
     k_reduce_tiles<<<kNoAllocReduceBlocks, kReduceThreads, 0, st>>>(tile_fsum, n_tiles, block_f,
                                                                     tiles, ctr, block_lines);
     k_finalize<<<1, 32, 0, st>>>(block_f, block_lines, kNoAllocReduceBlocks, tiles, ctr);

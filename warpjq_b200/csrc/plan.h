@@ -48,6 +48,7 @@ struct PlanNode {
   uint8_t has_key_children;
   uint8_t has_index_children;
   uint8_t key_first;     // first key byte, a cheap reject before comparing
+  uint32_t key_w[2];     // the key's first 8 bytes, little-endian, zero past its end
 };
 
 struct PlanCmp {

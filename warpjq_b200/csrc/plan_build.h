@@ -137,6 +137,9 @@ inline warpjq_status build_plan(const warpjq_program *p, DevPlan &P, char *err, 
     d.next_sibling = kNoNode;
     d.subtree_end = (uint8_t)subtree_end[order[i]];
     d.key_first = (!x.is_index && x.key_len) ? p->blob[x.key_off] : 0;
+    d.key_w[0] = d.key_w[1] = 0;
+    for (uint32_t b = 0; !x.is_index && b < x.key_len && b < 8; b++)
+      d.key_w[b >> 2] |= (uint32_t)p->blob[x.key_off + b] << (8 * (b & 3));
     d.key_len_mask = 0;
     for (size_t k = 0; k < x.kids.size(); k++) {
       const TmpNode &c = tn[x.kids[k]];

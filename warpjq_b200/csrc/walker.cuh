@@ -472,6 +472,27 @@ __device__ __forceinline__ uint32_t win_atom(const uint8_t *w, uint32_t i, uint3
   return j;
 }
 
+// match_key for a key body at w[off, off + len) of a window: keys of up to
+// 8 bytes compare as two words.
+__device__ __forceinline__ uint8_t match_key_win(const DevPlan &P, uint8_t node, const uint8_t *w,
+                                                 uint32_t off, uint32_t len, bool esc) {
+  if (esc) return match_key(P, node, w + off, len, esc);
+  const uint32_t w0 = load4(w, off), w1 = load4(w, off + 4);
+  const uint32_t m0 = len >= 4 ? 0xFFFFFFFFu : (1u << (8 * len)) - 1u;
+  const uint32_t m1 = len >= 8 ? 0xFFFFFFFFu : len > 4 ? (1u << (8 * (len - 4))) - 1u : 0u;
+  for (uint8_t c = P.nodes[node].first_child; c != kNoNode; c = P.nodes[c].next_sibling) {
+    const PlanNode &nd = P.nodes[c];
+    if (nd.is_index || nd.key_len != len) continue;
+    if ((w0 & m0) != nd.key_w[0] || (w1 & m1) != nd.key_w[1]) continue;
+    if (len <= 8) return c;
+    const uint8_t *k = P.blob + nd.key_off;
+    uint32_t t = 8;
+    while (t < len && w[off + t] == k[t]) t++;
+    if (t >= len) return c;
+  }
+  return kNoNode;
+}
+
 }  // namespace detail
 
 // Walks the line w[s, e) of a window.  w must be 4-byte aligned, w[e] must
@@ -517,7 +538,7 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
       if (cur_lm) {
         const uint32_t kl = q - i - 1;
         if (esc || ((cur_lm >> (kl < 63u ? kl : 63u)) & 1ull))
-          vn = match_key(P, (uint8_t)cur, w + i + 1, kl, esc);
+          vn = match_key_win(P, (uint8_t)cur, w, i + 1, kl, esc);
       }
       // ':' and the value's first byte, usually in one read
       const uint32_t la = load4(w, q + 1);
