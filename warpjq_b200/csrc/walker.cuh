@@ -368,43 +368,26 @@ __device__ __forceinline__ bool simple_escape(uint32_t e) {
          e == 't';
 }
 
-// Flag mask keeping the bytes of a word at or after byte `sh` of it (sh <= 0:
-// all of them; sh >= 4: none).
-__device__ __forceinline__ uint32_t below_mask(int sh) {
-  return sh <= 0 ? 0xFFFFFFFFu : sh >= 4 ? 0u : (0xFFFFFFFFu << (8 * sh));
-}
-
 // Closing quote of the string opened at w[i], or 0 when the string is
 // malformed (a bad escape, a raw control byte) or reaches the newline.
 // `esc` reports whether the body holds a backslash.  Ordinary bytes are
-// skipped 16 at a time, then 32 at a time; the byte that stops a step is
-// taken from the loaded word.
+// skipped four at a time up to a 16-byte boundary, then 32 at a time; the
+// byte that stops a step is taken from the loaded word.
 __device__ __forceinline__ uint32_t win_string(const uint8_t *w, uint32_t i, bool &esc) {
   uint32_t p = i + 1;
   esc = false;
   for (;;) {
-    // One aligned 16-byte step with the bytes before p masked off (the same
-    // step for every lane, whatever its alignment), then 32-byte steps.
-    uint32_t wa = p & ~15u;
-    const int lo = (int)(p - wa);
-    uint32_t x, f;
-    {
-      const uint4 u = *(const uint4 *)(w + wa);
-      const uint32_t g0 = str_special(u.x) & below_mask(lo), g1 = str_special(u.y) & below_mask(lo - 4),
-                     g2 = str_special(u.z) & below_mask(lo - 8), g3 = str_special(u.w) & below_mask(lo - 12);
-      if (g0) {
-        f = g0; x = u.x;
-      } else if (g1) {
-        f = g1; x = u.y; wa += 4;
-      } else if (g2) {
-        f = g2; x = u.z; wa += 8;
-      } else if (g3) {
-        f = g3; x = u.w; wa += 12;
-      } else {
-        f = 0; x = 0; wa += 16;
-      }
-    }
+    uint32_t wa = p & ~3u;
+    uint32_t x = *(const uint32_t *)(w + wa);
+    uint32_t f = str_special(x) & (0xFFFFFFFFu << ((p & 3u) * 8u));
     if (!f) {
+      wa += 4;
+      while (wa & 15u) {
+        x = *(const uint32_t *)(w + wa);
+        f = str_special(x);
+        if (f) break;
+        wa += 4;
+      }
       while (!f) {
         const uint4 u = *(const uint4 *)(w + wa);
         const uint4 v = *(const uint4 *)(w + wa + 16);
