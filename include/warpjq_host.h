@@ -77,6 +77,17 @@ uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t
 uint64_t warpjq_gen_nginx_block(uint64_t seed, uint64_t block, uint64_t first_line, uint8_t *out,
                                 uint64_t cap, uint64_t *n_lines);
 
+/* The same for a nested, dirty schema: objects 3-5 levels deep with shuffled
+ * key order (req.user.{id, tier, geo{cc, lat, lon}}, req.method, req.path,
+ * resp.{code, latency, size}, meta.trace.span.{id, depth}, ts), about 10% of
+ * strings with escapes, latencies in decimal and exponent forms, user ids
+ * Zipf(0.9) over [1, n_users], and about 2% malformed lines (cut short, a
+ * bare NaN, a leading zero). */
+uint64_t warpjq_gen_nested(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                           unsigned threads, uint64_t n_users, uint64_t *total_lines);
+uint64_t warpjq_gen_nested_block(uint64_t seed, uint64_t block, uint64_t first_line, uint64_t n_users,
+                                 uint8_t *out, uint64_t cap, uint64_t *n_lines);
+
 #ifdef __cplusplus
 }
 #endif

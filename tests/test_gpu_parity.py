@@ -186,3 +186,41 @@ def test_contexts_with_different_tilings_interleave():
             assert r.rc == 0, r.err
             c = orc.run(q.query, data)
             assert r.out == c.out, q.query
+
+
+NESTED_QUERIES = [
+    'select(.req.user.tier == "gold" and .resp.code != 200) | {u: .req.user.id, l: .resp.latency}',
+    "group_by(.req.user.id) | avg(.resp.latency)", "group_by(.req.user.tier) | count",
+    "select(.meta.trace.span.depth > 5) | .req.path", "max(.resp.latency)", "sum(.resp.size)",
+    "select(.req.user.geo.cc == \"jp\") | {c: .req.user.geo, m: .req.method}",
+]
+
+
+def test_nested_dirty_schema_queries():
+    """The nested, dirty workload (objects 3-5 levels deep, shuffled keys,
+    escapes, mixed number forms, ~2% malformed lines): host path with small
+    chunks, in all output formats."""
+    buf, used, _ = wjq.gen_nested(6 << 20, seed=21, n_users=50_000)
+    agree(bytes(buf[:used]), NESTED_QUERIES, "nested",
+          fractional={"group_by(.req.user.id) | avg(.resp.latency)"})
+
+
+def test_group_table_grows_past_its_first_size():
+    """group_by over ~150k distinct ids in one chunk: more keys than the
+    table's first size, so the run grows the table and repeats on the device;
+    the host and device-resident paths both match the oracle."""
+    import torch
+    buf, used, _ = wjq.gen_nested(40 << 20, seed=22, n_users=1_000_000)
+    data = bytes(buf[:used])
+    q = "group_by(.req.user.id) | avg(.resp.latency)"
+    want = orc.run(q, data)
+    got = wjq.run_bytes(q, data, chunk_bytes=64 << 20)
+    assert got.rc == 0 and close_enough(got.out, want.out)
+    assert want.out.count(b"\n") > 100_000
+    Q = wjq.Query(q)
+    dev = torch.empty(len(data) + 16, dtype=torch.uint8, device="cuda")
+    dev[:len(data)].copy_(torch.frombuffer(bytearray(data), dtype=torch.uint8))
+    Q.launch_device(dev.data_ptr(), len(data), torch.cuda.current_stream().cuda_stream)
+    r = Q.collect_device()
+    assert close_enough(Q.render_device(r, data), want.out)
+    Q.close()

@@ -41,6 +41,7 @@ HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
     "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
     "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
+    "warpjq_gen_nested", "warpjq_gen_nested_block",
 ]
 
 
@@ -104,6 +105,8 @@ def _load():
     h.warpjq_host_free.argtypes = [vp]
     h.warpjq_gen_nginx.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
     h.warpjq_gen_nginx.restype = u64
+    h.warpjq_gen_nested.argtypes = [u64, vp, u64, u64, ctypes.c_uint, u64, ctypes.POINTER(u64)]
+    h.warpjq_gen_nested.restype = u64
     _kern, _host = k, h
     return k, h
 
@@ -408,6 +411,18 @@ def device_name() -> str:
     buf = ctypes.create_string_buffer(256)
     k.warpjq_device_name(buf, len(buf))
     return buf.value.decode()
+
+
+def gen_nested(n_bytes: int, seed: int = 1, n_users: int = 1_000_000, threads: int = 0, into=None):
+    """About n_bytes of the nested, dirty schema (warpjq_host.h
+    warpjq_gen_nested); returns (buffer, used_bytes, n_lines)."""
+    import numpy as np
+    _, h = _load()
+    buf = into if into is not None else np.empty(n_bytes, dtype=np.uint8)
+    lines = ctypes.c_uint64()
+    used = h.warpjq_gen_nested(seed, buf.ctypes.data, n_bytes, 1 << 20, threads, n_users,
+                               ctypes.byref(lines))
+    return buf, int(used), int(lines.value)
 
 
 def gen_nginx(n_bytes: int, seed: int = 1, threads: int = 0, into=None):

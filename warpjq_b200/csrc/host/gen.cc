@@ -134,9 +134,182 @@ char *nginx_line(char *p, Rng &r, uint64_t i) {
   return p;
 }
 
+// ---------------------------------------------------------------------------
+// Nested, dirty schema: objects 3-5 levels deep with shuffled key order,
+// escaped strings, mixed number forms and a share of malformed lines.
+//   ts     integer
+//   req    {user: {id: "u<Zipf(0.9) over n_users>", tier, geo: {cc, lat, lon}}, method, path}
+//   resp   {code, latency (decimal or exponent form of the same value), size}
+//   meta   {trace: {span: {id, depth}}}
+// About 10% of path strings carry a \uXXXX escape or an escaped quote; about
+// 2% of lines are malformed: cut short, a bare NaN, or a leading zero.
+// ---------------------------------------------------------------------------
+
+const char *kTiers[4] = {"gold", "silver", "bronze", "free"};
+const char *kCcs[6] = {"us", "de", "jp", "br", "in", "fr"};
+const char *kMethods[4] = {"GET", "POST", "PUT", "DELETE"};
+
+char *put_dec3(char *p, uint64_t milli) {  // milli/1000 with three decimals
+  p = put_u64(p, milli / 1000);
+  *p++ = '.';
+  *p++ = (char)('0' + milli / 100 % 10);
+  *p++ = (char)('0' + milli / 10 % 10);
+  *p++ = (char)('0' + milli % 10);
+  return p;
+}
+
+// The same value (milli / 1000) as a decimal, an exponent form, or a
+// decimal exponent form.
+char *put_mixed(char *p, Rng &r, uint64_t milli) {
+  uint32_t form = r.below(3);
+  if (form == 0) return put_dec3(p, milli);
+  if (form == 1) {  // <milli>e-3
+    p = put_u64(p, milli);
+    return put(p, "e-3");
+  }
+  p = put_dec3(p, milli * 10);  // (milli*10/1000)E-1
+  return put(p, "E-1");
+}
+
+uint64_t zipf(Rng &r, uint64_t n, double s) {
+  // inverse of the continuous approximation of the Zipf CDF on [1, n]
+  const double a = 1.0 - s;
+  double k = std::pow(1.0 + r.uniform() * (std::pow((double)n, a) - 1.0), 1.0 / a);
+  uint64_t v = (uint64_t)k;
+  return v < 1 ? 1 : (v > n ? n : v);
+}
+
+char *nested_line(char *p, Rng &r, uint64_t i, uint64_t n_users) {
+  char *start = p;
+  const uint32_t bad = r.below(100) < 2 ? 1 + r.below(3) : 0;  // 1 cut, 2 NaN, 3 leading zero
+  char buf[4][256];
+  char *e[4];
+  // req
+  {
+    char *q = buf[0];
+    const char *parts[3];
+    char user[160], *u = user;
+    const char *uk[3];
+    char idb[40], *ip = idb;
+    ip = put(ip, "\"id\":\"u");
+    ip = put_u64(ip, zipf(r, n_users, 0.9));
+    ip = put(ip, "\"");
+    *ip = 0;
+    char tb[32], *tp = tb;
+    tp = put(tp, "\"tier\":\"");
+    tp = put(tp, kTiers[r.below(4)]);
+    tp = put(tp, "\"");
+    *tp = 0;
+    char gb[96], *gp = gb;
+    gp = put(gp, "\"geo\":{\"cc\":\"");
+    gp = put(gp, kCcs[r.below(6)]);
+    gp = put(gp, "\",\"lat\":");
+    gp = put_dec3(gp, r.below(90000));
+    gp = put(gp, ",\"lon\":-");
+    gp = put_dec3(gp, r.below(180000));
+    gp = put(gp, "}");
+    *gp = 0;
+    uk[0] = idb; uk[1] = tb; uk[2] = gb;
+    for (int k = 2; k > 0; k--) { int j = r.below(k + 1); const char *t = uk[k]; uk[k] = uk[j]; uk[j] = t; }
+    u = put(u, "\"user\":{");
+    for (int k = 0; k < 3; k++) { if (k) *u++ = ','; u = put(u, uk[k]); }
+    *u++ = '}';
+    *u = 0;
+    char mb[32], *mp = mb;
+    mp = put(mp, "\"method\":\"");
+    mp = put(mp, kMethods[r.below(4)]);
+    mp = put(mp, "\"");
+    *mp = 0;
+    char pb[96], *pp = pb;
+    pp = put(pp, "\"path\":\"/api/v2/");
+    pp = put(pp, kTiers[r.below(4)]);
+    const uint32_t esc = r.below(10);
+    if (esc == 0) pp = put(pp, "/caf\\u00e9");
+    else if (esc == 1) pp = put(pp, "/say \\\"hi\\\"");
+    pp = put(pp, "\"");
+    *pp = 0;
+    parts[0] = user; parts[1] = mb; parts[2] = pb;
+    for (int k = 2; k > 0; k--) { int j = r.below(k + 1); const char *t = parts[k]; parts[k] = parts[j]; parts[j] = t; }
+    q = put(q, "\"req\":{");
+    for (int k = 0; k < 3; k++) { if (k) *q++ = ','; q = put(q, parts[k]); }
+    *q++ = '}';
+    e[0] = q;
+  }
+  // resp
+  {
+    char *q = buf[1];
+    const uint32_t c = r.below(100);
+    const char *code = c < 75 ? "200" : c < 80 ? "201" : c < 84 ? "204" : c < 87 ? "301" : c < 92 ? "400"
+                       : c < 96 ? "404" : c < 99 ? "500" : "503";
+    char cb[32], *cp = cb;
+    cp = put(cp, "\"code\":");
+    if (bad == 3) *cp++ = '0';
+    cp = put(cp, code);
+    *cp = 0;
+    char lb[48], *lp = lb;
+    lp = put(lp, "\"latency\":");
+    if (bad == 2) lp = put(lp, "NaN");
+    else lp = put_mixed(lp, r, (uint64_t)std::llround(std::exp(3.0 + r.normal()) * 1000.0));
+    *lp = 0;
+    char sb[40], *sp = sb;
+    sp = put(sp, "\"size\":");
+    sp = put_u64(sp, r.below(1000000));
+    *sp = 0;
+    const char *f[3] = {cb, lb, sb};
+    for (int k = 2; k > 0; k--) { int j = r.below(k + 1); const char *t = f[k]; f[k] = f[j]; f[j] = t; }
+    q = put(q, "\"resp\":{");
+    for (int k = 0; k < 3; k++) { if (k) *q++ = ','; q = put(q, f[k]); }
+    *q++ = '}';
+    e[1] = q;
+  }
+  // meta and ts
+  {
+    char *q = buf[2];
+    q = put(q, "\"meta\":{\"trace\":{\"span\":{\"id\":\"");
+    static const char hx[] = "0123456789abcdef";
+    for (int k = 0; k < 16; k++) *q++ = hx[r.below(16)];
+    q = put(q, "\",\"depth\":");
+    q = put_u64(q, r.below(8));
+    q = put(q, "}}}");
+    e[2] = q;
+    char *t = buf[3];
+    t = put(t, "\"ts\":");
+    t = put_u64(t, 1700000000ull + i);
+    e[3] = t;
+  }
+  int order[4] = {0, 1, 2, 3};
+  for (int k = 3; k > 0; k--) { int j = r.below(k + 1); int t = order[k]; order[k] = order[j]; order[j] = t; }
+  *p++ = '{';
+  for (int k = 0; k < 4; k++) {
+    if (k) *p++ = ',';
+    size_t n = (size_t)(e[order[k]] - buf[order[k]]);
+    memcpy(p, buf[order[k]], n);
+    p += n;
+  }
+  *p++ = '}';
+  if (bad == 1) p = start + 1 + r.below((uint32_t)(p - start - 1));  // cut short
+  *p++ = '\n';
+  return p;
+}
+
 }  // namespace
 
 extern "C" {
+
+// The nested schema (above), like warpjq_gen_nginx_block; a line is at most
+// 1 KiB.
+uint64_t warpjq_gen_nested_block(uint64_t seed, uint64_t block, uint64_t first_line, uint64_t n_users,
+                                 uint8_t *out, uint64_t cap, uint64_t *n_lines) {
+  Rng r(seed * 0x100000001B3ull ^ (block * 0xD1B54A32D192ED03ull) ^ 0x5EED5EEDull);
+  char *p = (char *)out, *end = (char *)out + cap;
+  uint64_t i = first_line;
+  while (end - p >= 1024) {
+    p = nested_line(p, r, i, n_users ? n_users : 1);
+    i++;
+  }
+  if (n_lines) *n_lines = i - first_line;
+  return (uint64_t)(p - (char *)out);
+}
 
 // Fills `out[0, cap)` with whole nginx lines for the block `block` of `seed`,
 // starting at line index `first_line`.  Returns bytes written and the number
@@ -157,8 +330,8 @@ uint64_t warpjq_gen_nginx_block(uint64_t seed, uint64_t block, uint64_t first_li
 // Generates about `target` bytes of nginx NDJSON into `out` (capacity cap
 // >= target), in parallel blocks of `block_bytes`.  Each block is padded
 // with its lines only (no partial lines).  Returns the bytes written.
-uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
-                          unsigned threads, uint64_t *total_lines) {
+static uint64_t gen_parallel(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                             unsigned threads, uint64_t *total_lines, uint64_t n_users, bool nested) {
   if (block_bytes < 4096) block_bytes = 4096;
   uint64_t nb = (target + block_bytes - 1) / block_bytes;
   std::vector<uint64_t> len(nb), lines(nb);
@@ -171,8 +344,10 @@ uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t
         // Blocks are generated in place at their nominal offset; lines of a
         // block never cross into the next block.
         uint64_t cap = std::min<uint64_t>(block_bytes, target - b * block_bytes);
-        len[b] = warpjq_gen_nginx_block(seed, b, b * (block_bytes / 64), out + b * block_bytes, cap,
-                                        &lines[b]);
+        len[b] = nested ? warpjq_gen_nested_block(seed, b, b * (block_bytes / 64), n_users,
+                                                  out + b * block_bytes, cap, &lines[b])
+                        : warpjq_gen_nginx_block(seed, b, b * (block_bytes / 64), out + b * block_bytes,
+                                                 cap, &lines[b]);
       }
     });
   }
@@ -186,6 +361,18 @@ uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t
   }
   if (total_lines) *total_lines = total;
   return w;
+}
+
+uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                          unsigned threads, uint64_t *total_lines) {
+  return gen_parallel(seed, out, target, block_bytes, threads, total_lines, 0, false);
+}
+
+// Generates about `target` bytes of the nested schema with user ids drawn
+// from [1, n_users].
+uint64_t warpjq_gen_nested(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                           unsigned threads, uint64_t n_users, uint64_t *total_lines) {
+  return gen_parallel(seed, out, target, block_bytes, threads, total_lines, n_users, true);
 }
 
 }  // extern "C"
