@@ -111,6 +111,11 @@ warpjq_status warpjq_submit_host(warpjq_ctx *ctx, uint32_t slot, const uint8_t *
  * else 0.  No reference counterpart. */
 int warpjq_host_is_pinned(const void *p);
 
+/* Page-locked host memory for input buffers (null on failure), and its
+ * release (waits for the device).  No reference counterpart. */
+void *warpjq_host_alloc_pinned(uint64_t n_bytes);
+void warpjq_host_free_pinned(void *p);
+
 /* One input's result within a batch (warpjq_batch_collect).  Line indexes
  * are relative to the input. */
 typedef struct {

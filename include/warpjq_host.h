@@ -55,6 +55,14 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
                      uint64_t max_line_bytes, char **out, size_t *out_len, uint64_t *stats,
                      char *err, size_t err_len);
 
+/* Runs the query over a file: read with parallel preads into page-locked
+ * buffers, in newline-aligned chunks, each chunk read while the device works
+ * on the one before.  Output and stats as warpjq_query_run; error messages
+ * name the file. */
+int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid,
+                          uint64_t max_line_bytes, char **out, size_t *out_len, uint64_t *stats,
+                          char *err, size_t err_len);
+
 /* One-shot: open, run, close. */
 int warpjq_run_bytes(const char *query, const uint8_t *data, size_t len, uint32_t format,
                      uint32_t on_invalid, uint64_t chunk_bytes, uint64_t max_line_bytes,

@@ -35,13 +35,14 @@ ABI_SYMBOLS = [
 EXT_SYMBOLS = [
     "warpjq_launch_device", "warpjq_collect_device", "warpjq_slot_first_errors",
     "warpjq_set_tiling", "warpjq_autotile", "warpjq_submit_host", "warpjq_host_is_pinned",
-    "warpjq_batch_launch", "warpjq_batch_collect",
+    "warpjq_batch_launch", "warpjq_batch_collect", "warpjq_host_alloc_pinned",
+    "warpjq_host_free_pinned",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
     "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
     "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
-    "warpjq_gen_nested", "warpjq_gen_nested_block",
+    "warpjq_gen_nested", "warpjq_gen_nested_block", "warpjq_query_run_file",
 ]
 
 
@@ -97,6 +98,9 @@ def _load():
     h.warpjq_query_run.argtypes = [vp, vp, sz, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
                                    ctypes.POINTER(u64), cp, sz]
     h.warpjq_query_run.restype = ctypes.c_int
+    h.warpjq_query_run_file.argtypes = [vp, cp, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
+                                        ctypes.POINTER(u64), cp, sz]
+    h.warpjq_query_run_file.restype = ctypes.c_int
     h.warpjq_run_bytes.argtypes = [cp, cp, sz, u32, u32, u64, u64, ctypes.POINTER(vp),
                                    ctypes.POINTER(sz), ctypes.POINTER(u64), cp, sz]
     h.warpjq_run_bytes.restype = ctypes.c_int
@@ -285,6 +289,20 @@ class Query:
         rc = self._h.warpjq_query_run(self._q, addr, n_bytes, ON_INVALID[on_invalid],
                                       max_line_bytes, ctypes.byref(out), ctypes.byref(n), st, err,
                                       len(err))
+        body = _take(out, n) if copy_out else _view(out, n)
+        return RunResult(rc, body, _stats(st), err.value.decode(errors="replace"))
+
+    def run_file(self, path: str, on_invalid: str = "skip", max_line_bytes: int = 0,
+                 copy_out: bool = True) -> RunResult:
+        """Runs over a file (parallel reads into page-locked buffers,
+        overlapped with the device)."""
+        out = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        st = (ctypes.c_uint64 * 5)()
+        err = ctypes.create_string_buffer(4096)
+        rc = self._h.warpjq_query_run_file(self._q, path.encode(), ON_INVALID[on_invalid],
+                                           max_line_bytes, ctypes.byref(out), ctypes.byref(n), st,
+                                           err, len(err))
         body = _take(out, n) if copy_out else _view(out, n)
         return RunResult(rc, body, _stats(st), err.value.decode(errors="replace"))
 

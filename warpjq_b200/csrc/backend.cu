@@ -622,6 +622,19 @@ warpjq_status warpjq_submit_host(warpjq_ctx *ctx, uint32_t slot, const uint8_t *
   return WARPJQ_OK;
 }
 
+void *warpjq_host_alloc_pinned(uint64_t n_bytes) {
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, n_bytes ? n_bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void warpjq_host_free_pinned(void *p) {
+  if (p) cudaFreeHost(p);
+}
+
 int warpjq_host_is_pinned(const void *p) {
   if (!p) return 0;
   cudaPointerAttributes a;

@@ -6,8 +6,15 @@
 // flight (fill n+1 while n computes), merges every chunk's rows and
 // aggregates in input order, and formats the output bytes.  There is no CPU
 // evaluation of any line: every line of every chunk is decided on the device.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
+#include <cerrno>
 #include <charconv>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +33,8 @@
 #pragma weak warpjq_submit_host
 #pragma weak warpjq_host_is_pinned
 #pragma weak warpjq_slot_first_errors
+#pragma weak warpjq_host_alloc_pinned
+#pragma weak warpjq_host_free_pinned
 #include "query.h"
 
 namespace wjqh {
@@ -467,9 +476,23 @@ warpjq_ctx *warpjq_query_ctx(warpjq_query *q) { return q ? q->ctx : nullptr; }
 
 int warpjq_query_is_aggregate(const warpjq_query *q) { return q && q->prog.is_aggregate(); }
 
-int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t on_invalid,
-                     uint64_t max_line_bytes, char **out, size_t *out_len, uint64_t *stats,
-                     char *err, size_t err_len) {
+// One newline-aligned chunk of input, at host address `data`; `pinned` when
+// it is page-locked (copied to the device straight from there).
+struct Chunk {
+  const uint8_t *data = nullptr;
+  uint64_t n = 0;
+  bool pinned = false;
+};
+
+// The run loop shared by memory and file input: `next` yields chunks (false
+// at the end; a nonempty error message stops the run), `total` is the input
+// size (for sizing the output), `sample` the input's first bytes (for the
+// tiling).  A chunk's bytes must stay valid until the chunk after the next
+// one has been asked for.
+static int run_chunks(warpjq_query *q, uint64_t total, const uint8_t *sample, size_t sample_len,
+                      const std::function<bool(Chunk &, std::string &)> &next, const char *name,
+                      uint32_t on_invalid, uint64_t max_line_bytes, char **out, size_t *out_len,
+                      uint64_t *stats, char *err, size_t err_len) {
   *out = nullptr;
   if (out_len) *out_len = 0;
   if (!max_line_bytes) max_line_bytes = 64ull << 20;
@@ -478,11 +501,8 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
   w.fmt = q->fmt;
   w.header(P);
   Totals tot;
-  uint64_t st_lines = 0, st_malformed = 0, st_type = 0, lines_seen = 0;
+  uint64_t st_lines = 0, st_malformed = 0, st_type = 0, lines_seen = 0, done_bytes = 0;
   char e[512] = {0};
-
-  // Strip a UTF-8 byte-order mark (chunk.rs:210-212).
-  size_t pos = (len >= 3 && data[0] == 0xEF && data[1] == 0xBB && data[2] == 0xBF) ? 3 : 0;
 
   struct Flight {
     uint32_t slot;
@@ -512,13 +532,15 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     st_lines += r.n_lines - r.n_blank;
     st_malformed += r.n_invalid;
     st_type += r.n_type_error;
+    done_bytes += f.n;
     if (on_invalid == WARPJQ_ON_INVALID_ABORT && (r.n_invalid || r.n_type_error)) {
       uint64_t fi = r.first_invalid == 0xFFFFFFFFu ? ~0ull : r.first_invalid;
       uint64_t ft = ~0ull, dummy = 0;
       if (warpjq_slot_first_errors) warpjq_slot_first_errors(q->ctx, f.slot, &dummy, &ft);
       uint64_t bad = std::min(fi, ft);
       return fail("malformed JSON on line " + std::to_string(first_line + (bad == ~0ull ? 0 : bad)) +
-                  " of <memory>: " + (fi <= ft ? "line is not valid JSON" : "a path hit a value of the wrong type") +
+                  " of " + name + ": " +
+                  (fi <= ft ? "line is not valid JSON" : "a path hit a value of the wrong type") +
                   "\n  help: pass --skip-invalid to drop bad lines instead of stopping");
     }
     if (P.is_aggregate()) {
@@ -535,9 +557,8 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
       w.bulk(r.out_bytes + r.out_row_off[0], (size_t)(r.out_row_off[r.n_selected] - r.out_row_off[0]),
              r.n_selected);
       // Size the output once from the first chunk's share of it.
-      const uint64_t done = (uint64_t)(f.data - data) + f.n;
-      if (!reserved && done < len) {
-        w.reserve_rows((size_t)((double)w.bulk_rows.n * (double)len / (double)done * 1.05));
+      if (!reserved && done_bytes < total) {
+        w.reserve_rows((size_t)((double)w.bulk_rows.n * (double)total / (double)done_bytes * 1.05));
         reserved = true;
       }
     }
@@ -545,48 +566,30 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
     return 0;
   };
 
-  // Page-locked input is copied to the device straight from the caller's
-  // memory; anything else is staged through the slots' pinned buffers.
-  const bool pinned = len && warpjq_host_is_pinned && warpjq_submit_host &&
-                      warpjq_host_is_pinned(data) && warpjq_host_is_pinned(data + len - 1);
-  // Tiles sized from the input's own line lengths (first MiB of the run).
-  if (!q->tiled && len) {
-    if (warpjq_autotile &&
-        warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
-        WARPJQ_OK)
-      return fail("CUDA error in choosing the device tiling");
+  // Tiles sized from the input's own line lengths (its first MiB).
+  auto tile = [&]() -> bool {
+    return !warpjq_autotile || !sample_len ||
+           warpjq_autotile(q->ctx, sample, std::min<uint64_t>(sample_len, 1ull << 20), nullptr,
+                           nullptr) == WARPJQ_OK;
+  };
+  if (!q->tiled) {
+    if (!tile()) return fail("CUDA error in choosing the device tiling");
     q->tiled = true;
   }
-  while (pos < len) {
-    // Next newline-aligned chunk of at most `cap` bytes (chunk.rs:234-278).
-    uint64_t want = std::min<uint64_t>(q->cap, len - pos);
-    uint64_t end = pos + want;
-    if (end < len) {
-      const uint8_t *nl = nullptr;
-      for (uint64_t k = end; k > pos; k--)
-        if (data[k - 1] == '\n') {
-          nl = data + k - 1;
-          break;
-        }
-      if (nl) {
-        end = (uint64_t)(nl - data) + 1;
-      } else {
-        // One line longer than a slot: grow the slots to hold it.
-        const uint8_t *n2 = (const uint8_t *)memchr(data + end, '\n', len - end);
-        end = n2 ? (uint64_t)(n2 - data) + 1 : len;
-      }
-    }
-    uint64_t n = end - pos;
+  Chunk c;
+  std::string why;
+  while (next(c, why)) {
+    const uint64_t n = c.n;
     // --max-line-bytes (chunk.rs:259-270): only a chunk without any newline
     // but its last byte can hold an over-long line.
     if (n > max_line_bytes) {
-      const uint8_t *inner = (const uint8_t *)memchr(data + pos, '\n', n - 1 > 0 ? n - 1 : 0);
+      const uint8_t *inner = (const uint8_t *)memchr(c.data, '\n', n - 1 > 0 ? n - 1 : 0);
       if (!inner)
         return fail("line " + std::to_string(lines_seen + 1) + " is at least " + std::to_string(n) +
                     " bytes, over the " + std::to_string(max_line_bytes) +
                     " byte limit (raise it with --max-line-bytes)");
     }
-    if (n > q->cap) {
+    if (n > q->cap) {  // one line longer than a slot: grow the slots to hold it
       for (auto &f : flight)
         if (drain(f)) return 1;
       flight.clear();
@@ -595,10 +598,7 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
       q->cap = n;
       if (warpjq_ctx_create(&q->low.prog, q->cap, q->n_slots, &q->ctx, e, sizeof e) != WARPJQ_OK)
         return fail(std::string("CUDA error in creating the device context: ") + e);
-      if (warpjq_autotile &&
-          warpjq_autotile(q->ctx, data, std::min<uint64_t>(len, 1ull << 20), nullptr, nullptr) !=
-          WARPJQ_OK)
-        return fail("CUDA error in choosing the device tiling");
+      if (!tile()) return fail("CUDA error in choosing the device tiling");
       next_slot = 0;
     }
     uint32_t slot = next_slot;
@@ -609,20 +609,20 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
       flight.erase(flight.begin());
     }
     warpjq_status sub;
-    if (pinned) {
-      sub = warpjq_submit_host(q->ctx, slot, data + pos, n, e, sizeof e);
+    if (c.pinned && warpjq_submit_host) {
+      sub = warpjq_submit_host(q->ctx, slot, c.data, n, e, sizeof e);
     } else {
-      copy_to_pinned(warpjq_slot_buffer(q->ctx, slot), data + pos, n);
+      copy_to_pinned(warpjq_slot_buffer(q->ctx, slot), c.data, n);
       sub = warpjq_submit(q->ctx, slot, n, e, sizeof e);
     }
     if (sub != WARPJQ_OK) return fail(std::string("CUDA error in submitting a chunk: ") + e);
-    flight.push_back({slot, data + pos, n});
+    flight.push_back({slot, c.data, n});
     if (flight.size() > 1) {
       if (drain(flight.front())) return 1;
       flight.erase(flight.begin());
     }
-    pos = end;
   }
+  if (!why.empty()) return fail(why);
   for (auto &f : flight)
     if (drain(f)) return 1;
 
@@ -641,7 +641,7 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
   char *res = w.finish(res_len);
   if (!res) return fail("out of host memory for the output");
   if (stats) {
-    stats[0] = len;
+    stats[0] = total;
     stats[1] = st_lines;
     stats[2] = rows;
     stats[3] = st_malformed;
@@ -650,6 +650,189 @@ int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t 
   *out = res;
   if (out_len) *out_len = res_len;
   return 0;
+}
+
+int warpjq_query_run(warpjq_query *q, const uint8_t *data, size_t len, uint32_t on_invalid,
+                     uint64_t max_line_bytes, char **out, size_t *out_len, uint64_t *stats,
+                     char *err, size_t err_len) {
+  // Strip a UTF-8 byte-order mark (chunk.rs:210-212).
+  size_t pos = (len >= 3 && data[0] == 0xEF && data[1] == 0xBB && data[2] == 0xBF) ? 3 : 0;
+  // Page-locked input is copied to the device straight from the caller's
+  // memory; anything else is staged through the slots' pinned buffers.
+  const bool pinned = len && warpjq_host_is_pinned && warpjq_submit_host &&
+                      warpjq_host_is_pinned(data) && warpjq_host_is_pinned(data + len - 1);
+  auto next = [&](Chunk &c, std::string &) -> bool {
+    if (pos >= len) return false;
+    // Next newline-aligned chunk of at most `cap` bytes (chunk.rs:234-278).
+    uint64_t end = pos + std::min<uint64_t>(q->cap, len - pos);
+    if (end < len) {
+      const uint8_t *nl = nullptr;
+      for (uint64_t k = end; k > pos; k--)
+        if (data[k - 1] == '\n') {
+          nl = data + k - 1;
+          break;
+        }
+      if (nl) {
+        end = (uint64_t)(nl - data) + 1;
+      } else {  // one line longer than a slot
+        const uint8_t *n2 = (const uint8_t *)memchr(data + end, '\n', len - end);
+        end = n2 ? (uint64_t)(n2 - data) + 1 : len;
+      }
+    }
+    c.data = data + pos;
+    c.n = end - pos;
+    c.pinned = pinned;
+    pos = end;
+    return true;
+  };
+  return run_chunks(q, len, data, len, next, "<memory>", on_invalid, max_line_bytes, out, out_len,
+                    stats, err, err_len);
+}
+
+int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid,
+                          uint64_t max_line_bytes, char **out, size_t *out_len, uint64_t *stats,
+                          char *err, size_t err_len) {
+  *out = nullptr;
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) {
+    put_err(err, err_len, std::string("cannot open ") + path + ": " + strerror(errno));
+    return 1;
+  }
+  struct stat sb;
+  if (fstat(fd, &sb) != 0) {
+    put_err(err, err_len, std::string("cannot stat ") + path + ": " + strerror(errno));
+    close(fd);
+    return 1;
+  }
+  const uint64_t size = (uint64_t)sb.st_size;
+  // Three page-locked buffers: the chunk being read, and the two the device
+  // may still be working on.  A buffer holds a chunk plus the partial line
+  // carried over from the one before.
+  uint64_t bufcap = std::max<uint64_t>(q->cap, 1 << 20) + (1 << 20);
+  std::vector<uint8_t *> bufs(3, nullptr);
+  // Page-locked when the backend provides it (then chunks are copied to the
+  // device straight from these buffers), plain memory otherwise.
+  const bool can_pin = warpjq_host_alloc_pinned && warpjq_host_free_pinned;
+  auto host_alloc = [&](uint64_t n) -> uint8_t * {
+    return can_pin ? (uint8_t *)warpjq_host_alloc_pinned(n) : (uint8_t *)malloc(n);
+  };
+  auto host_free = [&](uint8_t *b) {
+    if (can_pin) warpjq_host_free_pinned(b);
+    else free(b);
+  };
+  auto free_bufs = [&]() {
+    for (auto &b : bufs) {
+      if (b) host_free(b);
+      b = nullptr;
+    }
+  };
+  for (auto &b : bufs) {
+    b = host_alloc(bufcap);
+    if (!b) {
+      free_bufs();
+      close(fd);
+      put_err(err, err_len, "cannot allocate page-locked read buffers");
+      return 1;
+    }
+  }
+  const unsigned threads = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 16);
+  uint64_t pos = 0;          // file offset of the next byte to read
+  uint64_t carry_len = 0;    // bytes of a partial line waiting in `carry_from`
+  const uint8_t *carry_from = nullptr;
+  uint32_t k = 0;
+  bool first = true;
+  std::vector<uint8_t> sample;
+  {  // the first MiB, for the tiling
+    sample.resize(std::min<uint64_t>(size, 1 << 20));
+    if (!sample.empty() && pread(fd, sample.data(), sample.size(), 0) != (ssize_t)sample.size())
+      sample.clear();
+  }
+  // Reads [off, off + n) into dst with parallel preads.
+  auto read_range = [&](uint8_t *dst, uint64_t off, uint64_t n) -> bool {
+    if (n == 0) return true;
+    const uint64_t piece = std::max<uint64_t>((n + threads - 1) / threads, 1 << 20);
+    std::vector<std::thread> ws;
+    std::atomic<bool> ok{true};
+    for (uint64_t a = 0; a < n; a += piece) {
+      const uint64_t b = std::min(n, a + piece);
+      ws.emplace_back([&, a, b] {
+        uint64_t at = a;
+        while (at < b) {
+          ssize_t got = pread(fd, dst + at, b - at, (off_t)(off + at));
+          if (got <= 0) {
+            ok = false;
+            return;
+          }
+          at += (uint64_t)got;
+        }
+      });
+    }
+    for (auto &t : ws) t.join();
+    return ok;
+  };
+  auto next = [&](Chunk &c, std::string &why) -> bool {
+    if (pos >= size && carry_len == 0) return false;
+    uint8_t *buf = bufs[k % 3];
+    // the carried partial line first (it may come from the buffer of the
+    // chunk before, which the device no longer needs)
+    if (carry_len) memmove(buf, carry_from, carry_len);
+    uint64_t have = carry_len;
+    for (;;) {
+      const uint64_t want = std::min<uint64_t>(bufcap - have, size - pos);
+      if (!read_range(buf + have, pos, want)) {
+        why = std::string("read error on ") + path;
+        return false;
+      }
+      pos += want;
+      have += want;
+      uint64_t start = 0;
+      if (first) {  // a UTF-8 byte-order mark (chunk.rs:210-212)
+        first = false;
+        if (have >= 3 && buf[0] == 0xEF && buf[1] == 0xBB && buf[2] == 0xBF) start = 3;
+      }
+      if (pos >= size) {  // the rest of the file
+        c.data = buf + start;
+        c.n = have - start;
+        c.pinned = can_pin;
+        carry_len = 0;
+        break;
+      }
+      uint64_t end = have;
+      while (end > start && buf[end - 1] != '\n') end--;
+      if (end > start) {
+        c.data = buf + start;
+        c.n = end - start;
+        c.pinned = can_pin;
+        carry_from = buf + end;
+        carry_len = have - end;
+        break;
+      }
+      // No newline in a full buffer: a line longer than the buffers; grow
+      // them (the bytes read so far move to the new buffer).
+      uint8_t *big = host_alloc(bufcap * 2);
+      if (!big) {
+        why = "cannot allocate page-locked read buffers";
+        return false;
+      }
+      memcpy(big, buf, have);
+      host_free(buf);
+      bufs[k % 3] = big;
+      buf = big;
+      bufcap *= 2;
+      if (start) {
+        memmove(buf, buf + start, have - start);
+        have -= start;
+      }
+    }
+    if (c.n == 0 && pos >= size) return false;
+    k++;
+    return true;
+  };
+  int rc = run_chunks(q, size, sample.data(), sample.size(), next, path, on_invalid, max_line_bytes,
+                      out, out_len, stats, err, err_len);
+  free_bufs();
+  close(fd);
+  return rc;
 }
 
 int warpjq_run_bytes(const char *query, const uint8_t *data, size_t len, uint32_t format,
