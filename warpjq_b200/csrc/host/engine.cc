@@ -708,7 +708,9 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
   // Three page-locked buffers: the chunk being read, and the two the device
   // may still be working on.  A buffer holds a chunk plus the partial line
   // carried over from the one before.
-  uint64_t bufcap = std::max<uint64_t>(q->cap, 1 << 20) + (1 << 20);
+  // A chunk is filled up to the context's slot size (a larger one would make
+  // the run loop grow the context); only a longer line grows the buffers.
+  uint64_t bufcap = std::max<uint64_t>(q->cap, 1 << 16);
   std::vector<uint8_t *> bufs(3, nullptr);
   // Page-locked when the backend provides it (then chunks are copied to the
   // device straight from these buffers), plain memory otherwise.
@@ -740,7 +742,6 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
   uint64_t carry_len = 0;    // bytes of a partial line waiting in `carry_from`
   const uint8_t *carry_from = nullptr;
   uint32_t k = 0;
-  bool first = true;
   std::vector<uint8_t> sample;
   {  // the first MiB, for the tiling
     sample.resize(std::min<uint64_t>(size, 1 << 20));
@@ -770,63 +771,73 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
     for (auto &t : ws) t.join();
     return ok;
   };
+  std::vector<uint64_t> caps(bufs.size(), bufcap);  // each buffer's size
+  auto grow = [&](uint32_t bi, uint64_t keep) -> bool {
+    uint8_t *big = host_alloc(caps[bi] * 2);
+    if (!big) return false;
+    if (keep) memcpy(big, bufs[bi], keep);
+    host_free(bufs[bi]);
+    bufs[bi] = big;
+    caps[bi] *= 2;
+    return true;
+  };
   auto next = [&](Chunk &c, std::string &why) -> bool {
     if (pos >= size && carry_len == 0) return false;
-    uint8_t *buf = bufs[k % 3];
-    // the carried partial line first (it may come from the buffer of the
-    // chunk before, which the device no longer needs)
-    if (carry_len) memmove(buf, carry_from, carry_len);
+    const uint32_t bi = k % 3;
+    // The partial line carried over first (from the buffer of the chunk
+    // before, which the device does not read past that chunk's end).
+    while (caps[bi] < carry_len + 1)
+      if (!grow(bi, 0)) {
+        why = "cannot allocate page-locked read buffers";
+        return false;
+      }
+    if (carry_len) memmove(bufs[bi], carry_from, carry_len);
     uint64_t have = carry_len;
+    // Fill up to the context's slot size (a larger chunk would make the run
+    // loop grow the context); read on past it only for a longer line.
+    uint64_t limit = std::max<uint64_t>(std::min<uint64_t>(caps[bi], std::max<uint64_t>(q->cap, 1 << 16)),
+                                        have + 1);
     for (;;) {
-      const uint64_t want = std::min<uint64_t>(bufcap - have, size - pos);
-      if (!read_range(buf + have, pos, want)) {
+      const bool at_start = pos == 0;
+      const uint64_t want = std::min<uint64_t>(limit - have, size - pos);
+      if (!read_range(bufs[bi] + have, pos, want)) {
         why = std::string("read error on ") + path;
         return false;
       }
       pos += want;
       have += want;
-      uint64_t start = 0;
-      if (first) {  // a UTF-8 byte-order mark (chunk.rs:210-212)
-        first = false;
-        if (have >= 3 && buf[0] == 0xEF && buf[1] == 0xBB && buf[2] == 0xBF) start = 3;
+      uint8_t *buf = bufs[bi];
+      if (at_start && have >= 3 && buf[0] == 0xEF && buf[1] == 0xBB && buf[2] == 0xBF) {
+        memmove(buf, buf + 3, have - 3);  // a UTF-8 byte-order mark (chunk.rs:210-212)
+        have -= 3;
       }
       if (pos >= size) {  // the rest of the file
-        c.data = buf + start;
-        c.n = have - start;
+        c.data = buf;
+        c.n = have;
         c.pinned = can_pin;
         carry_len = 0;
         break;
       }
       uint64_t end = have;
-      while (end > start && buf[end - 1] != '\n') end--;
-      if (end > start) {
-        c.data = buf + start;
-        c.n = end - start;
+      while (end > 0 && buf[end - 1] != '\n') end--;
+      if (end > 0) {
+        c.data = buf;
+        c.n = end;
         c.pinned = can_pin;
         carry_from = buf + end;
         carry_len = have - end;
         break;
       }
-      // No newline in a full buffer: a line longer than the buffers; grow
-      // them (the bytes read so far move to the new buffer).
-      uint8_t *big = host_alloc(bufcap * 2);
-      if (!big) {
+      // No newline yet: a line longer than a chunk.  Read on, growing the
+      // buffer when it is full (the bytes read so far move with it).
+      if (have == caps[bi] && !grow(bi, have)) {
         why = "cannot allocate page-locked read buffers";
         return false;
       }
-      memcpy(big, buf, have);
-      host_free(buf);
-      bufs[k % 3] = big;
-      buf = big;
-      bufcap *= 2;
-      if (start) {
-        memmove(buf, buf + start, have - start);
-        have -= start;
-      }
+      limit = caps[bi];
     }
-    if (c.n == 0 && pos >= size) return false;
     k++;
-    return true;
+    return c.n > 0;
   };
   int rc = run_chunks(q, size, sample.data(), sample.size(), next, path, on_invalid, max_line_bytes,
                       out, out_len, stats, err, err_len);
