@@ -12,6 +12,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <memory>
+#include <mutex>
 #include <cerrno>
 #include <charconv>
 #include <functional>
@@ -365,6 +368,50 @@ struct Writer {
 
 using namespace wjqh;
 
+// A fixed set of threads for parallel reads: run(n, f) calls f(0..n-1) on
+// the workers and returns when all have finished.
+struct ReadPool {
+  std::vector<std::thread> ws;
+  std::mutex mu;
+  std::condition_variable cv, done_cv;
+  std::function<void(unsigned)> job;
+  unsigned n_jobs = 0, next_job = 0, done = 0;
+  bool stop = false;
+  explicit ReadPool(unsigned n) {
+    for (unsigned t = 0; t < n; t++)
+      ws.emplace_back([this] {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+          cv.wait(lk, [&] { return stop || next_job < n_jobs; });
+          if (stop) return;
+          const unsigned j = next_job++;
+          lk.unlock();
+          job(j);
+          lk.lock();
+          if (++done == n_jobs) done_cv.notify_all();
+        }
+      });
+  }
+  void run(unsigned n, std::function<void(unsigned)> f) {
+    std::unique_lock<std::mutex> lk(mu);
+    job = std::move(f);
+    next_job = 0;
+    done = 0;
+    n_jobs = n;
+    cv.notify_all();
+    done_cv.wait(lk, [&] { return done == n_jobs; });
+    n_jobs = 0;
+  }
+  ~ReadPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv.notify_all();
+    for (auto &w : ws) w.join();
+  }
+};
+
 struct warpjq_query {
   Program prog;
   Lowered low;
@@ -373,6 +420,22 @@ struct warpjq_query {
   uint64_t cap = 0;
   uint32_t n_slots = 2;
   bool tiled = false;  // device tiling chosen from the first bytes of a run
+  // file input: read buffers (page-locked when `rpinned`) and read threads,
+  // kept across runs
+  std::vector<uint8_t *> rbufs;
+  std::vector<uint64_t> rcaps;
+  bool rpinned = false;
+  std::unique_ptr<ReadPool> pool;
+  void free_read_bufs() {
+    for (auto &b : rbufs) {
+      if (!b) continue;
+      if (rpinned) warpjq_host_free_pinned(b);
+      else free(b);
+    }
+    rbufs.clear();
+    rcaps.clear();
+  }
+  ~warpjq_query() { free_read_bufs(); }
 };
 
 namespace {
@@ -705,15 +768,11 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
     return 1;
   }
   const uint64_t size = (uint64_t)sb.st_size;
-  // Three page-locked buffers: the chunk being read, and the two the device
-  // may still be working on.  A buffer holds a chunk plus the partial line
-  // carried over from the one before.
-  // A chunk is filled up to the context's slot size (a larger one would make
-  // the run loop grow the context); only a longer line grows the buffers.
-  uint64_t bufcap = std::max<uint64_t>(q->cap, 1 << 16);
-  std::vector<uint8_t *> bufs(3, nullptr);
-  // Page-locked when the backend provides it (then chunks are copied to the
-  // device straight from these buffers), plain memory otherwise.
+  // Three buffers, kept with the query across runs: the chunk being read,
+  // and the two the device may still be working on.  A chunk is filled up to
+  // the context's slot size (a larger one would make the run loop grow the
+  // context); only a longer line grows a buffer.  Page-locked when the
+  // backend provides it (chunks then go to the device straight from them).
   const bool can_pin = warpjq_host_alloc_pinned && warpjq_host_free_pinned;
   auto host_alloc = [&](uint64_t n) -> uint8_t * {
     return can_pin ? (uint8_t *)warpjq_host_alloc_pinned(n) : (uint8_t *)malloc(n);
@@ -722,21 +781,27 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
     if (can_pin) warpjq_host_free_pinned(b);
     else free(b);
   };
-  auto free_bufs = [&]() {
-    for (auto &b : bufs) {
-      if (b) host_free(b);
-      b = nullptr;
-    }
-  };
-  for (auto &b : bufs) {
-    b = host_alloc(bufcap);
-    if (!b) {
-      free_bufs();
+  const uint64_t bufcap = std::max<uint64_t>(q->cap, 1 << 16);
+  if (q->rbufs.size() != 3 || q->rpinned != can_pin) {
+    q->free_read_bufs();
+    q->rpinned = can_pin;
+    q->rbufs.assign(3, nullptr);
+    q->rcaps.assign(3, 0);
+  }
+  for (size_t i = 0; i < 3; i++) {
+    if (q->rbufs[i] && q->rcaps[i] >= bufcap) continue;
+    if (q->rbufs[i]) host_free(q->rbufs[i]);
+    q->rbufs[i] = host_alloc(bufcap);
+    q->rcaps[i] = bufcap;
+    if (!q->rbufs[i]) {
+      q->free_read_bufs();
       close(fd);
-      put_err(err, err_len, "cannot allocate page-locked read buffers");
+      put_err(err, err_len, "cannot allocate read buffers");
       return 1;
     }
   }
+  std::vector<uint8_t *> &bufs = q->rbufs;
+  std::vector<uint64_t> &caps = q->rcaps;
   const unsigned threads = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 16);
   uint64_t pos = 0;          // file offset of the next byte to read
   uint64_t carry_len = 0;    // bytes of a partial line waiting in `carry_from`
@@ -748,30 +813,26 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
     if (!sample.empty() && pread(fd, sample.data(), sample.size(), 0) != (ssize_t)sample.size())
       sample.clear();
   }
+  if (!q->pool) q->pool.reset(new ReadPool(threads));
   // Reads [off, off + n) into dst with parallel preads.
   auto read_range = [&](uint8_t *dst, uint64_t off, uint64_t n) -> bool {
     if (n == 0) return true;
     const uint64_t piece = std::max<uint64_t>((n + threads - 1) / threads, 1 << 20);
-    std::vector<std::thread> ws;
+    const unsigned parts = (unsigned)((n + piece - 1) / piece);
     std::atomic<bool> ok{true};
-    for (uint64_t a = 0; a < n; a += piece) {
-      const uint64_t b = std::min(n, a + piece);
-      ws.emplace_back([&, a, b] {
-        uint64_t at = a;
-        while (at < b) {
-          ssize_t got = pread(fd, dst + at, b - at, (off_t)(off + at));
-          if (got <= 0) {
-            ok = false;
-            return;
-          }
-          at += (uint64_t)got;
+    q->pool->run(parts, [&](unsigned j) {
+      const uint64_t a = (uint64_t)j * piece, b = std::min(n, a + piece);
+      for (uint64_t at = a; at < b;) {
+        const ssize_t got = pread(fd, dst + at, b - at, (off_t)(off + at));
+        if (got <= 0) {
+          ok = false;
+          return;
         }
-      });
-    }
-    for (auto &t : ws) t.join();
+        at += (uint64_t)got;
+      }
+    });
     return ok;
   };
-  std::vector<uint64_t> caps(bufs.size(), bufcap);  // each buffer's size
   auto grow = [&](uint32_t bi, uint64_t keep) -> bool {
     uint8_t *big = host_alloc(caps[bi] * 2);
     if (!big) return false;
@@ -841,7 +902,6 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
   };
   int rc = run_chunks(q, size, sample.data(), sample.size(), next, path, on_invalid, max_line_bytes,
                       out, out_len, stats, err, err_len);
-  free_bufs();
   close(fd);
   return rc;
 }
