@@ -230,6 +230,60 @@ warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, const uint8_t
                                        uint64_t n_bytes, void *stream,
                                        warpjq_noalloc_result *d_result, char *err, size_t err_len);
 
+/* CSV input.  The reference reads NDJSON only (its --csv flag formats
+ * output, crates/warpjq-core/src/output.rs:45-85); these entry points have
+ * no reference counterpart.  A converter turns RFC 4180 CSV into NDJSON in
+ * device memory, which any query then scans like other input:
+ *   - a '\n' ends a row when an even number of '"' bytes precede it; a
+ *     '\r' before it is dropped;
+ *   - the first row is the header (a UTF-8 byte-order mark before it is
+ *     dropped); each later row becomes one line, an empty row an empty line;
+ *   - fields are split at ','; a field starting with '"' is quoted up to the
+ *     next '"' not doubled, "" inside it stands for '"', and bytes after the
+ *     closing quote up to the next ',' are kept;
+ *   - a row is an object of the header's names, in order, over its first
+ *     min(fields, names) fields;
+ *   - an unquoted field that is a JSON number stays a number, an unquoted
+ *     empty field is null, anything else is a JSON string (escaped like
+ *     the names).
+ * Line i of the NDJSON is data row i (the scan's line numbers are row
+ * numbers after the header). */
+typedef struct warpjq_csv warpjq_csv;
+
+#define WARPJQ_CSV_FINAL 1u      /* the input ends with this chunk */
+#define WARPJQ_CSV_HOST_INPUT 2u /* `src` is host memory (copied to the device first) */
+
+warpjq_status warpjq_csv_create(warpjq_csv **out);
+void warpjq_csv_destroy(warpjq_csv *c);
+
+/* The next chunk converted starts a new input (its first row is a header). */
+void warpjq_csv_reset(warpjq_csv *c);
+
+/* Converts the rows of one chunk, n bytes at `src` (device memory unless
+ * WARPJQ_CSV_HOST_INPUT), enqueued on `stream` with a few host waits.  An
+ * input can arrive in chunks: each chunk must start where the previous
+ * one's *consumed bytes ended; without WARPJQ_CSV_FINAL, bytes after the last
+ * row-ending newline are not consumed (pass them again at the start of the
+ * next chunk), and a chunk with no whole row consumes nothing.  The header
+ * row's names are kept for the later chunks until warpjq_csv_reset.
+ * *d_ndjson (in the converter's memory, valid until its next call) holds
+ * *ndjson_len bytes of NDJSON, one line per data row converted
+ * (*records, may be null). */
+warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, uint32_t flags,
+                                 void *stream, const uint8_t **d_ndjson, uint64_t *ndjson_len,
+                                 uint64_t *consumed, uint64_t *records, char *err, size_t err_len);
+
+/* Copies the device byte slices d_src[offsets[i], + lengths[i]), i < n, to
+ * host memory h_dst back to back (e.g. the group keys of a run over
+ * converted CSV, whose NDJSON lives only on the device).  Synchronous. */
+warpjq_status warpjq_csv_gather(warpjq_csv *c, const uint8_t *d_src, const uint64_t *offsets,
+                                const uint32_t *lengths, uint64_t n, uint8_t *h_dst, void *stream,
+                                char *err, size_t err_len);
+
+/* Copies n bytes of device memory to host memory on `stream` and waits. */
+warpjq_status warpjq_device_read(void *h_dst, const void *d_src, uint64_t n, void *stream,
+                                 char *err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,18 @@ int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r,
 
 void warpjq_host_free(void *p);
 
+/* Runs the query over RFC 4180 CSV input in host memory: the header row
+ * names the keys and each later row is one object, converted on the device
+ * by the mapping warpjq_ext.h gives for warpjq_csv_convert, then scanned like
+ * NDJSON.  Output, stats and return codes as warpjq_query_run (rows that a
+ * query passes through print as the converted NDJSON; --strict errors name
+ * the data row, counted after the header).  Chunks of the context's chunk
+ * size are converted and scanned one after another.  The query must have a
+ * device context (warpjq_query_open).  No reference counterpart: the
+ * reference reads NDJSON only. */
+int warpjq_query_run_csv(warpjq_query *q, const uint8_t *data, size_t len, uint32_t on_invalid,
+                         char **out, size_t *out_len, uint64_t *stats, char *err, size_t err_len);
+
 /* Seeded synthetic input in the benchmark's nginx-style schema (keys ts,
  * host, method, path, status, bytes, latency_ms, ua).  Writes whole lines,
  * about `target` bytes, into out (capacity >= target), generating blocks of
@@ -84,6 +96,14 @@ uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t
                           unsigned threads, uint64_t *total_lines);
 uint64_t warpjq_gen_nginx_block(uint64_t seed, uint64_t block, uint64_t first_line, uint8_t *out,
                                 uint64_t cap, uint64_t *n_lines);
+
+/* The same records rendered as CSV: a header row naming the columns
+ * (ts,host,method,path,status,bytes,latency_ms,ua), then one row per record
+ * with ua always quoted ('"' doubled).  Returns the bytes written. */
+uint64_t warpjq_gen_nginx_csv(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                              unsigned threads, uint64_t *total_lines);
+uint64_t warpjq_gen_nginx_csv_block(uint64_t seed, uint64_t block, uint64_t first_line, uint8_t *out,
+                                    uint64_t cap, uint64_t *n_lines);
 
 /* The same for a nested, dirty schema: objects 3-5 levels deep with shuffled
  * key order (req.user.{id, tier, geo{cc, lat, lon}}, req.method, req.path,

@@ -36,13 +36,15 @@ EXT_SYMBOLS = [
     "warpjq_launch_device", "warpjq_collect_device", "warpjq_slot_first_errors",
     "warpjq_set_tiling", "warpjq_autotile", "warpjq_submit_host", "warpjq_host_is_pinned",
     "warpjq_batch_launch", "warpjq_batch_collect", "warpjq_host_alloc_pinned",
-    "warpjq_host_free_pinned",
+    "warpjq_host_free_pinned", "warpjq_csv_create", "warpjq_csv_destroy", "warpjq_csv_reset",
+    "warpjq_csv_convert", "warpjq_csv_gather", "warpjq_device_read",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
     "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
     "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
-    "warpjq_gen_nested", "warpjq_gen_nested_block", "warpjq_query_run_file",
+    "warpjq_gen_nested", "warpjq_gen_nested_block", "warpjq_query_run_file", "warpjq_query_run_csv",
+    "warpjq_gen_nginx_csv", "warpjq_gen_nginx_csv_block",
 ]
 
 
@@ -101,6 +103,18 @@ def _load():
     h.warpjq_query_run_file.argtypes = [vp, cp, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
                                         ctypes.POINTER(u64), cp, sz]
     h.warpjq_query_run_file.restype = ctypes.c_int
+    k.warpjq_csv_create.argtypes = [ctypes.POINTER(vp)]
+    k.warpjq_csv_create.restype = ctypes.c_int
+    k.warpjq_csv_destroy.argtypes = [vp]
+    k.warpjq_csv_reset.argtypes = [vp]
+    k.warpjq_csv_convert.argtypes = [vp, vp, u64, u32, vp, ctypes.POINTER(vp), ctypes.POINTER(u64),
+                                     ctypes.POINTER(u64), ctypes.POINTER(u64), cp, sz]
+    k.warpjq_csv_convert.restype = ctypes.c_int
+    h.warpjq_query_run_csv.argtypes = [vp, vp, sz, u32, ctypes.POINTER(vp), ctypes.POINTER(sz),
+                                       ctypes.POINTER(u64), cp, sz]
+    h.warpjq_query_run_csv.restype = ctypes.c_int
+    h.warpjq_gen_nginx_csv.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
+    h.warpjq_gen_nginx_csv.restype = u64
     h.warpjq_run_bytes.argtypes = [cp, cp, sz, u32, u32, u64, u64, ctypes.POINTER(vp),
                                    ctypes.POINTER(sz), ctypes.POINTER(u64), cp, sz]
     h.warpjq_run_bytes.restype = ctypes.c_int
@@ -306,6 +320,24 @@ class Query:
         body = _take(out, n) if copy_out else _view(out, n)
         return RunResult(rc, body, _stats(st), err.value.decode(errors="replace"))
 
+    def run_csv(self, data, on_invalid: str = "skip", copy_out: bool = True) -> RunResult:
+        """Runs over CSV in host memory (bytes or a numpy uint8 array): the
+        header names the keys, each later row is one object, converted on
+        the device (warpjq_query_run_csv)."""
+        if isinstance(data, (bytes, bytearray)):
+            keep = ctypes.c_char_p(bytes(data))
+            addr, n_bytes = ctypes.cast(keep, ctypes.c_void_p), len(data)
+        else:
+            addr, n_bytes = ctypes.c_void_p(data.ctypes.data), int(data.nbytes)
+        out = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        st = (ctypes.c_uint64 * 5)()
+        err = ctypes.create_string_buffer(4096)
+        rc = self._h.warpjq_query_run_csv(self._q, addr, n_bytes, ON_INVALID[on_invalid], ctypes.byref(out),
+                                          ctypes.byref(n), st, err, len(err))
+        body = _take(out, n) if copy_out else _view(out, n)
+        return RunResult(rc, body, _stats(st), err.value.decode(errors="replace"))
+
     def set_tiling(self, tile_bytes: int = 0, halo_bytes: int = 0):
         k, _ = _load()
         if k.warpjq_set_tiling(self.ctx, tile_bytes, halo_bytes) != 0:
@@ -416,6 +448,49 @@ class Query:
         return _take(out, n)
 
 
+class CsvConverter:
+    """RFC 4180 CSV to NDJSON in device memory (warpjq_ext.h
+    warpjq_csv_convert): the header row names the keys, each later row
+    becomes one line."""
+
+    def __init__(self):
+        k, _ = _load()
+        self._k = k
+        self._c = ctypes.c_void_p()
+        if k.warpjq_csv_create(ctypes.byref(self._c)):
+            raise MemoryError("warpjq_csv_create")
+
+    def reset(self):
+        """The next chunk starts a new input (with a header row)."""
+        self._k.warpjq_csv_reset(self._c)
+
+    def convert(self, src: int, n: int, final: bool = True, host: bool = False, stream: int = 0):
+        """Converts n bytes at address src (device memory, or host memory
+        with host=True).  Returns (device address, NDJSON bytes, bytes
+        consumed, data rows); the NDJSON stays valid until the next call."""
+        d = ctypes.c_void_p()
+        nd, used, recs = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        err = ctypes.create_string_buffer(1024)
+        flags = (1 if final else 0) | (2 if host else 0)
+        rc = self._k.warpjq_csv_convert(self._c, ctypes.c_void_p(src), n, flags, ctypes.c_void_p(stream),
+                                        ctypes.byref(d), ctypes.byref(nd), ctypes.byref(used),
+                                        ctypes.byref(recs), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+        return (d.value or 0), nd.value, used.value, recs.value
+
+    def close(self):
+        if self._c:
+            self._k.warpjq_csv_destroy(self._c)
+            self._c = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def probe() -> str:
     """'' when a usable sm_100 device is present, else the reason."""
     k, _ = _load()
@@ -440,6 +515,17 @@ def gen_nested(n_bytes: int, seed: int = 1, n_users: int = 1_000_000, threads: i
     lines = ctypes.c_uint64()
     used = h.warpjq_gen_nested(seed, buf.ctypes.data, n_bytes, 1 << 20, threads, n_users,
                                ctypes.byref(lines))
+    return buf, int(used), int(lines.value)
+
+
+def gen_nginx_csv(n_bytes: int, seed: int = 1, threads: int = 0, into=None):
+    """About n_bytes of the nginx records as CSV (a header row, then one row
+    per record, ua quoted); returns (buffer, used_bytes, n_rows)."""
+    import numpy as np
+    _, h = _load()
+    buf = into if into is not None else np.empty(n_bytes, dtype=np.uint8)
+    lines = ctypes.c_uint64()
+    used = h.warpjq_gen_nginx_csv(seed, buf.ctypes.data, n_bytes, 1 << 20, threads, ctypes.byref(lines))
     return buf, int(used), int(lines.value)
 
 

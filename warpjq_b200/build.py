@@ -24,11 +24,12 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
-KERNEL_SRCS = [os.path.join(CSRC, "backend.cu"), os.path.join(CSRC, "noalloc.cu")]
+KERNEL_SRCS = [os.path.join(CSRC, "backend.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "csv.cu")]
 KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "plan.h")]
 HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc")]
 CLI_SRCS = [os.path.join(CSRC, "host", "cli.cc")]
 HEADERS = [os.path.join(ROOT, "include", f) for f in ("warpjq_kernels.h", "warpjq_ext.h", "warpjq_host.h")]
+EXPORTS = os.path.join(CSRC, "exports.map")  # only the C ABI is exported
 
 
 def _stale(target, deps):
@@ -46,10 +47,11 @@ def _run(cmd):
 def build(force: bool = False, verbose_ptxas: bool = False) -> None:
     os.makedirs(LIB, exist_ok=True)
     so = os.path.join(LIB, "libwarpjq_kernels.so")
-    deps = KERNEL_SRCS + KERNEL_DEPS + HEADERS
+    deps = KERNEL_SRCS + KERNEL_DEPS + HEADERS + [EXPORTS]
     if force or _stale(so, deps):
         extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-        _run([NVCC, *NVFLAGS, *extra, "-shared", "-o", so, *KERNEL_SRCS])
+        _run([NVCC, *NVFLAGS, *extra, "-shared", "-Xlinker", "--version-script=" + EXPORTS, "-o", so,
+              *KERNEL_SRCS])
     static = os.path.join(LIB, "libwarpjq_kernels.a")
     if force or _stale(static, deps):
         objs = []
@@ -63,9 +65,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> None:
         for obj in objs:
             os.remove(obj)
     host = os.path.join(LIB, "libwarpjq_host.so")
-    hdeps = HOST_SRCS + [os.path.join(CSRC, "host", "query.h")] + HEADERS + [so]
+    hdeps = HOST_SRCS + [os.path.join(CSRC, "host", "query.h")] + HEADERS + [so, EXPORTS]
     if force or _stale(host, hdeps):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", host, *HOST_SRCS,
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wl,--version-script=" + EXPORTS, "-o", host,
+              *HOST_SRCS,
               "-L" + LIB, "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN", "-lpthread"])
     cli = os.path.join(LIB, "warpjq")
     if all(os.path.exists(s) for s in CLI_SRCS) and (force or _stale(cli, CLI_SRCS + [host])):

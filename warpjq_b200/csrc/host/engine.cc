@@ -38,6 +38,14 @@
 #pragma weak warpjq_slot_first_errors
 #pragma weak warpjq_host_alloc_pinned
 #pragma weak warpjq_host_free_pinned
+#pragma weak warpjq_launch_device
+#pragma weak warpjq_collect_device
+#pragma weak warpjq_csv_create
+#pragma weak warpjq_csv_destroy
+#pragma weak warpjq_csv_reset
+#pragma weak warpjq_csv_convert
+#pragma weak warpjq_csv_gather
+#pragma weak warpjq_device_read
 #include "query.h"
 
 namespace wjqh {
@@ -426,6 +434,10 @@ struct warpjq_query {
   std::vector<uint64_t> rcaps;
   bool rpinned = false;
   std::unique_ptr<ReadPool> pool;
+  // CSV input: the converter and a page-locked staging buffer
+  warpjq_csv *csv = nullptr;
+  uint8_t *csv_stage = nullptr;
+  uint64_t csv_stage_cap = 0;
   void free_read_bufs() {
     for (auto &b : rbufs) {
       if (!b) continue;
@@ -435,7 +447,11 @@ struct warpjq_query {
     rbufs.clear();
     rcaps.clear();
   }
-  ~warpjq_query() { free_read_bufs(); }
+  ~warpjq_query() {
+    free_read_bufs();
+    if (csv_stage) warpjq_host_free_pinned(csv_stage);
+    if (csv) warpjq_csv_destroy(csv);
+  }
 };
 
 namespace {
@@ -904,6 +920,143 @@ int warpjq_query_run_file(warpjq_query *q, const char *path, uint32_t on_invalid
                       out, out_len, stats, err, err_len);
   close(fd);
   return rc;
+}
+
+// CSV input (warpjq_host.h): chunks of the input are converted to NDJSON on
+// the device (warpjq_csv_convert) and scanned there (warpjq_launch_device),
+// one chunk at a time; rows and aggregates merge in input order as for
+// NDJSON, and group keys are gathered from the device copy.
+int warpjq_query_run_csv(warpjq_query *q, const uint8_t *data, size_t len, uint32_t on_invalid,
+                         char **out, size_t *out_len, uint64_t *stats, char *err, size_t err_len) {
+  *out = nullptr;
+  if (out_len) *out_len = 0;
+  auto fail = [&](const std::string &m) {
+    put_err(err, err_len, m);
+    return 1;
+  };
+  if (!warpjq_csv_convert || !warpjq_launch_device || !warpjq_collect_device || !warpjq_host_alloc_pinned)
+    return fail("this device backend has no CSV input");
+  if (!q->ctx) return fail("the query has no device context");
+  if (!q->csv && warpjq_csv_create(&q->csv) != WARPJQ_OK) return fail("out of memory for the CSV converter");
+  warpjq_csv_reset(q->csv);
+  const Program &P = q->prog;
+  Writer w;
+  w.fmt = q->fmt;
+  w.header(P);
+  Totals tot;
+  uint64_t st_lines = 0, st_malformed = 0, st_type = 0, records = 0;
+  char e[512] = {0};
+  const bool pinned = len && warpjq_host_is_pinned && warpjq_host_is_pinned(data) &&
+                      warpjq_host_is_pinned(data + len - 1);
+  uint64_t cap = std::max<uint64_t>(q->cap, 1 << 20);
+  std::vector<uint64_t> k_off;
+  std::vector<uint32_t> k_len;
+  std::vector<uint8_t> k_bytes, rows;
+  uint64_t pos = 0;
+  for (;;) {
+    const uint64_t n = std::min<uint64_t>(cap, len - pos);
+    const bool final_ = pos + n == len;
+    const uint8_t *src = data + pos;
+    if (!pinned && n) {
+      if (q->csv_stage_cap < n) {
+        if (q->csv_stage) warpjq_host_free_pinned(q->csv_stage);
+        q->csv_stage = (uint8_t *)warpjq_host_alloc_pinned(n);
+        q->csv_stage_cap = q->csv_stage ? n : 0;
+        if (!q->csv_stage) return fail("out of page-locked host memory for the CSV input");
+      }
+      copy_to_pinned(q->csv_stage, src, n);
+      src = q->csv_stage;
+    }
+    const uint8_t *d_nd = nullptr;
+    uint64_t nd_len = 0, used = 0, recs = 0;
+    if (warpjq_csv_convert(q->csv, src, n, WARPJQ_CSV_HOST_INPUT | (final_ ? WARPJQ_CSV_FINAL : 0u), nullptr,
+                           &d_nd, &nd_len, &used, &recs, e, sizeof e) != WARPJQ_OK)
+      return fail(std::string("CUDA error in converting CSV: ") + e);
+    if (!final_ && used == 0) {  // one row longer than a chunk
+      cap *= 2;
+      continue;
+    }
+    if (nd_len && !q->tiled && warpjq_autotile) {  // tiles shaped by the converted lines
+      std::vector<uint8_t> sample((size_t)std::min<uint64_t>(nd_len, 1 << 20));
+      if (warpjq_device_read(sample.data(), d_nd, sample.size(), nullptr, e, sizeof e) != WARPJQ_OK ||
+          warpjq_autotile(q->ctx, sample.data(), sample.size(), nullptr, nullptr) != WARPJQ_OK)
+        return fail("CUDA error in choosing the device tiling");
+      q->tiled = true;
+    }
+    if (nd_len) {
+      warpjq_device_result r;
+      if (warpjq_launch_device(q->ctx, d_nd, nd_len, nullptr, e, sizeof e) != WARPJQ_OK ||
+          warpjq_collect_device(q->ctx, &r, e, sizeof e) != WARPJQ_OK)
+        return fail(std::string("CUDA error in scanning converted CSV: ") + e);
+      st_lines += r.n_lines - r.n_blank;
+      st_malformed += r.n_invalid;
+      st_type += r.n_type_error;
+      if (on_invalid == WARPJQ_ON_INVALID_ABORT && (r.n_invalid || r.n_type_error)) {
+        const uint64_t bad = std::min(r.first_invalid, r.first_type_error);
+        return fail("bad value in CSV row " + std::to_string(records + bad + 1) + " (after the header): " +
+                    (r.first_invalid <= r.first_type_error ? "row is not valid JSON once converted"
+                                                           : "a path hit a value of the wrong type") +
+                    "\n  help: pass --skip-invalid to drop bad rows instead of stopping");
+      }
+      if (P.is_aggregate()) {
+        if (!P.has_group) {
+          tot.scalar.merge(r.count, r.numeric, r.sum, r.min, r.max);
+        } else if (r.n_groups) {
+          k_off.resize(r.n_groups);
+          k_len.resize(r.n_groups);
+          uint64_t kb = 0;
+          for (uint32_t k = 0; k < r.n_groups; k++) {
+            k_off[k] = r.groups[k].key_off;
+            k_len[k] = r.groups[k].key_len;
+            kb += k_len[k];
+          }
+          k_bytes.resize(kb + 1);
+          if (warpjq_csv_gather(q->csv, d_nd, k_off.data(), k_len.data(), r.n_groups, k_bytes.data(), nullptr, e,
+                                sizeof e) != WARPJQ_OK)
+            return fail(std::string("CUDA error in reading group keys: ") + e);
+          uint64_t at = 0;
+          for (uint32_t k = 0; k < r.n_groups; k++) {
+            const warpjq_group_ext &g = r.groups[k];
+            tot.groups[device_key(k_bytes.data(), at, g.key_len, g.key_kind)].merge(g.count, g.numeric, g.sum,
+                                                                                     g.min, g.max);
+            at += g.key_len;
+          }
+        }
+      } else if (r.n_selected) {
+        rows.resize(r.out_len + 1);
+        if (warpjq_device_read(rows.data(), r.d_out_bytes, r.out_len, nullptr, e, sizeof e) != WARPJQ_OK)
+          return fail(std::string("CUDA error in reading rows: ") + e);
+        w.bulk(rows.data(), (size_t)r.out_len, r.n_selected);
+        if (w.oom) return fail("out of host memory for the output");
+      }
+    }
+    records += recs;
+    pos += used;
+    if (final_) break;
+  }
+  if (P.is_aggregate()) {
+    if (!P.has_group) {
+      w.aggregate(P.agg, tot.scalar);
+    } else {
+      std::vector<std::pair<GroupKey, Agg>> gs(tot.groups.begin(), tot.groups.end());
+      std::sort(gs.begin(), gs.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+      w.groups(P.group_key_name(), P.agg, gs);
+    }
+  }
+  const uint64_t n_rows = w.rows;
+  size_t res_len = 0;
+  char *res = w.finish(res_len);
+  if (!res) return fail("out of host memory for the output");
+  if (stats) {
+    stats[0] = len;
+    stats[1] = st_lines;
+    stats[2] = n_rows;
+    stats[3] = st_malformed;
+    stats[4] = st_type;
+  }
+  *out = res;
+  if (out_len) *out_len = res_len;
+  return 0;
 }
 
 int warpjq_run_bytes(const char *query, const uint8_t *data, size_t len, uint32_t format,

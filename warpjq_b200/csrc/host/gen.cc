@@ -1,4 +1,5 @@
-// Seeded synthetic NDJSON for benchmarks and tests.
+// Seeded synthetic NDJSON (and a CSV rendering of the nginx schema) for
+// benchmarks and tests.
 //
 // The nginx-style schema of the benchmark workload: keys in fixed order
 //   ts          1700000000 + line index + uniform jitter 0..3
@@ -95,26 +96,30 @@ char *put_u64(char *p, uint64_t v) {
   return p;
 }
 
-// Writes one line (with '\n') for line index `i`; returns the end.
-char *nginx_line(char *p, Rng &r, uint64_t i) {
-  p = put(p, "{\"ts\":");
+// Writes one line (with '\n') for line index `i`; returns the end.  With
+// `csv` the same draws render as a CSV row of the columns in key order, ua
+// always quoted (a '"' inside doubled).
+char *nginx_line(char *p, Rng &r, uint64_t i, bool csv = false) {
+  const char *sep_host = csv ? "," : ",\"host\":\"", *sep_method = csv ? "," : "\",\"method\":\"";
+  const char *sep_path = csv ? "," : "\",\"path\":\"", *sep_status = csv ? "," : "\",\"status\":";
+  if (!csv) p = put(p, "{\"ts\":");
   p = put_u64(p, 1700000000ull + i + r.below(4));
-  p = put(p, ",\"host\":\"");
+  p = put(p, sep_host);
   p = put(p, kHosts[r.below(8)]);
-  p = put(p, "\",\"method\":\"");
+  p = put(p, sep_method);
   uint32_t m = r.below(100);
   p = put(p, m < 70 ? "GET" : m < 90 ? "POST" : m < 95 ? "PUT" : "DELETE");
-  p = put(p, "\",\"path\":\"");
+  p = put(p, sep_path);
   double u = r.uniform();
   int k = 0;
   while (k < 31 && u > kT.path_cdf[k]) k++;
   p = put(p, kPaths[k]);
-  p = put(p, "\",\"status\":");
+  p = put(p, sep_status);
   uint32_t s = r.below(100);
   p = put(p, s < 80 ? "200" : s < 85 ? "304" : s < 94 ? "404" : s < 99 ? "500" : "503");
-  p = put(p, ",\"bytes\":");
+  p = put(p, csv ? "," : ",\"bytes\":");
   p = put_u64(p, (uint64_t)std::floor(std::exp(std::log(100.0) + r.uniform() * (std::log(1e7) - std::log(100.0)))));
-  p = put(p, ",\"latency_ms\":");
+  p = put(p, csv ? "," : ",\"latency_ms\":");
   double lat = std::exp(3.0 + r.normal());
   uint64_t milli = (uint64_t)std::llround(lat * 1000.0);
   p = put_u64(p, milli / 1000);
@@ -123,14 +128,14 @@ char *nginx_line(char *p, Rng &r, uint64_t i) {
   *p++ = (char)('0' + f / 100);
   *p++ = (char)('0' + f / 10 % 10);
   *p++ = (char)('0' + f % 10);
-  p = put(p, ",\"ua\":\"");
+  p = put(p, csv ? ",\"" : ",\"ua\":\"");
   uint32_t n = 40 + r.below(81);
   for (uint32_t j = 0; j < n; j++) {
     char c = (char)(0x20 + r.below(95));
-    if (c == '"' || c == '\\') *p++ = '\\';
+    if (csv ? c == '"' : (c == '"' || c == '\\')) *p++ = csv ? '"' : '\\';
     *p++ = c;
   }
-  p = put(p, "\"}\n");
+  p = put(p, csv ? "\"\n" : "\"}\n");
   return p;
 }
 
@@ -327,11 +332,25 @@ uint64_t warpjq_gen_nginx_block(uint64_t seed, uint64_t block, uint64_t first_li
   return (uint64_t)(p - (char *)out);
 }
 
+// The same records as CSV rows (no header), like warpjq_gen_nginx_block.
+uint64_t warpjq_gen_nginx_csv_block(uint64_t seed, uint64_t block, uint64_t first_line, uint8_t *out,
+                                    uint64_t cap, uint64_t *n_lines) {
+  Rng r(seed * 0x100000001B3ull ^ (block * 0xD1B54A32D192ED03ull));
+  char *p = (char *)out, *end = (char *)out + cap;
+  uint64_t i = first_line;
+  while (end - p >= 512) {
+    p = nginx_line(p, r, i, true);
+    i++;
+  }
+  if (n_lines) *n_lines = i - first_line;
+  return (uint64_t)(p - (char *)out);
+}
+
 // Generates about `target` bytes of nginx NDJSON into `out` (capacity cap
 // >= target), in parallel blocks of `block_bytes`.  Each block is padded
 // with its lines only (no partial lines).  Returns the bytes written.
 static uint64_t gen_parallel(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
-                             unsigned threads, uint64_t *total_lines, uint64_t n_users, bool nested) {
+                             unsigned threads, uint64_t *total_lines, uint64_t n_users, int kind) {
   if (block_bytes < 4096) block_bytes = 4096;
   uint64_t nb = (target + block_bytes - 1) / block_bytes;
   std::vector<uint64_t> len(nb), lines(nb);
@@ -344,10 +363,11 @@ static uint64_t gen_parallel(uint64_t seed, uint8_t *out, uint64_t target, uint6
         // Blocks are generated in place at their nominal offset; lines of a
         // block never cross into the next block.
         uint64_t cap = std::min<uint64_t>(block_bytes, target - b * block_bytes);
-        len[b] = nested ? warpjq_gen_nested_block(seed, b, b * (block_bytes / 64), n_users,
-                                                  out + b * block_bytes, cap, &lines[b])
-                        : warpjq_gen_nginx_block(seed, b, b * (block_bytes / 64), out + b * block_bytes,
-                                                 cap, &lines[b]);
+        uint8_t *o = out + b * block_bytes;
+        const uint64_t first = b * (block_bytes / 64);
+        len[b] = kind == 1   ? warpjq_gen_nested_block(seed, b, first, n_users, o, cap, &lines[b])
+                 : kind == 2 ? warpjq_gen_nginx_csv_block(seed, b, first, o, cap, &lines[b])
+                             : warpjq_gen_nginx_block(seed, b, first, o, cap, &lines[b]);
       }
     });
   }
@@ -365,14 +385,28 @@ static uint64_t gen_parallel(uint64_t seed, uint8_t *out, uint64_t target, uint6
 
 uint64_t warpjq_gen_nginx(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
                           unsigned threads, uint64_t *total_lines) {
-  return gen_parallel(seed, out, target, block_bytes, threads, total_lines, 0, false);
+  return gen_parallel(seed, out, target, block_bytes, threads, total_lines, 0, 0);
 }
 
 // Generates about `target` bytes of the nested schema with user ids drawn
 // from [1, n_users].
 uint64_t warpjq_gen_nested(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
                            unsigned threads, uint64_t n_users, uint64_t *total_lines) {
-  return gen_parallel(seed, out, target, block_bytes, threads, total_lines, n_users, true);
+  return gen_parallel(seed, out, target, block_bytes, threads, total_lines, n_users, 1);
+}
+
+// About `target` bytes of the nginx records as CSV: a header row naming the
+// columns (ts,host,method,path,status,bytes,latency_ms,ua), then the rows.
+uint64_t warpjq_gen_nginx_csv(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                              unsigned threads, uint64_t *total_lines) {
+  static const char kHead[] = "ts,host,method,path,status,bytes,latency_ms,ua\n";
+  const uint64_t h = sizeof kHead - 1;
+  if (target < h) {
+    if (total_lines) *total_lines = 0;
+    return 0;
+  }
+  memcpy(out, kHead, h);
+  return h + gen_parallel(seed, out + h, target - h, block_bytes, threads, total_lines, 0, 2);
 }
 
 }  // extern "C"
