@@ -326,7 +326,7 @@ def measure_nested(wjq, n_bytes=2_000_000_000, reps=3):
 CSV_QUERY = "group_by(.path) | max(.latency_ms)"
 
 
-def measure_csv(wjq, n_bytes=2_000_000_000, reps=3):
+def measure_csv(wjq, n_bytes=2_000_000_000, reps=3, e2e=True):
     """The nginx records as 2 GB of CSV (RFC 4180 quoting on ua), query
     group_by(.path) | max(.latency_ms).  Device-resident GB/s of CSV bytes
     (conversion to NDJSON on the device plus the scan; CUDA events around
@@ -358,21 +358,23 @@ def measure_csv(wjq, n_bytes=2_000_000_000, reps=3):
     Q.close()
     conv.close()
     del dev
-    Qh = wjq.Query(CSV_QUERY)
-    Qh.run_csv(host.numpy()[:n])
-    t0 = time.perf_counter()
-    rr = Qh.run_csv(host.numpy()[:n])
-    el = time.perf_counter() - t0
-    if rr.rc:
-        raise RuntimeError(rr.err)
-    Qh.close()
+    el = None
+    if e2e:
+        Qh = wjq.Query(CSV_QUERY)
+        Qh.run_csv(host.numpy()[:n])
+        t0 = time.perf_counter()
+        rr = Qh.run_csv(host.numpy()[:n])
+        el = time.perf_counter() - t0
+        if rr.rc:
+            raise RuntimeError(rr.err)
+        Qh.close()
     return {"query": CSV_QUERY, "csv_bytes": n, "rows": rows, "ndjson_bytes": nd,
             "residency": "device (value) / pinned host (e2e)",
             "value": round(n / (best[0] / 1e3) / 1e9, 2), "unit": "GB/s of CSV",
             "convert_gbs": round(n / (best[1] / 1e3) / 1e9, 2),
             "scan_gbs_of_ndjson": round(nd / (best[2] / 1e3) / 1e9, 2),
             "ms": [round(x, 3) for x in best],
-            "e2e_gbs": round(n / el / 1e9, 3)}
+            "e2e_gbs": round(n / el / 1e9, 3) if el else None}
 
 
 def measure_file(wjq, hnp, n, n_bytes=2_000_000_000):
@@ -453,6 +455,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch and serving legs")
+    ap.add_argument("--csv-only", type=int, default=0, metavar="BYTES",
+                    help="only the device-resident CSV leg, on BYTES of CSV (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -467,6 +471,9 @@ def main():
     import numpy as np
     import torch
     import warpjq_b200 as wjq
+    if args.csv_only:
+        print(json.dumps({"csv": measure_csv(wjq, args.csv_only, reps=args.steps, e2e=False)}), flush=True)
+        return
 
     torch.cuda.set_device(local)
     dist = None

@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 KERNEL_SRCS = [os.path.join(CSRC, "backend.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "csv.cu")]
-KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "plan.h")]
+KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "plan.h", "csv_rows.cuh")]
 HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc")]
 CLI_SRCS = [os.path.join(CSRC, "host", "cli.cc")]
 HEADERS = [os.path.join(ROOT, "include", f) for f in ("warpjq_kernels.h", "warpjq_ext.h", "warpjq_host.h")]

@@ -44,10 +44,11 @@
 #include <vector>
 
 #include "../../include/warpjq_ext.h"
+#include "csv_rows.cuh"
+
+using namespace wjq_csv;
 
 namespace {
-
-typedef unsigned long long u64;
 
 constexpr uint32_t kRun = 256;                     // bytes a thread owns in the row passes
 constexpr int kCsvThreads = 256;                   // threads per tile
@@ -94,13 +95,6 @@ __device__ u64 block_excl(u64 v, u64 &total) {
   total = all;
   __syncthreads();
   return kXor ? (before ^ inc ^ v) : (before + inc - v);
-}
-
-// Bit k (k < 4) set when byte k of `w` equals the byte repeated in `pat`.
-__device__ __forceinline__ uint32_t eq4(uint32_t w, uint32_t pat) {
-  const uint32_t x = w ^ pat;
-  const uint32_t z = ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);  // 0x80 at equal bytes
-  return (((z >> 7) * 0x00204081u) >> 21) & 0xFu;  // gathers the four flags in byte order
 }
 
 // Quote and newline masks of the 16-byte aligned block at `blk`.
@@ -229,197 +223,6 @@ __global__ void k_csv_close(u64 *row_end, u64 n, int final_, u64 *info) {
   info[2] = r ? row_end[0] : 0;
 }
 
-// Reads bytes through 16-byte aligned loads (same page argument as above).
-struct Rd {
-  const uint8_t *d;
-  uintptr_t blk;
-  uint4 v;
-  __device__ __forceinline__ explicit Rd(const uint8_t *d_) : d(d_), blk(1) {}
-  __device__ __forceinline__ uint8_t operator()(u64 i) {
-    const uintptr_t p = (uintptr_t)(d + i), b = p & ~(uintptr_t)15;
-    if (b != blk) {
-      blk = b;
-      v = __ldg(reinterpret_cast<const uint4 *>(b));
-    }
-    const uint32_t o = (uint32_t)(p & 15);
-    const uint32_t w = o < 8 ? (o < 4 ? v.x : v.y) : (o < 12 ? v.z : v.w);
-    return (uint8_t)(w >> ((o & 3) * 8));
-  }
-};
-
-// Writes bytes from `p` on, as aligned 4-byte stores wherever a word lies
-// inside the line, byte stores at its edges (the neighbouring lines'
-// threads own those words' other bytes).
-struct Wr {
-  uint8_t *p, *row0;
-  uint32_t acc;
-  __device__ __forceinline__ explicit Wr(uint8_t *p_) : p(p_), row0(p_), acc(0) {}
-  __device__ __forceinline__ void put(uint8_t c) {
-    const uint32_t k = (uint32_t)((uintptr_t)p & 3);
-    acc |= (uint32_t)c << (8 * k);
-    if (k == 3) {
-      uint8_t *w = p - 3;
-      if (w >= row0) {
-        *reinterpret_cast<uint32_t *>(w) = acc;
-      } else {
-        for (uint32_t j = (uint32_t)(row0 - w); j < 4; j++) w[j] = (uint8_t)(acc >> (8 * j));
-      }
-      acc = 0;
-    }
-    p++;
-  }
-  __device__ __forceinline__ void flush() {
-    const uint32_t k = (uint32_t)((uintptr_t)p & 3);
-    if (!k) return;
-    uint8_t *w = p - k;
-    for (uint32_t j = w < row0 ? (uint32_t)(row0 - w) : 0; j < k; j++) w[j] = (uint8_t)(acc >> (8 * j));
-  }
-};
-
-// JSON string bytes of one raw byte.
-__device__ __forceinline__ uint32_t esc_len(uint8_t c) {
-  if (c >= 0x20) return (c == '"' || c == '\\') ? 2 : 1;
-  return (c == '\n' || c == '\r' || c == '\t' || c == 8 || c == 12) ? 2 : 6;
-}
-
-template <bool kWrite>
-__device__ __forceinline__ void put_esc(Wr &w, uint8_t c) {
-  if (!kWrite) return;
-  if (c >= 0x20 && c != '"' && c != '\\') {
-    w.put(c);
-    return;
-  }
-  w.put('\\');
-  switch (c) {
-    case '"': w.put('"'); return;
-    case '\\': w.put('\\'); return;
-    case '\n': w.put('n'); return;
-    case '\r': w.put('r'); return;
-    case '\t': w.put('t'); return;
-    case 8: w.put('b'); return;
-    case 12: w.put('f'); return;
-    default: {
-      const uint32_t h = c >> 4, l = c & 15;
-      w.put('u');
-      w.put('0');
-      w.put('0');
-      w.put((uint8_t)('0' + h));
-      w.put((uint8_t)(l < 10 ? '0' + l : 'a' + l - 10));
-    }
-  }
-}
-
-// True when [a, b) is a JSON number: -?(0|[1-9][0-9]*)(.[0-9]+)?([eE][+-]?[0-9]+)?
-__device__ bool is_number(Rd &rd, u64 a, u64 b) {
-  u64 i = a;
-  if (i < b && rd(i) == '-') i++;
-  if (i >= b) return false;
-  uint8_t c = rd(i);
-  if (c < '0' || c > '9') return false;
-  i++;
-  if (c != '0')
-    while (i < b && (c = rd(i)) >= '0' && c <= '9') i++;
-  if (i < b && rd(i) == '.') {
-    i++;
-    if (i >= b || (c = rd(i)) < '0' || c > '9') return false;
-    while (i < b && (c = rd(i)) >= '0' && c <= '9') i++;
-  }
-  if (i < b && ((c = rd(i)) == 'e' || c == 'E')) {
-    i++;
-    if (i < b && ((c = rd(i)) == '+' || c == '-')) i++;
-    if (i >= b || (c = rd(i)) < '0' || c > '9') return false;
-    while (i < b && (c = rd(i)) >= '0' && c <= '9') i++;
-  }
-  return i == b;
-}
-
-struct KeySet {
-  const uint8_t *text;  // key k: text[off[k], off[k+1]) = `"name":`, with a leading ',' for k > 0
-  const uint32_t *off;
-  uint32_t n;
-};
-
-// One row [s, e) to NDJSON: its length, and with kWrite its bytes.
-template <bool kWrite>
-__device__ u64 row_json(Rd &rd, u64 s, u64 e, const KeySet &ks, Wr &w) {
-  if (e > s && rd(e - 1) == '\r') e--;
-  if (e == s) {  // an empty row: an empty line
-    if (kWrite) w.put('\n');
-    return 1;
-  }
-  u64 len = 3;  // "{" "}\n"
-  if (kWrite) w.put('{');
-  u64 p = s;
-  bool more = true;
-  for (uint32_t k = 0; k < ks.n && more; k++) {
-    const uint32_t ka = ks.off[k], kb = ks.off[k + 1];
-    len += kb - ka;
-    if (kWrite)
-      for (uint32_t j = ka; j < kb; j++) w.put(ks.text[j]);
-    if (p < e && rd(p) == '"') {  // quoted
-      len += 2;
-      if (kWrite) w.put('"');
-      p++;
-      while (p < e) {
-        const uint8_t c = rd(p);
-        if (c == '"') {
-          if (p + 1 < e && rd(p + 1) == '"') {
-            len += 2;
-            put_esc<kWrite>(w, '"');
-            p += 2;
-            continue;
-          }
-          p++;  // the closing quote
-          break;
-        }
-        len += esc_len(c);
-        put_esc<kWrite>(w, c);
-        p++;
-      }
-      while (p < e) {  // bytes after the closing quote
-        const uint8_t c = rd(p);
-        if (c == ',') break;
-        len += esc_len(c);
-        put_esc<kWrite>(w, c);
-        p++;
-      }
-      if (kWrite) w.put('"');
-    } else {
-      const u64 a = p;
-      while (p < e && rd(p) != ',') p++;
-      if (a == p) {
-        len += 4;
-        if (kWrite) {
-          w.put('n');
-          w.put('u');
-          w.put('l');
-          w.put('l');
-        }
-      } else if (is_number(rd, a, p)) {
-        len += p - a;
-        if (kWrite)
-          for (u64 i = a; i < p; i++) w.put(rd(i));
-      } else {
-        len += 2;
-        if (kWrite) w.put('"');
-        for (u64 i = a; i < p; i++) {
-          const uint8_t c = rd(i);
-          len += esc_len(c);
-          put_esc<kWrite>(w, c);
-        }
-        if (kWrite) w.put('"');
-      }
-    }
-    more = p < e;  // a ',' follows
-    p++;
-  }
-  if (kWrite) {
-    w.put('}');
-    w.put('\n');
-  }
-  return len;
-}
-
 // Rows [row0, rows) of the chunk, one thread each: pass 0 writes the NDJSON
 // length of line r - row0 to len_off, pass 1 writes the line at out +
 // len_off[r - row0] (len_off by then an exclusive prefix).
@@ -427,14 +230,14 @@ template <bool kWrite>
 __global__ void __launch_bounds__(kJsonThreads) k_csv_json(const uint8_t *d, const u64 *row_end, u64 row0,
                                                            u64 rows, KeySet ks, u64 *len_off, uint8_t *out) {
   for (u64 r = row0 + blockIdx.x * (u64)blockDim.x + threadIdx.x; r < rows; r += (u64)gridDim.x * blockDim.x) {
-    const u64 s = r ? row_end[r - 1] + 1 : 0, e = row_end[r];
-    Rd rd(d);
+    const u64 s = r ? __ldg(row_end + r - 1) + 1 : 0, e = __ldg(row_end + r);
+    WordIn in(d);
     if (!kWrite) {
-      Wr w(nullptr);
-      len_off[r - row0] = row_json<false>(rd, s, e, ks, w);
+      WordOut w(nullptr);
+      len_off[r - row0] = row_json<false>(in, s, e, ks, w);
     } else {
-      Wr w(out + len_off[r - row0]);
-      row_json<true>(rd, s, e, ks, w);
+      WordOut w(out + len_off[r - row0]);
+      row_json<true>(in, s, e, ks, w);
       w.flush();
     }
   }
@@ -515,83 +318,16 @@ struct DBuf {  // device buffer that only grows
   }
 };
 
-void escape_into(std::string &o, const uint8_t *s, size_t n) {
-  static const char *hx = "0123456789abcdef";
-  for (size_t i = 0; i < n; i++) {
-    const uint8_t c = s[i];
-    switch (c) {
-      case '"': o += "\\\""; break;
-      case '\\': o += "\\\\"; break;
-      case '\n': o += "\\n"; break;
-      case '\r': o += "\\r"; break;
-      case '\t': o += "\\t"; break;
-      case 8: o += "\\b"; break;
-      case 12: o += "\\f"; break;
-      default:
-        if (c < 0x20) {
-          o += "\\u00";
-          o += hx[c >> 4];
-          o += hx[c & 15];
-        } else {
-          o += (char)c;
-        }
-    }
-  }
-}
-
-// Header names from the raw header row, by the field rules above, as the
-// key texts `"name":` (with a leading ',' after the first).
-void parse_header(const uint8_t *h, size_t n, std::string &text, std::vector<uint32_t> &offs) {
-  text.clear();
-  offs.assign(1, 0);
-  if (n >= 3 && h[0] == 0xEF && h[1] == 0xBB && h[2] == 0xBF) {
-    h += 3;
-    n -= 3;
-  }
-  if (n && h[n - 1] == '\r') n--;
-  if (!n) return;
-  size_t p = 0;
-  bool more = true;
-  while (more) {
-    std::string name;
-    if (p < n && h[p] == '"') {
-      p++;
-      while (p < n) {
-        if (h[p] == '"') {
-          if (p + 1 < n && h[p + 1] == '"') {
-            name += '"';
-            p += 2;
-            continue;
-          }
-          p++;
-          break;
-        }
-        name += (char)h[p++];
-      }
-      while (p < n && h[p] != ',') name += (char)h[p++];
-    } else {
-      while (p < n && h[p] != ',') name += (char)h[p++];
-    }
-    more = p < n;
-    p++;
-    if (offs.size() > 1) text += ',';
-    text += '"';
-    escape_into(text, (const uint8_t *)name.data(), name.size());
-    text += "\":";
-    offs.push_back((uint32_t)text.size());
-  }
-}
-
 }  // namespace
 
 struct warpjq_csv {
   DBuf<uint8_t> in;  // device copy of host input
-  DBuf<uint32_t> run_stat, tile_state, key_off, g_len;
+  DBuf<uint32_t> run_stat, tile_state, keys, key_off, g_len;  // keys: key texts by words; key_off: their meta
   DBuf<u64> tile_stat, tile_row, row_end, lens, bt, info, g_off, g_dst;
-  DBuf<uint8_t> keys, out, g_out;
+  DBuf<uint8_t> out, g_out;
   bool have_header = false;  // header names taken from an earlier chunk
   std::string key_text;
-  std::vector<uint32_t> key_offs;
+  std::vector<uint32_t> key_offs, key_words, key_meta;
   ~warpjq_csv() {
     in.release();
     run_stat.release();
@@ -627,6 +363,8 @@ void warpjq_csv_reset(warpjq_csv *c) {
   c->have_header = false;
   c->key_text.clear();
   c->key_offs.clear();
+  c->key_words.clear();
+  c->key_meta.clear();
 }
 
 warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, uint32_t flags, void *stream,
@@ -681,13 +419,15 @@ warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, 
       else CSV_CK(cudaMemcpy(head.data(), d, h_end, cudaMemcpyDeviceToHost), "copy of the CSV header");
     }
     parse_header(head.data(), head.size(), c->key_text, c->key_offs);
-    CSV_CK(c->keys.ensure(c->key_text.size() + 1), "device memory for CSV keys");
-    CSV_CK(c->key_off.ensure(c->key_offs.size()), "device memory for CSV keys");
-    if (!c->key_text.empty())
-      CSV_CK(cudaMemcpyAsync(c->keys.p, c->key_text.data(), c->key_text.size(), cudaMemcpyHostToDevice, st),
+    pack_keys(c->key_text, c->key_offs, c->key_words, c->key_meta);
+    CSV_CK(c->keys.ensure(c->key_words.size() + 1), "device memory for CSV keys");
+    CSV_CK(c->key_off.ensure(c->key_meta.size() + 1), "device memory for CSV keys");
+    if (!c->key_words.empty())
+      CSV_CK(cudaMemcpyAsync(c->keys.p, c->key_words.data(), c->key_words.size() * 4, cudaMemcpyHostToDevice, st),
              "copy of the CSV keys");
-    CSV_CK(cudaMemcpyAsync(c->key_off.p, c->key_offs.data(), c->key_offs.size() * 4, cudaMemcpyHostToDevice, st),
-           "copy of the CSV keys");
+    if (!c->key_meta.empty())
+      CSV_CK(cudaMemcpyAsync(c->key_off.p, c->key_meta.data(), c->key_meta.size() * 4, cudaMemcpyHostToDevice, st),
+             "copy of the CSV keys");
     c->have_header = true;
     row0 = 1;
   }
@@ -695,7 +435,7 @@ warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, 
   const u64 m = rows - row0;
   if (records) *records = m;
   if (m == 0) return WARPJQ_OK;
-  KeySet ks{c->keys.p, c->key_off.p, (uint32_t)c->key_offs.size() - 1};
+  KeySet ks{c->keys.p, c->key_off.p, (uint32_t)(c->key_meta.size() / 2)};
   CSV_CK(c->lens.ensure(m + 1), "device memory for CSV lines");
   const unsigned grid = (unsigned)std::min<u64>((m + kJsonThreads - 1) / kJsonThreads, 148ull * 64);
   k_csv_json<false><<<grid, kJsonThreads, 0, st>>>(d, c->row_end.p, row0, rows, ks, c->lens.p, nullptr);
