@@ -184,8 +184,9 @@ def batch_workload(hnp, n, n_inputs=4096, lo=4096, hi=4 << 20, seed=7):
 
 def measure_batch(wjq, dev, offs, lens, qidx):
     """Aggregate GB/s over all inputs: plain (one run and host round trip
-    per input) and batched (one batched run per query, collected at the
-    end); wall clock, results on the host in both."""
+    per input), batched (one batched run per query, collected at the end)
+    and graph (the same batches replayed from one CUDA graph); wall clock,
+    results on the host in all three."""
     import torch
     stream = torch.cuda.current_stream().cuda_stream
     ptr = dev.data_ptr()
@@ -206,22 +207,36 @@ def measure_batch(wjq, dev, offs, lens, qidx):
         for k in range(len(groups)):
             batch_q[k].batch_collect()
 
+    graph_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
+    graph = wjq.BatchGraph([(graph_q[k], ptr, [offs[i] for i in g], [lens[i] for i in g])
+                            for k, g in enumerate(groups)])
+
+    def replay():
+        graph.launch(stream)
+        for k in range(len(groups)):
+            graph_q[k].batch_collect()
+
     out = {}
-    for name, fn in (("plain", plain), ("batched", batched)):
+    for name, fn in (("plain", plain), ("batched", batched), ("graph", replay)):
         fn()  # warm: buffers reach their sizes
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         fn()
         torch.cuda.synchronize()
         out[name] = time.perf_counter() - t0
+    graph.close()
     return {"inputs": len(offs), "bytes": total,
             "sizes": "log-uniform 4 KiB - 4 MiB (rescaled from 4 KB - 64 MB, whose ~28 GB does not "
                      "fit the bench's time budget)",
             "queries": len(BATCH_QUERIES), "residency": "device",
             "plain_gbs": round(total / out["plain"] / 1e9, 3),
             "batched_gbs": round(total / out["batched"] / 1e9, 3),
+            "graph_gbs": round(total / out["graph"] / 1e9, 3),
             "plain_s": round(out["plain"], 4), "batched_s": round(out["batched"], 4),
-            "speedup": round(out["plain"] / out["batched"], 2)}
+            "graph_s": round(out["graph"], 4),
+            "graph": "one CUDA graph: the 8 queries' batches captured on forked streams, one launch",
+            "speedup": round(out["plain"] / out["batched"], 2),
+            "graph_speedup": round(out["plain"] / out["graph"], 2)}
 
 
 def measure_serving(wjq, dev, offs, lens, qidx, rate=2000.0, n_req=4096, seed=11):

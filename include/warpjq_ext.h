@@ -169,6 +169,31 @@ warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const 
 warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
                                    warpjq_device_result *all, char *err, size_t err_len);
 
+/* A CUDA graph of batched runs: the launch sequences of one batch per
+ * context (each context its own query, each batch its own inputs), captured
+ * once on forked streams into one graph and replayed with one launch.  No
+ * reference counterpart.
+ *
+ * warpjq_batch_graph_create first runs every batch once, plainly (this
+ * sizes every device buffer for the layout and leaves the batch tables on
+ * the device), then captures.  A replay re-reads the same device addresses:
+ * change the inputs' bytes in place between replays, not their offsets or
+ * lengths.  After warpjq_batch_graph_launch, collect each batch with
+ * warpjq_batch_collect on its context, in any order.  A replay is refused
+ * (WARPJQ_ERR_INVALID_ARG) once one of its contexts has run a plain batch
+ * or grown a buffer (a collect that found an overflow reruns the batch
+ * plainly with larger buffers, so its result stays complete): create the
+ * graph again then.  The contexts must outlive the graph. */
+typedef struct warpjq_batch_graph warpjq_batch_graph;
+
+warpjq_status warpjq_batch_graph_create(warpjq_ctx *const *ctxs, uint32_t n_ctx,
+                                        const uint8_t *const *d_data, const uint64_t *const *offsets,
+                                        const uint64_t *const *lengths, const uint32_t *n_inputs,
+                                        warpjq_batch_graph **out, char *err, size_t err_len);
+warpjq_status warpjq_batch_graph_launch(warpjq_batch_graph *g, void *stream, char *err,
+                                        size_t err_len);
+void warpjq_batch_graph_destroy(warpjq_batch_graph *g);
+
 /* Device-resident scan tunables: bytes per tile (one warp walks the lines
  * starting in a tile, one line per lane) and the halo staged after it (a line
  * that runs past tile + halo is walked from global memory, more slowly).

@@ -37,7 +37,8 @@ EXT_SYMBOLS = [
     "warpjq_set_tiling", "warpjq_autotile", "warpjq_submit_host", "warpjq_host_is_pinned",
     "warpjq_batch_launch", "warpjq_batch_collect", "warpjq_host_alloc_pinned",
     "warpjq_host_free_pinned", "warpjq_csv_create", "warpjq_csv_destroy", "warpjq_csv_reset",
-    "warpjq_csv_convert", "warpjq_csv_gather", "warpjq_device_read",
+    "warpjq_csv_convert", "warpjq_csv_gather", "warpjq_device_read", "warpjq_batch_graph_create",
+    "warpjq_batch_graph_launch", "warpjq_batch_graph_destroy",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
@@ -103,6 +104,12 @@ def _load():
     h.warpjq_query_run_file.argtypes = [vp, cp, u32, u64, ctypes.POINTER(vp), ctypes.POINTER(sz),
                                         ctypes.POINTER(u64), cp, sz]
     h.warpjq_query_run_file.restype = ctypes.c_int
+    k.warpjq_batch_graph_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                            ctypes.POINTER(vp), ctypes.POINTER(u32), ctypes.POINTER(vp), cp, sz]
+    k.warpjq_batch_graph_create.restype = ctypes.c_int
+    k.warpjq_batch_graph_launch.argtypes = [vp, vp, cp, sz]
+    k.warpjq_batch_graph_launch.restype = ctypes.c_int
+    k.warpjq_batch_graph_destroy.argtypes = [vp]
     k.warpjq_csv_create.argtypes = [ctypes.POINTER(vp)]
     k.warpjq_csv_create.restype = ctypes.c_int
     k.warpjq_csv_destroy.argtypes = [vp]
@@ -446,6 +453,55 @@ class Query:
         self._h.warpjq_query_render_device(self._q, ctypes.byref(r), addr, ctypes.byref(out),
                                            ctypes.byref(n))
         return _take(out, n)
+
+
+class BatchGraph:
+    """One CUDA graph replaying a batch per query (warpjq_ext.h
+    warpjq_batch_graph_*): batches[i] = (query, device base address,
+    offsets, lengths).  Each Query must be used by one batch only; after
+    launch(), collect each with query.batch_collect()."""
+
+    def __init__(self, batches):
+        k, _ = _load()
+        self._k = k
+        n = len(batches)
+        self._queries = [b[0] for b in batches]
+        self._keep = []
+        ctxs = (ctypes.c_void_p * n)(*[q.ctx for q, _, _, _ in batches])
+        datas = (ctypes.c_void_p * n)(*[d for _, d, _, _ in batches])
+        offs = (ctypes.c_void_p * n)()
+        lens = (ctypes.c_void_p * n)()
+        counts = (ctypes.c_uint32 * n)()
+        for i, (q, _, o, l) in enumerate(batches):
+            oa = (ctypes.c_uint64 * max(1, len(o)))(*o)
+            la = (ctypes.c_uint64 * max(1, len(l)))(*l)
+            self._keep += [oa, la]
+            offs[i] = ctypes.cast(oa, ctypes.c_void_p)
+            lens[i] = ctypes.cast(la, ctypes.c_void_p)
+            counts[i] = len(o)
+            q._b_n = len(o)
+        self._g = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(1024)
+        rc = k.warpjq_batch_graph_create(ctxs, n, datas, offs, lens, counts, ctypes.byref(self._g), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+
+    def launch(self, stream: int = 0):
+        err = ctypes.create_string_buffer(1024)
+        rc = self._k.warpjq_batch_graph_launch(self._g, ctypes.c_void_p(stream), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+
+    def close(self):
+        if self._g:
+            self._k.warpjq_batch_graph_destroy(self._g)
+            self._g = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class CsvConverter:

@@ -158,6 +158,7 @@ struct Slot {
   bool launched = false;
   uint32_t kernels = 0;
   cudaEvent_t scan_t0 = nullptr, scan_t1 = nullptr;  // around the scan kernel
+  bool timed = false;  // the last run recorded scan_t0/scan_t1 (not a graph replay)
   unsigned long long last_first_invalid = ~0ull;
   unsigned long long last_first_type = ~0ull;
 };
@@ -182,6 +183,8 @@ struct warpjq_ctx {
   // batched runs (warpjq_batch_launch): host copies of the tables
   struct Batch {
     bool active = false;
+    bool tables_on_device = false;  // enqueue without uploading the tables (graph capture)
+    uint64_t epoch = 0;             // bumped whenever a plain batch replaces the device tables
     const uint8_t *d_data = nullptr;
     cudaStream_t stream = nullptr;
     unsigned long long n_tiles = 0, total = 0;
@@ -287,7 +290,10 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
   const DevPlan &P = c->plan;
   bool groups = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
   const uint32_t n_inputs = b ? (uint32_t)b->start.size() : 0;
-  if (b) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(st, &cap), "capture status");
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  if (b && !b->tables_on_device) {
     CK(rb.b_in_start.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
     CK(rb.b_in_end.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
     CK(rb.b_in_tile0.ensure(n_inputs + 1), "alloc batch tables");
@@ -305,8 +311,8 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       CK(cudaMemcpyAsync(rb.b_tile_input.p, b->tile_input.data(), n_tiles * 4ull,
                          cudaMemcpyHostToDevice, st),
          "H2D batch tables");
-    if (n_inputs) k_batch_reset<<<(n_inputs + 255) / 256, 256, 0, st>>>(rb.b_in_ctr.p, n_inputs);
   }
+  if (b && n_inputs) k_batch_reset<<<(n_inputs + 255) / 256, 256, 0, st>>>(rb.b_in_ctr.p, n_inputs);
   GroupTable g = group_view(rb, groups);
   s.kernels = 0;
   k_reset_run<<<256, 256, 0, st>>>(rb.ctr.p, g, groups ? rb.g_cap : 0, groups ? rb.g_key_cap : 0);
@@ -336,18 +342,19 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       sp.in_ctr = rb.b_in_ctr.p;
     }
     unsigned grid = (unsigned)std::min<unsigned long long>(c->grid, n_tiles);
-    if (!s.scan_t0) {
+    if (!s.scan_t0 && !capturing) {
       CK(cudaEventCreate(&s.scan_t0), "event");
       CK(cudaEventCreate(&s.scan_t1), "event");
     }
-    CK(cudaEventRecord(s.scan_t0, st), "event record");
+    s.timed = !capturing;  // a captured sequence is not timed
+    if (s.timed) CK(cudaEventRecord(s.scan_t0, st), "event record");
     if (P.needs_rows)
       k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     else
       k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     s.kernels++;
     CK(cudaGetLastError(), "launch scan");
-    CK(cudaEventRecord(s.scan_t1, st), "event record");
+    if (s.timed) CK(cudaEventRecord(s.scan_t1, st), "event record");
     if (P.needs_rows) {
       const uint32_t tpb = rows_tiles_per_block(n_tiles);
       const unsigned nb = (unsigned)((n_tiles + tpb - 1) / tpb);
@@ -458,6 +465,35 @@ warpjq_status run_to_completion(warpjq_ctx *c, Slot &s, const uint8_t *d_data,
   }
   set_err(err, err_len, "device buffers kept overflowing");
   return WARPJQ_ERR_OOM;
+}
+
+// Everything a captured batch bakes in from its context: buffer addresses
+// and sizes, capacities, tiling and grid.  A graph replays only while this
+// is unchanged (a grown or released buffer would leave it writing to freed
+// memory).
+uint64_t bufs_signature(const warpjq_ctx *c) {
+  const RunBufs &rb = c->dev.rb;
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto mix = [&](uint64_t v) {
+    h ^= v;
+    h *= 0x100000001b3ull;
+  };
+  mix((uintptr_t)rb.ctr.p); mix(rb.ctr.n);
+  mix((uintptr_t)rb.tiles.p); mix(rb.tiles.n);
+  mix((uintptr_t)rb.row_tiles.p); mix(rb.row_tiles.n);
+  mix((uintptr_t)rb.row_bsum.p); mix(rb.row_bsum.n);
+  mix((uintptr_t)rb.b_tile_input.p); mix(rb.b_tile_input.n);
+  mix((uintptr_t)rb.b_in_start.p); mix((uintptr_t)rb.b_in_end.p);
+  mix((uintptr_t)rb.b_in_tile0.p); mix((uintptr_t)rb.b_in_ctr.p);
+  mix((uintptr_t)rb.recs.p); mix(rb.recs.n);
+  mix((uintptr_t)rb.out.p); mix(rb.out.n);
+  mix((uintptr_t)rb.row_off.p); mix((uintptr_t)rb.line_idx.p);
+  mix((uintptr_t)rb.tile_fsum.p); mix((uintptr_t)rb.block_f.p); mix((uintptr_t)rb.block_lines.p);
+  mix((uintptr_t)rb.deep.p); mix(rb.deep.n);
+  mix((uintptr_t)rb.g_slots.p); mix((uintptr_t)rb.g_keys.p); mix((uintptr_t)rb.g_acc.p);
+  mix(rb.rec_cap_per_cta); mix(rb.out_cap); mix(rb.rows_cap); mix(rb.g_cap); mix(rb.g_key_cap);
+  mix(rb.deep_levels); mix(c->tile_bytes); mix(c->halo_bytes); mix(c->grid); mix(c->scan_smem);
+  return h;
 }
 
 double i128_to_double(unsigned long long lo, unsigned long long hi) {
@@ -911,7 +947,7 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
   }
   out->kernels_launched = s.kernels;
   out->scan_ms = 0.0;
-  if (s.scan_t0 && ctx->dev_n) {
+  if (s.scan_t0 && s.timed && ctx->dev_n) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, s.scan_t0, s.scan_t1) == cudaSuccess) out->scan_ms = ms;
   }
@@ -924,6 +960,7 @@ warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const 
   if (!ctx || (n_inputs && (!d_data || !offsets || !lengths))) return WARPJQ_ERR_INVALID_ARG;
   warpjq_ctx::Batch &b = ctx->batch;
   b.active = false;
+  b.epoch++;
   b.d_data = d_data;
   b.stream = (cudaStream_t)stream;
   b.start.resize(n_inputs);
@@ -1031,10 +1068,142 @@ warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
     all->groups = b.groups.data();
     all->n_groups = (uint32_t)b.groups.size();
     all->kernels_launched = s.kernels;
-    if (s.scan_t0 && b.total) {
+    if (s.scan_t0 && s.timed && b.total) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, s.scan_t0, s.scan_t1) == cudaSuccess) all->scan_ms = ms;
     }
+  }
+  return WARPJQ_OK;
+}
+
+struct warpjq_batch_graph {
+  std::vector<warpjq_ctx *> ctxs;
+  std::vector<uint64_t> epochs, sigs;
+  std::vector<uint32_t> kernels;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+void warpjq_batch_graph_destroy(warpjq_batch_graph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+}
+
+warpjq_status warpjq_batch_graph_create(warpjq_ctx *const *ctxs, uint32_t n_ctx, const uint8_t *const *d_data,
+                                        const uint64_t *const *offsets, const uint64_t *const *lengths,
+                                        const uint32_t *n_inputs, warpjq_batch_graph **out, char *err,
+                                        size_t err_len) {
+  if (!out || !ctxs || !n_ctx || !d_data || !offsets || !lengths || !n_inputs) return WARPJQ_ERR_INVALID_ARG;
+  *out = nullptr;
+  for (uint32_t i = 0; i < n_ctx; i++)
+    for (uint32_t j = 0; j < i; j++)
+      if (!ctxs[i] || ctxs[i] == ctxs[j]) {
+        set_err(err, err_len, "each batch of a graph needs its own context");
+        return WARPJQ_ERR_INVALID_ARG;
+      }
+  // 1. A plain run of every batch: sizes every buffer for this layout (and
+  //    its contents) and leaves the batch tables on the device.
+  for (uint32_t i = 0; i < n_ctx; i++) {
+    warpjq_status rc = warpjq_batch_launch(ctxs[i], d_data[i], offsets[i], lengths[i], n_inputs[i], nullptr,
+                                           err, err_len);
+    if (rc != WARPJQ_OK) return rc;
+    std::vector<warpjq_batch_item> items(std::max<uint32_t>(n_inputs[i], 1));
+    rc = warpjq_batch_collect(ctxs[i], items.data(), nullptr, err, err_len);
+    if (rc != WARPJQ_OK) return rc;
+  }
+  // 2. Capture every batch's launch sequence on its own stream, forked from
+  //    and joined back to one capture stream.
+  auto *g = new warpjq_batch_graph();
+  cudaStream_t s0 = nullptr;
+  std::vector<cudaStream_t> ss(n_ctx, nullptr);
+  std::vector<cudaEvent_t> joins(n_ctx, nullptr);
+  cudaEvent_t fork = nullptr;
+  warpjq_status rc = WARPJQ_OK;
+  auto fail = [&](cudaError_t e, const char *what) {
+    set_err(err, err_len, "%s: %s", what, cudaGetErrorString(e));
+    rc = WARPJQ_ERR_CUDA;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking);
+  if (e != cudaSuccess) fail(e, "capture stream");
+  if (rc == WARPJQ_OK && (e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess)
+    fail(e, "capture event");
+  for (uint32_t i = 0; rc == WARPJQ_OK && i < n_ctx; i++) {
+    if ((e = cudaStreamCreateWithFlags(&ss[i], cudaStreamNonBlocking)) != cudaSuccess) fail(e, "capture stream");
+    else if ((e = cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming)) != cudaSuccess) fail(e, "capture event");
+  }
+  bool began = false;
+  if (rc == WARPJQ_OK) {
+    if ((e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) fail(e, "begin capture");
+    else began = true;
+  }
+  if (rc == WARPJQ_OK && (e = cudaEventRecord(fork, s0)) != cudaSuccess) fail(e, "capture fork");
+  for (uint32_t i = 0; rc == WARPJQ_OK && i < n_ctx; i++) {
+    warpjq_ctx *c = ctxs[i];
+    if ((e = cudaStreamWaitEvent(ss[i], fork, 0)) != cudaSuccess) {
+      fail(e, "capture fork");
+      break;
+    }
+    c->batch.tables_on_device = true;
+    rc = enqueue_run(c, c->dev, c->batch.d_data, c->batch.total, ss[i], err, err_len, &c->batch);
+    c->batch.tables_on_device = false;
+    g->kernels.push_back(c->dev.kernels);
+    if (rc != WARPJQ_OK) break;
+    if ((e = cudaEventRecord(joins[i], ss[i])) != cudaSuccess) fail(e, "capture join");
+    else if ((e = cudaStreamWaitEvent(s0, joins[i], 0)) != cudaSuccess) fail(e, "capture join");
+  }
+  if (began) {
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(s0, &graph);
+    if (rc == WARPJQ_OK && e != cudaSuccess) fail(e, "end capture");
+    if (rc == WARPJQ_OK) {
+      g->graph = graph;
+      if ((e = cudaGraphInstantiate(&g->exec, graph, 0)) != cudaSuccess) fail(e, "graph instantiate");
+    } else if (graph) {
+      cudaGraphDestroy(graph);
+    }
+  }
+  for (uint32_t i = 0; i < n_ctx; i++) {
+    if (ss[i]) cudaStreamDestroy(ss[i]);
+    if (joins[i]) cudaEventDestroy(joins[i]);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (s0) cudaStreamDestroy(s0);
+  if (rc != WARPJQ_OK) {
+    cudaGetLastError();
+    warpjq_batch_graph_destroy(g);
+    return rc;
+  }
+  for (uint32_t i = 0; i < n_ctx; i++) {
+    g->ctxs.push_back(ctxs[i]);
+    g->epochs.push_back(ctxs[i]->batch.epoch);
+    g->sigs.push_back(bufs_signature(ctxs[i]));
+  }
+  *out = g;
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_batch_graph_launch(warpjq_batch_graph *g, void *stream, char *err, size_t err_len) {
+  if (!g || !g->exec) return WARPJQ_ERR_INVALID_ARG;
+  for (size_t i = 0; i < g->ctxs.size(); i++) {
+    warpjq_ctx *c = g->ctxs[i];
+    if (c->batch.epoch != g->epochs[i] || bufs_signature(c) != g->sigs[i]) {
+      set_err(err, err_len,
+              "batch %zu's context ran another batch or grew its buffers since the capture; create the graph again",
+              i);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaGraphLaunch(g->exec, st), "graph launch");
+  for (size_t i = 0; i < g->ctxs.size(); i++) {
+    warpjq_ctx *c = g->ctxs[i];
+    c->batch.active = true;
+    c->batch.stream = st;
+    c->dev.launched = true;
+    c->dev.timed = false;
+    c->dev.kernels = g->kernels[i];
   }
   return WARPJQ_OK;
 }
