@@ -239,62 +239,91 @@ def measure_batch(wjq, dev, offs, lens, qidx):
             "graph_speedup": round(out["plain"] / out["graph"], 2)}
 
 
-def measure_serving(wjq, dev, offs, lens, qidx, rate=2000.0, n_req=4096, seed=11):
-    """Open-loop Poisson arrivals at `rate` req/s over the batch inputs.
-    "batched": at each step the server takes every request that has arrived
-    and runs one batch per query among them; "one-at-a-time": one run per
-    request.  Latency = completion - arrival (wall clock)."""
+SERVE_QUERIES = BATCH_QUERIES + [
+    "count", "min(.bytes)", "group_by(.method) | avg(.latency_ms)", "group_by(.status) | count",
+    'select(.method == "POST") | {t: .ts, l: .latency_ms}', "select(.bytes > 5000000) | count",
+    "select(.latency_ms > 100) | .path", "max(.bytes)",
+]
+
+
+def serve_csv_inputs(wjq, n_inputs=512, lo=4096, hi=4 << 20, seed=13):
+    """Device-resident CSV requests: a header row and a run of rows of the
+    nginx records as CSV, log-uniform sizes; a list of device tensors."""
+    import math
     import random
     import torch
     rng = random.Random(seed)
-    stream = torch.cuda.current_stream().cuda_stream
-    ptr = dev.data_ptr()
-    reqs = [rng.randrange(len(offs)) for _ in range(n_req)]
-    gaps = [rng.expovariate(rate) for _ in range(n_req)]
-    qs = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
-    for q in qs:  # warm
-        q.batch_launch(ptr, offs[:64], lens[:64], stream)
-        q.batch_collect()
+    buf, used, _ = wjq.gen_nginx_csv(256 << 20, seed=seed)
+    raw = bytes(buf[:used])
+    head_end = raw.index(b"\n") + 1
+    head = raw[:head_end]
+    parts, pos = [], head_end
+    for _ in range(n_inputs):
+        sz = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+        if pos + sz >= used:
+            pos = head_end
+        end = raw.index(b"\n", pos + sz - 1) + 1 if raw.find(b"\n", pos + sz - 1) >= 0 else used
+        parts.append(head + raw[pos:end])
+        pos = end
+    return [torch.frombuffer(bytearray(p), dtype=torch.uint8).cuda() for p in parts]
 
-    def run(mode):
+
+def measure_serving(wjq, dev, offs, lens, csv_inputs, rate=2000.0, n_req=4096, seed=11):
+    """Open-loop Poisson arrivals at `rate` req/s, 16 queries, 20% of the
+    requests CSV, all inputs device-resident.  "batched": the continuous-
+    batching server (warpjq_b200/serve.py: 3 slots, every arrived request
+    that fits the 120 GB budget joins the next free slot, slots overlap on
+    the device); "one_at_a_time": the same server with one slot taking one
+    request at a time.  Latency = completion - arrival (wall clock)."""
+    import random
+    import torch
+    from warpjq_b200.serve import Server
+    rng = random.Random(seed)
+    reqs = []
+    for _ in range(n_req):
+        q = SERVE_QUERIES[rng.randrange(len(SERVE_QUERIES))]
+        if rng.random() < 0.2:
+            t = csv_inputs[rng.randrange(len(csv_inputs))]
+            reqs.append((q, t, "csv"))
+        else:
+            i = rng.randrange(len(offs))
+            reqs.append((q, dev[offs[i]:offs[i] + lens[i]], "ndjson"))
+    gaps = [rng.expovariate(rate) for _ in range(n_req)]
+    total = sum(int(t.numel()) for _, t, _ in reqs)
+
+    def run(slots, max_batch):
+        srv = Server(SERVE_QUERIES, n_slots=slots, budget_bytes=120 << 30, max_batch=max_batch)
+        for q, t, f in reqs[:64]:  # warm: contexts and arenas reach their sizes
+            srv.submit(q, t, f)
+        srv.drain()
+        srv.done.clear()
+        torch.cuda.synchronize()
         t0 = time.perf_counter() + 0.01
         arrive, t = [], t0
         for g in gaps:
             t += g
             arrive.append(t)
-        lat = [0.0] * n_req
-        nxt = 0
-        while nxt < n_req:
+        nxt, hs = 0, []
+        while nxt < n_req or srv.pending():
             now = time.perf_counter()
-            if arrive[nxt] > now:
-                continue  # open loop: wait for the next arrival
-            k = nxt
-            while k < n_req and arrive[k] <= now:
-                k += 1
-            if mode == "one":
-                k = nxt + 1
-            todo = list(range(nxt, k))
-            by_q = {}
-            for r in todo:
-                by_q.setdefault(qidx[reqs[r]], []).append(reqs[r])
-            for qi, ins in by_q.items():
-                qs[qi].batch_launch(ptr, [offs[i] for i in ins], [lens[i] for i in ins], stream)
-            for qi in by_q:
-                qs[qi].batch_collect()
-            done = time.perf_counter()
-            for r in todo:
-                lat[r] = done - arrive[r]
-            nxt = k
+            while nxt < n_req and arrive[nxt] <= now:
+                q, x, f = reqs[nxt]
+                hs.append(srv.submit(q, x, f, t_arrive=arrive[nxt]))
+                nxt += 1
+            srv.poll()
         span = time.perf_counter() - t0
-        lat.sort()
+        srv.close()
+        assert all(not h.error for h in hs)
+        lat = sorted(h.latency for h in hs)
         pick = lambda f: round(lat[min(n_req - 1, int(f * n_req))] * 1e3, 3)
         return {"p50_ms": pick(0.50), "p99_ms": pick(0.99), "p999_ms": pick(0.999),
-                "sustained_gbs": round(sum(lens[i] for i in reqs) / span / 1e9, 3)}
+                "sustained_gbs": round(total / span / 1e9, 3)}
 
-    return {"offered_req_per_s": rate, "requests": n_req, "residency": "device",
-            "sizes": "the batch inputs (log-uniform 4 KiB - 4 MiB, rescaled from 1 KB - 256 MB)",
-            "offered_gbs": round(sum(lens[i] for i in reqs) / sum(gaps) / 1e9, 3),
-            "batched": run("batched"), "one_at_a_time": run("one")}
+    return {"offered_req_per_s": rate, "requests": n_req, "queries": len(SERVE_QUERIES), "csv_share": 0.2,
+            "residency": "device",
+            "sizes": "log-uniform 4 KiB - 4 MiB (rescaled from 1 KB - 256 MB)",
+            "offered_gbs": round(total / sum(gaps) / 1e9, 3),
+            "batched": run(3, 0), "one_at_a_time": run(1, 1)}
 
 
 NESTED_QUERIES = [
@@ -610,7 +639,9 @@ def main():
         # the configuration's top rate, and ten times it (the rescaled inputs
         # are ~35x smaller than the configuration's, so its offered bytes
         # per second need the higher rate)
-        serve = [measure_serving(wjq, bdev, boffs, blens, bq, rate=r) for r in (2000.0, 20000.0)]
+        csv_in = serve_csv_inputs(wjq)
+        serve = [measure_serving(wjq, bdev, boffs, blens, csv_in, rate=r) for r in (2000.0, 20000.0)]
+        del csv_in
         del bdev
         nested = measure_nested(wjq)
         csv_leg = measure_csv(wjq)

@@ -148,7 +148,9 @@ typedef struct {
 
 /* Batched device-resident run: the context's query over n_inputs separate
  * inputs that are already in device memory, input i being
- * d_data[offsets[i], offsets[i] + lengths[i]) (each start 16-byte aligned),
+ * d_data[offsets[i], offsets[i] + lengths[i]) (each start 16-byte aligned;
+ * with d_data NULL the offsets are device addresses, so the inputs may lie
+ * in different allocations, and group key_off values are addresses too),
  * in one launch sequence on `stream` with no host synchronisation.  Every
  * input gets exactly the result a run over it alone would give; lines never
  * continue from one input into the next.  Use it when many small inputs
@@ -299,7 +301,8 @@ warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, 
                                  uint64_t *consumed, uint64_t *records, char *err, size_t err_len);
 
 /* Copies the device byte slices d_src[offsets[i], + lengths[i]), i < n, to
- * host memory h_dst back to back (e.g. the group keys of a run over
+ * host memory h_dst back to back (d_src may be NULL: offsets are then
+ * device addresses) (e.g. the group keys of a run over
  * converted CSV, whose NDJSON lives only on the device).  Synchronous. */
 warpjq_status warpjq_csv_gather(warpjq_csv *c, const uint8_t *d_src, const uint64_t *offsets,
                                 const uint32_t *lengths, uint64_t n, uint8_t *h_dst, void *stream,

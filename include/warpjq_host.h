@@ -73,6 +73,17 @@ int warpjq_run_bytes(const char *query, const uint8_t *data, size_t len, uint32_
 int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r,
                                const uint8_t *data, char **out, size_t *out_len);
 
+/* Every input's output of a collected batch (warpjq_batch_collect), back to
+ * back in one buffer (free with warpjq_host_free): input i's bytes are
+ * (*out)[offsets[i], offsets[i + 1]) -- what a run over it alone prints.
+ * `groups` is the batch's group array (warpjq_device_result.groups) and
+ * `key_data` the host bytes its key_off values index; `rows` and `row_off`
+ * a host copy of the batch's rows and row offsets (null for aggregates).
+ * offsets has n + 1 entries.  No reference counterpart. */
+int warpjq_query_render_batch(warpjq_query *q, const warpjq_batch_item *items, uint32_t n,
+                              const warpjq_group_ext *groups, const uint8_t *key_data, const uint8_t *rows,
+                              const uint64_t *row_off, char **out, size_t *out_len, uint64_t *offsets);
+
 void warpjq_host_free(void *p);
 
 /* Runs the query over RFC 4180 CSV input in host memory: the header row

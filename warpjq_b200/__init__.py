@@ -45,7 +45,7 @@ HOST_SYMBOLS = [
     "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
     "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
     "warpjq_gen_nested", "warpjq_gen_nested_block", "warpjq_query_run_file", "warpjq_query_run_csv",
-    "warpjq_gen_nginx_csv", "warpjq_gen_nginx_csv_block",
+    "warpjq_gen_nginx_csv", "warpjq_gen_nginx_csv_block", "warpjq_query_render_batch",
 ]
 
 
@@ -117,6 +117,8 @@ def _load():
     k.warpjq_csv_convert.argtypes = [vp, vp, u64, u32, vp, ctypes.POINTER(vp), ctypes.POINTER(u64),
                                      ctypes.POINTER(u64), ctypes.POINTER(u64), cp, sz]
     k.warpjq_csv_convert.restype = ctypes.c_int
+    k.warpjq_csv_gather.argtypes = [vp, vp, ctypes.POINTER(u64), ctypes.POINTER(u32), u64, vp, vp, cp, sz]
+    k.warpjq_csv_gather.restype = ctypes.c_int
     h.warpjq_query_run_csv.argtypes = [vp, vp, sz, u32, ctypes.POINTER(vp), ctypes.POINTER(sz),
                                        ctypes.POINTER(u64), cp, sz]
     h.warpjq_query_run_csv.restype = ctypes.c_int
@@ -127,6 +129,9 @@ def _load():
     h.warpjq_run_bytes.restype = ctypes.c_int
     h.warpjq_query_render_device.argtypes = [vp, vp, vp, ctypes.POINTER(vp), ctypes.POINTER(sz)]
     h.warpjq_query_render_device.restype = ctypes.c_int
+    h.warpjq_query_render_batch.argtypes = [vp, vp, u32, vp, vp, vp, vp, ctypes.POINTER(vp), ctypes.POINTER(sz),
+                                            ctypes.POINTER(u64)]
+    h.warpjq_query_render_batch.restype = ctypes.c_int
     h.warpjq_host_free.argtypes = [vp]
     h.warpjq_gen_nginx.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
     h.warpjq_gen_nginx.restype = u64
@@ -406,39 +411,47 @@ class Query:
         rc = k.warpjq_batch_collect(self.ctx, items, ctypes.byref(all_), err, len(err))
         if rc:
             raise RuntimeError(err.value.decode(errors="replace"))
+        self._b_items = items
         return list(items)[: self._b_n], all_
 
     def batch_outputs(self, items, all_: DeviceResult, host_data) -> list:
-        """Each input's output bytes (what a run over it alone prints):
-        rows are cut from one copy of the batch's rows, aggregates and groups
-        rendered by the host formatter; `host_data` is the host copy of the
-        batch buffer (group keys are read from it)."""
+        """Each input's output bytes (what a run over it alone prints), from
+        one native call (warpjq_query_render_batch): rows cut from one copy
+        of the batch's rows, aggregates and groups rendered by the host
+        formatter; `host_data` (bytes or a numpy uint8 array) holds the bytes
+        the groups' key_off values index (the host copy of the batch buffer,
+        or keys gathered from the device)."""
         import numpy as np
-        rows = b""
-        row_off = None
+        n = len(items)
+        arr = getattr(self, "_b_items", None)
+        if arr is None or len(arr) < n or any(ctypes.addressof(a) != ctypes.addressof(b)
+                                              for a, b in zip(items[:1], arr[:1])):
+            arr = (BatchItem * max(1, n))(*items)
+        rows_p = row_off_p = None
+        keep = []
         if all_.n_selected and all_.d_out_bytes:  # row queries only
             import torch
             from .shard import _DeviceBytes
             nsel = all_.n_selected
-            rows = torch.as_tensor(_DeviceBytes(all_.d_out_bytes, all_.out_len), device="cuda").cpu().numpy().tobytes()
+            rows = torch.as_tensor(_DeviceBytes(all_.d_out_bytes, max(1, all_.out_len)), device="cuda").cpu()
             ro = torch.as_tensor(_DeviceBytes(all_.d_out_row_off, (nsel + 1) * 8), device="cuda").cpu()
-            row_off = np.frombuffer(ro.numpy().tobytes(), dtype=np.uint64)
-        outs = []
-        for it in items:
-            r = DeviceResult()
-            for f in ("n_lines", "n_blank", "n_invalid", "n_type_error", "n_selected", "count", "numeric",
-                      "isum_lo", "isum_hi", "n_int", "fsum", "min", "max", "sum", "saw_non_numeric"):
-                setattr(r, f, getattr(it, f))
-            if it.n_groups:
-                r.groups = ctypes.cast(ctypes.byref(all_.groups[it.group_begin]), ctypes.POINTER(_GroupExt))
-                r.n_groups = it.n_groups
-            head = self.render_device(r, host_data)
-            body = b""
-            if it.n_selected and row_off is not None:
-                a, b = int(row_off[it.row_begin]), int(row_off[it.row_begin + it.n_selected])
-                body = rows[a:b]
-            outs.append(head + body)
-        return outs
+            keep += [rows, ro]
+            rows_p, row_off_p = ctypes.c_void_p(rows.data_ptr()), ctypes.c_void_p(ro.data_ptr())
+        if isinstance(host_data, (bytes, bytearray)):
+            kb = ctypes.c_char_p(bytes(host_data))
+            keep.append(kb)
+            kaddr = ctypes.cast(kb, ctypes.c_void_p)
+        else:
+            kaddr = ctypes.c_void_p(np.asarray(host_data).ctypes.data)
+        out = ctypes.c_void_p()
+        ln = ctypes.c_size_t()
+        offs = (ctypes.c_uint64 * (n + 1))()
+        rc = self._h.warpjq_query_render_batch(self._q, arr, n, ctypes.cast(all_.groups, ctypes.c_void_p), kaddr,
+                                               rows_p, row_off_p, ctypes.byref(out), ctypes.byref(ln), offs)
+        if rc:
+            raise MemoryError("warpjq_query_render_batch")
+        body = _take(out, ln)
+        return [body[offs[i]:offs[i + 1]] for i in range(n)]
 
     def render_device(self, r: DeviceResult, host_data) -> bytes:
         """Formats a device-resident result; `host_data` (bytes or a numpy
@@ -534,6 +547,18 @@ class CsvConverter:
         if rc:
             raise RuntimeError(err.value.decode(errors="replace"))
         return (d.value or 0), nd.value, used.value, recs.value
+
+    def gather(self, d_src: int, offsets, lengths, n: int, out, stream: int = 0):
+        """Copies device slices d_src[offsets[i], + lengths[i]) back to back
+        into `out` (a writable numpy uint8 array large enough)."""
+        err = ctypes.create_string_buffer(1024)
+        if hasattr(offsets, "ctypes"):  # numpy arrays
+            offsets = offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+            lengths = lengths.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        rc = self._k.warpjq_csv_gather(self._c, ctypes.c_void_p(d_src), offsets, lengths, n,
+                                       ctypes.c_void_p(out.ctypes.data), ctypes.c_void_p(stream), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
 
     def close(self):
         if self._c:

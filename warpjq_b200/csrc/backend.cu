@@ -957,7 +957,9 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
 warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const uint64_t *offsets,
                                   const uint64_t *lengths, uint32_t n_inputs, void *stream,
                                   char *err, size_t err_len) {
-  if (!ctx || (n_inputs && (!d_data || !offsets || !lengths))) return WARPJQ_ERR_INVALID_ARG;
+  // d_data may be null: offsets are then device addresses, and the inputs
+  // may lie in different allocations.
+  if (!ctx || (n_inputs && (!offsets || !lengths))) return WARPJQ_ERR_INVALID_ARG;
   warpjq_ctx::Batch &b = ctx->batch;
   b.active = false;
   b.epoch++;

@@ -459,7 +459,7 @@ warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, 
 warpjq_status warpjq_csv_gather(warpjq_csv *c, const uint8_t *d_src, const uint64_t *offsets,
                                 const uint32_t *lengths, uint64_t n, uint8_t *h_dst, void *stream, char *err,
                                 size_t err_len) {
-  if (!c || (n && (!d_src || !offsets || !lengths || !h_dst))) {
+  if (!c || (n && (!offsets || !lengths || !h_dst))) {  // d_src null: offsets are addresses
     csv_err(err, err_len, "invalid argument");
     return WARPJQ_ERR_INVALID_ARG;
   }

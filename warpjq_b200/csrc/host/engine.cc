@@ -1071,24 +1071,24 @@ int warpjq_run_bytes(const char *query, const uint8_t *data, size_t len, uint32_
   return rc;
 }
 
-// Formats the result of a device-resident aggregate run (warpjq_ext.h) the
-// way the CLI prints it.  `data` is a host copy of the input, needed to
-// render group keys.
-int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r, const uint8_t *data,
-                               char **out, size_t *out_len) {
+// The head of one device-resident result (header, aggregate or groups)
+// into a fresh writer: what warpjq_query_render_device prints.
+static void render_head(const warpjq_query *q, Writer &w, uint64_t count, uint64_t numeric, double sum,
+                        double mn, double mx, const warpjq_group_ext *groups, uint32_t n_groups,
+                        uint64_t n_selected, const uint8_t *data) {
   const Program &P = q->prog;
-  Writer w;
   w.fmt = q->fmt;
   w.header(P);
   if (P.is_aggregate()) {
     if (!P.has_group) {
       Agg a;
-      a.merge(r->count, r->numeric, r->sum, r->min, r->max);
+      a.merge(count, numeric, sum, mn, mx);
       w.aggregate(P.agg, a);
     } else {
       std::vector<std::pair<GroupKey, Agg>> gs;
-      for (uint32_t k = 0; k < r->n_groups; k++) {
-        const warpjq_group_ext &g = r->groups[k];
+      gs.reserve(n_groups);
+      for (uint32_t k = 0; k < n_groups; k++) {
+        const warpjq_group_ext &g = groups[k];
         Agg a;
         a.merge(g.count, g.numeric, g.sum, g.min, g.max);
         gs.push_back({device_key(data, g.key_off, g.key_len, g.key_kind), a});
@@ -1097,13 +1097,59 @@ int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r, c
       w.groups(P.group_key_name(), P.agg, gs);
     }
   } else {
-    w.rows = r->n_selected;
+    w.rows = n_selected;
   }
+}
+
+// Formats the result of a device-resident aggregate run (warpjq_ext.h) the
+// way the CLI prints it.  `data` is a host copy of the input, needed to
+// render group keys.
+int warpjq_query_render_device(warpjq_query *q, const warpjq_device_result *r, const uint8_t *data,
+                               char **out, size_t *out_len) {
+  Writer w;
+  render_head(q, w, r->count, r->numeric, r->sum, r->min, r->max, r->groups, r->n_groups, r->n_selected,
+              data);
   size_t res_len = 0;
   char *res = w.finish(res_len);
   if (!res) return 1;
   *out = res;
   if (out_len) *out_len = res_len;
+  return 0;
+}
+
+// Every input's output of a collected batch (warpjq_batch_collect), back to
+// back in one malloc'd buffer: input i's bytes are out[offsets[i],
+// offsets[i+1]).  `groups` is the batch's group array, `key_data` the host
+// bytes its key_off values index; `rows` / `row_off` a host copy of the
+// batch's rows and row offsets (may be null for aggregates).
+int warpjq_query_render_batch(warpjq_query *q, const warpjq_batch_item *items, uint32_t n,
+                              const warpjq_group_ext *groups, const uint8_t *key_data, const uint8_t *rows,
+                              const uint64_t *row_off, char **out, size_t *out_len, uint64_t *offsets) {
+  *out = nullptr;
+  if (out_len) *out_len = 0;
+  std::string all;
+  offsets[0] = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const warpjq_batch_item &it = items[i];
+    Writer w;
+    render_head(q, w, it.count, it.numeric, it.sum, it.min, it.max, groups ? groups + it.group_begin : nullptr,
+                it.n_groups, it.n_selected, key_data);
+    size_t hl = 0;
+    char *h = w.finish(hl);
+    if (!h) return 1;
+    all.append(h, hl);
+    free(h);
+    if (it.n_selected && rows && row_off) {
+      const uint64_t a = row_off[it.row_begin], b = row_off[it.row_begin + it.n_selected];
+      all.append((const char *)rows + a, b - a);
+    }
+    offsets[i + 1] = all.size();
+  }
+  char *res = (char *)malloc(all.size() + 1);
+  if (!res) return 1;
+  memcpy(res, all.data(), all.size());
+  *out = res;
+  if (out_len) *out_len = all.size();
   return 0;
 }
 

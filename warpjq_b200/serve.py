@@ -1,0 +1,275 @@
+"""A resident serving loop over the device backend: continuous batching.
+
+The server keeps, per slot, a CUDA stream, one compiled query context per
+query, a device arena and a CSV converter, all alive across requests (no
+per-request context set-up).  Requests wait in arrival order.  Whenever a
+slot is free, it takes every waiting request that fits the device-memory
+budget, finds each one's NDJSON a 16-byte aligned device address (device
+inputs in place, CSV converted on the device, host inputs copied into the
+arena), and runs one batch per query among them (warpjq_batch_launch, by
+device address) on its stream, then returns to the loop: requests
+arriving meanwhile are admitted into the next free slot, so several slots'
+work overlaps on the device.  A finished slot is collected when its event
+has completed; each request's output is exactly what a run over its input
+alone prints (rows cut from the batch's rows, aggregates and groups
+rendered by the host formatter, group keys gathered from device memory).
+
+There is no reference counterpart: the reference runs one query per process
+invocation (crates/warpjq-cli).
+"""
+
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import CsvConverter, Query
+
+
+@dataclass
+class Request:
+    id: int
+    query: str
+    fmt: str                 # "ndjson" or "csv"
+    nbytes: int
+    data: object             # bytes / numpy uint8 (host) or a CUDA uint8 tensor
+    t_arrive: float = 0.0
+    t_admit: float = 0.0
+    t_done: float = 0.0
+    out: bytes = b""
+    n_lines: int = 0
+    error: str = ""
+    footprint: int = 0
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_arrive
+
+
+def footprint(nbytes: int, fmt: str) -> int:
+    """Device bytes a request may hold while in flight: its NDJSON in the
+    arena (CSV grows about 1.5x when converted, bounded here by 2x), row
+    output up to 1.25x, and a fixed part for tables."""
+    nd = nbytes * 2 if fmt == "csv" else nbytes
+    return nd + nd + nd // 4 + (1 << 20)
+
+
+def admit_count(footprints, in_flight: int, budget: int) -> int:
+    """How many of the waiting requests (in arrival order) a free slot takes:
+    the longest prefix whose footprints fit beside what is in flight.  A
+    request that does not fit waits, and so does everything behind it (no
+    overtaking, so a large request is not starved by small ones)."""
+    total, k = 0, 0
+    for f in footprints:
+        if in_flight + total + f > budget:
+            break
+        total += f
+        k += 1
+    return k
+
+
+class _Slot:
+    def __init__(self, queries, fmt_out, chunk_bytes):
+        import torch
+        self.stream = torch.cuda.Stream()
+        self.qs = {q: Query(q, fmt=fmt_out, chunk_bytes=chunk_bytes) for q in queries}
+        self.arena = torch.empty(0, dtype=torch.uint8, device="cuda")
+        self.conv = CsvConverter()
+        self.event = None
+        self.reqs: list = []
+        self.used_queries: dict = {}
+        self.keep: list = []  # converted CSV inputs of the batch in flight
+        self.footprint = 0
+
+    def busy(self) -> bool:
+        return bool(self.reqs)
+
+    def close(self):
+        for q in self.qs.values():
+            q.close()
+        self.conv.close()
+
+
+class Server:
+    """Continuous-batching server for a fixed set of queries.
+
+    submit() enqueues a request; poll() completes finished slots and admits
+    waiting requests into free ones (call it in a loop); drain() polls until
+    every submitted request is done.  `budget_bytes` caps the device memory
+    that admitted requests may hold at once (a request alone over the budget
+    is refused with an error); `max_batch` caps the requests a slot takes
+    (1 with one slot serves requests one at a time)."""
+
+    def __init__(self, queries, n_slots: int = 3, budget_bytes: int = 120 << 30, fmt_out: str = "ndjson",
+                 chunk_bytes: int = 1 << 20, max_batch: int = 0):
+        self.max_batch = max_batch  # requests per slot at most (0: no limit)
+        self.queries = list(dict.fromkeys(queries))
+        self.slots = [_Slot(self.queries, fmt_out, chunk_bytes) for _ in range(n_slots)]
+        self.budget = budget_bytes
+        self.waiting = collections.deque()
+        self.in_flight_bytes = 0
+        self.done: list = []
+        self._next_id = 0
+
+    # -- requests ---------------------------------------------------------
+    def submit(self, query: str, data, fmt: str = "ndjson", t_arrive: float | None = None) -> Request:
+        if query not in self.slots[0].qs:
+            raise KeyError(f"the server was not opened with query {query!r}")
+        if fmt not in ("ndjson", "csv"):
+            raise ValueError("fmt is 'ndjson' or 'csv'")
+        n = int(data.numel()) if hasattr(data, "numel") else len(data)
+        r = Request(self._next_id, query, fmt, n, data,
+                    t_arrive=time.perf_counter() if t_arrive is None else t_arrive)
+        r.footprint = footprint(n, fmt)
+        self._next_id += 1
+        if r.footprint > self.budget:
+            r.error = f"request of {n} bytes needs {r.footprint} bytes of device memory, over the budget"
+            r.t_done = time.perf_counter()
+            self.done.append(r)
+        else:
+            self.waiting.append(r)
+        return r
+
+    def pending(self) -> int:
+        return len(self.waiting) + sum(len(s.reqs) for s in self.slots)
+
+    # -- the loop ---------------------------------------------------------
+    def poll(self) -> list:
+        """One turn of the loop; returns the requests completed in it."""
+        finished = []
+        for s in self.slots:
+            if s.busy() and s.event.query():
+                finished += self._complete(s)
+        for s in self.slots:
+            if not s.busy() and self.waiting:
+                self._admit(s)
+        return finished
+
+    def drain(self) -> list:
+        out = []
+        while self.pending():
+            out += self.poll()
+        return out
+
+    def close(self):
+        for s in self.slots:
+            s.close()
+
+    # -- internals --------------------------------------------------------
+    def _admit(self, s: _Slot):
+        import torch
+        k = admit_count([r.footprint for r in self.waiting], self.in_flight_bytes, self.budget)
+        if self.max_batch:
+            k = min(k, self.max_batch)
+        if not k:
+            return
+        take = [self.waiting.popleft() for _ in range(k)]
+        total = sum(r.footprint for r in take)
+        now = time.perf_counter()
+        with torch.cuda.stream(s.stream):
+            # 1. every request's NDJSON at a 16-byte aligned device address:
+            #    device inputs in place, CSV converted on the device (the
+            #    converter's buffer serves one conversion at a time, so each
+            #    result is copied out), host inputs copied into the arena
+            addrs, keep, host = [None] * len(take), [], []
+            for i, r in enumerate(take):
+                r.t_admit = now
+                if r.fmt == "csv":
+                    src = self._device_bytes(r.data)
+                    s.conv.reset()
+                    d, nd, _, _ = s.conv.convert(src.data_ptr(), r.nbytes, stream=s.stream.cuda_stream)
+                    t = torch.empty(nd + 16, dtype=torch.uint8, device="cuda")
+                    if nd:
+                        t[:nd].copy_(_device_tensor(d, nd))
+                    keep.append(t)
+                    addrs[i] = (t.data_ptr(), nd)
+                elif hasattr(r.data, "is_cuda") and r.data.is_cuda and r.data.data_ptr() % 16 == 0:
+                    addrs[i] = (r.data.data_ptr(), r.nbytes)
+                else:
+                    host.append(i)
+            pos, offs = 0, {}
+            for i in host:
+                pos = (pos + 15) & ~15
+                offs[i] = pos
+                pos += take[i].nbytes
+            if host and s.arena.numel() < pos + 16:
+                s.arena = torch.empty(int((pos + 16) * 1.25), dtype=torch.uint8, device="cuda")
+            for i in host:
+                src, n, o = take[i].data, take[i].nbytes, offs[i]
+                if n:
+                    if hasattr(src, "is_cuda") and src.is_cuda:
+                        s.arena[o:o + n].copy_(src.view(torch.uint8).reshape(-1)[:n])
+                    else:
+                        h = np.frombuffer(bytes(src), dtype=np.uint8) if isinstance(src, (bytes, bytearray)) \
+                            else np.asarray(src, dtype=np.uint8).reshape(-1)
+                        s.arena[o:o + n].copy_(torch.from_numpy(h[:n].copy()).pin_memory(), non_blocking=True)
+                addrs[i] = (s.arena.data_ptr() + o, n)
+            # 2. one batch per query among them, by device address
+            by_q = {}
+            for r, (addr, n) in zip(take, addrs):
+                by_q.setdefault(r.query, []).append((r, addr, n))
+            for q, lst in by_q.items():
+                s.qs[q].batch_launch(0, [a for _, a, _ in lst], [n for _, _, n in lst], s.stream.cuda_stream)
+            s.event = torch.cuda.Event()
+            s.event.record(s.stream)
+        s.keep = keep
+        s.reqs = take
+        s.used_queries = by_q
+        s.footprint = total
+        self.in_flight_bytes += total
+
+    @staticmethod
+    def _device_bytes(data):
+        import torch
+        if hasattr(data, "is_cuda") and data.is_cuda:
+            return data.view(torch.uint8).reshape(-1)
+        host = np.frombuffer(bytes(data), dtype=np.uint8) if isinstance(data, (bytes, bytearray)) else np.asarray(data)
+        t = torch.empty(host.size + 16, dtype=torch.uint8, device="cuda")
+        if host.size:
+            t[:host.size].copy_(torch.from_numpy(host.copy()))
+        return t
+
+    def _complete(self, s: _Slot) -> list:
+        done_at = time.perf_counter()
+        out = []
+        for q, lst in s.used_queries.items():
+            Q = s.qs[q]
+            items, all_ = Q.batch_collect()
+            keys = self._gather_keys(s, all_)
+            outs = Q.batch_outputs(items, all_, keys)
+            for (r, _, _), it, o in zip(lst, items, outs):
+                r.out = o
+                r.n_lines = it.n_lines - it.n_blank
+                r.t_done = done_at
+                out.append(r)
+        self.in_flight_bytes -= s.footprint
+        s.reqs, s.used_queries, s.footprint, s.event, s.keep = [], {}, 0, None, []
+        self.done += out
+        return out
+
+    def _gather_keys(self, s: _Slot, all_) -> np.ndarray:
+        """Group keys of the batch, gathered from device memory into one host
+        buffer; the groups' key offsets (device addresses) are rewritten to
+        point into it."""
+        n = all_.n_groups
+        if not n:
+            return np.zeros(1, dtype=np.uint8)
+        g = np.ctypeslib.as_array(all_.groups, shape=(n,))
+        offs = np.ascontiguousarray(g["key_off"], dtype=np.uint64)
+        lens = np.ascontiguousarray(g["key_len"], dtype=np.uint32)
+        buf = np.zeros(int(lens.sum()) + 1, dtype=np.uint8)
+        s.conv.gather(0, offs, lens, n, buf, s.stream.cuda_stream)  # key_off values are addresses
+        at = np.zeros(n, dtype=np.uint64)
+        np.cumsum(lens[:-1], out=at[1:])
+        g["key_off"] = at
+        return buf
+
+
+def _device_tensor(ptr: int, n: int):
+    """A uint8 tensor viewing n bytes of device memory (no copy)."""
+    import torch
+    from .shard import _DeviceBytes
+    return torch.as_tensor(_DeviceBytes(ptr, n), device="cuda")
