@@ -293,7 +293,8 @@ def measure_serving(wjq, dev, offs, lens, csv_inputs, rate=2000.0, n_req=4096, s
 
     def run(slots, max_batch):
         srv = Server(SERVE_QUERIES, n_slots=slots, budget_bytes=120 << 30, max_batch=max_batch)
-        for q, t, f in reqs[:64]:  # warm: contexts and arenas reach their sizes
+        srv.warm(256 << 20)
+        for q, t, f in reqs[:64]:  # warm: the CSV path and the render path
             srv.submit(q, t, f)
         srv.drain()
         srv.done.clear()
@@ -632,6 +633,23 @@ def main():
         h2d = n * len(QUERIES)
         d2h = outs // args.e2e_steps
 
+    # The host link itself: plain pinned-to-device copies of 1 GiB (CUDA
+    # events), the ceiling of any end-to-end figure from host memory.
+    link_gbs = None
+    if args.e2e_steps > 0:
+        m = min(n, 1 << 30)
+        dst = torch.empty(m, dtype=torch.uint8, device="cuda")
+        dst.copy_(host[:m], non_blocking=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            dst.copy_(host[:m], non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        link_gbs = round(3 * m / (e0.elapsed_time(e1) / 1e3) / 1e9, 2)
+        del dst
+
     batch = serve = nested = e2e_file = csv_leg = None
     if rank == 0 and world == 1 and not args.no_batch:
         bdev, boffs, blens, bq = batch_workload(hnp, n)
@@ -679,7 +697,8 @@ def main():
                          "traffic": traffic, "peak_source": which,
                          "kernel": "k_scan (one launch per query; algorithmic bytes = input + output)"},
             "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "GB/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "host_link_h2d_gbs": link_gbs},
             "gpu_launches": kernels_per_step * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -90,6 +90,7 @@ def test_device_resident_requests():
     import torch
     reqs = workload(seed=9, n=40)
     srv = Server(QUERIES, n_slots=2)
+    srv.warm(1 << 20)
     hs = []
     for q, data, fmt in reqs:
         t = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()

@@ -47,13 +47,17 @@ template <class T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  // Grows to at least `want`; a buffer that grows again takes 1.5x its old
+  // size, so inputs of varying size reallocate (and synchronise the device
+  // in cudaFree) only a few times.
   cudaError_t ensure(size_t want) {
     if (want <= n && p) return cudaSuccess;
+    const size_t grown = n ? std::max(want, n + n / 2) : want;
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
-    cudaError_t e = cudaMalloc((void **)&p, std::max<size_t>(want, 1) * sizeof(T));
-    if (e == cudaSuccess) n = want;
+    cudaError_t e = cudaMalloc((void **)&p, std::max<size_t>(grown, 1) * sizeof(T));
+    if (e == cudaSuccess) n = grown;
     return e;
   }
   void release() {
@@ -244,13 +248,15 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
   if (P.needs_rows) {
     CK(rb.row_tiles.ensure(n_tiles), "alloc row tiles");
     CK(rb.row_bsum.ensure(3 * ((n_tiles + 31) / 32)), "alloc row prefixes");
-    // Records accumulate over all of a CTA's tiles: start with room for a
-    // row per KiB of input, grown on overflow.
-    if (!rb.rec_cap_per_cta) rb.rec_cap_per_cta = n / 1024 / std::max(1u, c->grid) + 1024;
+    // Records accumulate over all of a CTA's tiles: room for a row per KiB
+    // of input, grown on overflow; output and row capacities follow the
+    // input's size too (a larger input than the last does not overflow
+    // for that reason alone).
+    rb.rec_cap_per_cta = std::max(rb.rec_cap_per_cta, n / 1024 / std::max(1u, c->grid) + 1024);
     CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * P.rec_stride), "alloc records");
-    if (!rb.out_cap) rb.out_cap = n + n / 4 + (1u << 20);
+    rb.out_cap = std::max(rb.out_cap, n + n / 4 + (1u << 20));
     CK(rb.out.ensure(rb.out_cap), "alloc output");
-    if (!rb.rows_cap) rb.rows_cap = n / 32 + 4096;
+    rb.rows_cap = std::max(rb.rows_cap, n / 32 + 4096);
     CK(rb.row_off.ensure(rb.rows_cap + 1), "alloc row offsets");
     CK(rb.line_idx.ensure(rb.rows_cap), "alloc line index");
   }

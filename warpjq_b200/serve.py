@@ -133,6 +133,32 @@ class Server:
             self.waiting.append(r)
         return r
 
+    def warm(self, reserve_bytes: int = 64 << 20):
+        """Runs every slot's every query once over `reserve_bytes` of blank
+        lines, so contexts reach their start-up sizes (records, nesting
+        stack, group table, row buffers for inputs that large) before
+        requests arrive: the first request of a query on a slot then pays no
+        allocation."""
+        import torch
+        buf = torch.full((reserve_bytes + 16,), 0x20, dtype=torch.uint8, device="cuda")
+        buf[4095::4096] = 0x0A
+        line = b'{"a":"x","b":1}\n'
+        small = torch.frombuffer(bytearray(line + bytes(16)), dtype=torch.uint8).cuda()
+        csv = torch.frombuffer(bytearray(b"a,b\nx,1\n" + bytes(16)), dtype=torch.uint8).cuda()
+        for s in self.slots:
+            with torch.cuda.stream(s.stream):
+                for Q in s.qs.values():
+                    Q.batch_launch(buf.data_ptr(), [0], [reserve_bytes], s.stream.cuda_stream)
+                    Q.batch_collect()
+                    # the render path on a line with every kind of result
+                    Q.batch_launch(small.data_ptr(), [0], [len(line)], s.stream.cuda_stream)
+                    items, all_ = Q.batch_collect()
+                    Q.batch_outputs(items, all_, self._gather_keys(s, all_, base=small.data_ptr()))
+                # the CSV kernels and the converter's buffers
+                s.conv.reset()
+                s.conv.convert(csv.data_ptr(), 8, stream=s.stream.cuda_stream)
+        torch.cuda.synchronize()
+
     def pending(self) -> int:
         return len(self.waiting) + sum(len(s.reqs) for s in self.slots)
 
@@ -250,10 +276,10 @@ class Server:
         self.done += out
         return out
 
-    def _gather_keys(self, s: _Slot, all_) -> np.ndarray:
+    def _gather_keys(self, s: _Slot, all_, base: int = 0) -> np.ndarray:
         """Group keys of the batch, gathered from device memory into one host
-        buffer; the groups' key offsets (device addresses) are rewritten to
-        point into it."""
+        buffer; the groups' key offsets (device addresses, or offsets from
+        `base`) are rewritten to point into it."""
         n = all_.n_groups
         if not n:
             return np.zeros(1, dtype=np.uint8)
@@ -261,7 +287,7 @@ class Server:
         offs = np.ascontiguousarray(g["key_off"], dtype=np.uint64)
         lens = np.ascontiguousarray(g["key_len"], dtype=np.uint32)
         buf = np.zeros(int(lens.sum()) + 1, dtype=np.uint8)
-        s.conv.gather(0, offs, lens, n, buf, s.stream.cuda_stream)  # key_off values are addresses
+        s.conv.gather(base, offs, lens, n, buf, s.stream.cuda_stream)
         at = np.zeros(n, dtype=np.uint64)
         np.cumsum(lens[:-1], out=at[1:])
         g["key_off"] = at
