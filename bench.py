@@ -190,10 +190,19 @@ def measure_batch(wjq, dev, offs, lens, qidx):
     import torch
     stream = torch.cuda.current_stream().cuda_stream
     ptr = dev.data_ptr()
+    from warpjq_b200 import tune
     plain_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
     batch_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
     groups = [[i for i in range(len(offs)) if qidx[i] == k] for k in range(len(BATCH_QUERIES))]
     total = sum(lens)
+    # tile (and group capacity) per query, measured on the first 256 MB of
+    # the packed inputs, applied to every arm alike
+    m = min(total, 256 << 20)
+    sample = dev[:1 << 20].cpu().numpy().tobytes()
+    tuned = {q: tune.tune(q, ptr, m, sample, reps=2, use_cache=False) for q in BATCH_QUERIES}
+    for arm in (plain_q, batch_q):
+        for k, q in enumerate(BATCH_QUERIES):
+            tune.apply(arm[k], tuned[q])
 
     def plain():
         for i in range(len(offs)):
@@ -208,6 +217,8 @@ def measure_batch(wjq, dev, offs, lens, qidx):
             batch_q[k].batch_collect()
 
     graph_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
+    for k, q in enumerate(BATCH_QUERIES):
+        tune.apply(graph_q[k], tuned[q])
     graph = wjq.BatchGraph([(graph_q[k], ptr, [offs[i] for i in g], [lens[i] for i in g])
                             for k, g in enumerate(groups)])
 
@@ -236,7 +247,10 @@ def measure_batch(wjq, dev, offs, lens, qidx):
             "graph_s": round(out["graph"], 4),
             "graph": "one CUDA graph: the 8 queries' batches captured on forked streams, one launch",
             "speedup": round(out["plain"] / out["batched"], 2),
-            "graph_speedup": round(out["plain"] / out["graph"], 2)}
+            "graph_speedup": round(out["plain"] / out["graph"], 2),
+            "tuned": {q: {"tile": c["tile"], "halo": c["halo"], "group_keys": c["group_keys"],
+                          "gbs": c["gbs"], "autotile": c["autotile"], "autotile_gbs": c["autotile_gbs"]}
+                      for q, c in tuned.items()}}
 
 
 SERVE_QUERIES = BATCH_QUERIES + [

@@ -204,6 +204,15 @@ void warpjq_batch_graph_destroy(warpjq_batch_graph *g);
  * 64 KiB.  Waits for the device and releases the context's buffers. */
 warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t halo_bytes);
 
+/* Room for `keys` distinct keys (a power of two, 1024 .. 2^28; the table
+ * has twice as many slots) in a fresh group table of this context; it still
+ * grows on overflow.  Default 65,536.  A table sized for the input's
+ * cardinality avoids the rerun an overflow costs; a small one is cleared
+ * faster.  Waits for the device and releases the context's group table.  No
+ * reference counterpart (the reference's table is fixed at 65,536 slots,
+ * warpjq_kernels.cu:1232-1345). */
+warpjq_status warpjq_set_group_capacity(warpjq_ctx *ctx, uint32_t keys);
+
 /* Chooses the tiling for input shaped like `sample` (host bytes, e.g. the
  * first megabyte of the input): tiles holding close to a whole number of
  * 32-line rounds, and a halo longer than the longest line seen.  With fewer

@@ -38,7 +38,7 @@ EXT_SYMBOLS = [
     "warpjq_batch_launch", "warpjq_batch_collect", "warpjq_host_alloc_pinned",
     "warpjq_host_free_pinned", "warpjq_csv_create", "warpjq_csv_destroy", "warpjq_csv_reset",
     "warpjq_csv_convert", "warpjq_csv_gather", "warpjq_device_read", "warpjq_batch_graph_create",
-    "warpjq_batch_graph_launch", "warpjq_batch_graph_destroy",
+    "warpjq_batch_graph_launch", "warpjq_batch_graph_destroy", "warpjq_set_group_capacity",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
@@ -80,6 +80,8 @@ def _load():
     k.warpjq_collect_device.restype = ctypes.c_int
     k.warpjq_set_tiling.argtypes = [vp, u32, u32]
     k.warpjq_set_tiling.restype = ctypes.c_int
+    k.warpjq_set_group_capacity.argtypes = [vp, u32]
+    k.warpjq_set_group_capacity.restype = ctypes.c_int
     k.warpjq_autotile.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(u32),
                                   ctypes.POINTER(u32)]
     k.warpjq_autotile.restype = ctypes.c_int
@@ -354,6 +356,13 @@ class Query:
         k, _ = _load()
         if k.warpjq_set_tiling(self.ctx, tile_bytes, halo_bytes) != 0:
             raise ValueError("bad tiling")
+
+    def set_group_capacity(self, keys: int):
+        """Room for `keys` distinct keys in a fresh group table (a power of
+        two, 1024 .. 2^28); the table still grows on overflow."""
+        k, _ = _load()
+        if k.warpjq_set_group_capacity(self.ctx, keys) != 0:
+            raise ValueError("bad group capacity")
 
     def autotile(self, sample) -> tuple:
         """Chooses the device tiling from a host sample of the input (bytes or

@@ -175,6 +175,7 @@ struct warpjq_ctx {
   unsigned long long chunk_cap = 0;
   uint32_t tile_bytes = 6144;
   uint32_t halo_bytes = 2048;
+  uint32_t group_keys0 = 1u << 16;  // distinct keys a fresh group table has room for
   unsigned grid = 0;        // persistent CTAs for the scan kernel
   size_t scan_smem = 0;
   std::vector<Slot> slots;
@@ -262,8 +263,8 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
   }
   if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
     if (!rb.g_cap) {
-      rb.g_cap = 1u << 17;
-      rb.g_key_cap = 1u << 16;
+      rb.g_key_cap = c->group_keys0;
+      rb.g_cap = 2 * c->group_keys0;
     }
     CK(rb.g_slots.ensure(rb.g_cap), "alloc group table");
     CK(rb.g_keys.ensure(rb.g_key_cap), "alloc group keys");
@@ -849,6 +850,23 @@ warpjq_status warpjq_set_tiling(warpjq_ctx *ctx, uint32_t tile_bytes, uint32_t h
   for (auto &s : ctx->slots) s.rb.release();
   ctx->dev.rb.release();
   return configure_grid(ctx, err, err_len);
+}
+
+warpjq_status warpjq_set_group_capacity(warpjq_ctx *ctx, uint32_t keys) {
+  char *err = nullptr;
+  size_t err_len = 0;
+  if (!ctx || keys < 1024 || keys > (1u << 28) || (keys & (keys - 1))) return WARPJQ_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize(), "sync");
+  ctx->group_keys0 = keys;
+  auto drop = [](RunBufs &rb) {
+    rb.g_slots.release();
+    rb.g_keys.release();
+    rb.g_acc.release();
+    rb.g_cap = rb.g_key_cap = 0;
+  };
+  for (auto &s : ctx->slots) drop(s.rb);
+  drop(ctx->dev.rb);
+  return WARPJQ_OK;
 }
 
 warpjq_status warpjq_autotile(warpjq_ctx *ctx, const uint8_t *sample, uint64_t len,

@@ -301,12 +301,12 @@ template <typename T>
 struct DBuf {  // device buffer that only grows
   T *p = nullptr;
   size_t n = 0;
-  cudaError_t ensure(size_t want) {
+  cudaError_t ensure(size_t want) {  // grows by at least 1.5x (cudaFree synchronises the device)
     if (want <= n) return cudaSuccess;
+    want = std::max(want + want / 8, n + n / 2);
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
-    want += want / 8;
     cudaError_t e = cudaMalloc((void **)&p, want * sizeof(T));
     if (e == cudaSuccess) n = want;
     return e;

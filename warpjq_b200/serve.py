@@ -135,16 +135,18 @@ class Server:
 
     def warm(self, reserve_bytes: int = 64 << 20):
         """Runs every slot's every query once over `reserve_bytes` of blank
-        lines, so contexts reach their start-up sizes (records, nesting
-        stack, group table, row buffers for inputs that large) before
-        requests arrive: the first request of a query on a slot then pays no
-        allocation."""
+        lines, and every slot's CSV converter over up to 64 MiB, so contexts
+        and converters reach their sizes (records, nesting stack, group
+        table, row buffers, CSV tables for inputs that large) and every
+        kernel is loaded before requests arrive: serving then allocates
+        (and synchronises the device in cudaFree) only for larger inputs."""
         import torch
         buf = torch.full((reserve_bytes + 16,), 0x20, dtype=torch.uint8, device="cuda")
         buf[4095::4096] = 0x0A
         line = b'{"a":"x","b":1}\n'
         small = torch.frombuffer(bytearray(line + bytes(16)), dtype=torch.uint8).cuda()
-        csv = torch.frombuffer(bytearray(b"a,b\nx,1\n" + bytes(16)), dtype=torch.uint8).cuda()
+        rows = b"a,b\n" + b'"x",1\n' * (min(reserve_bytes, 64 << 20) // 6)
+        csv = torch.frombuffer(bytearray(rows + bytes(16)), dtype=torch.uint8).cuda()
         for s in self.slots:
             with torch.cuda.stream(s.stream):
                 for Q in s.qs.values():
@@ -156,7 +158,7 @@ class Server:
                     Q.batch_outputs(items, all_, self._gather_keys(s, all_, base=small.data_ptr()))
                 # the CSV kernels and the converter's buffers
                 s.conv.reset()
-                s.conv.convert(csv.data_ptr(), 8, stream=s.stream.cuda_stream)
+                s.conv.convert(csv.data_ptr(), len(rows), stream=s.stream.cuda_stream)
         torch.cuda.synchronize()
 
     def pending(self) -> int:

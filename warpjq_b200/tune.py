@@ -1,0 +1,119 @@
+"""Autotuner: measures, instead of guessing, the scan's tunables for a query
+on a sample of its input, and caches the choice.
+
+Swept, each timed with CUDA events around the device-resident run (best of
+`reps` after a warm-up):
+  - tile bytes (the bytes one warp stages and walks per tile; with one line
+    per lane, the tile sets how many 32-line rounds a warp runs per tile),
+    with the halo from warpjq_autotile's longest-line rule;
+  - for group_by queries, the group table's starting capacity (a table
+    sized for the input's cardinality avoids an overflow rerun; a small one
+    is cleared and cached faster).
+Lines per round are fixed at 32 by the design (one line per lane), so they
+are not swept.
+
+The cache is a JSON file keyed by device name, query and the sample's mean
+line length (rounded to a power of two), so inputs of the same shape reuse
+a choice without measuring again.  warpjq_autotile's analytic choice is
+always one of the candidates, so a tuned choice is never slower on the
+sample than the default.
+"""
+
+from __future__ import annotations
+
+import json
+import math
+import os
+
+from . import Query, device_name
+
+TILES = (2048, 3072, 4096, 5120, 6144, 6400, 7168, 8192, 10240, 12288, 16384)
+GROUP_KEYS = (1 << 12, 1 << 14, 1 << 16, 1 << 18, 1 << 20)
+
+
+def default_cache_path() -> str:
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "warpjq_b200", "tune.json")
+
+
+def shape_key(device: str, query: str, sample: bytes) -> str:
+    lines = sample.count(b"\n")
+    mean = len(sample) / max(1, lines)
+    return f"{device}|{query}|{2 ** round(math.log2(max(1.0, mean)))}"
+
+
+def load_cache(path: str) -> dict:
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def save_cache(path: str, cache: dict):
+    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(cache, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def _time(Q: Query, d_ptr: int, n: int, reps: int) -> float:
+    import torch
+    stream = torch.cuda.current_stream()
+    Q.launch_device(d_ptr, n, stream.cuda_stream)
+    Q.collect_device()
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Q.launch_device(d_ptr, n, stream.cuda_stream)
+        e1.record(stream)
+        Q.collect_device()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best
+
+
+def tune(query: str, d_ptr: int, n: int, sample: bytes, reps: int = 3, cache_path: str | None = None,
+         use_cache: bool = True) -> dict:
+    """Best tile (and group capacity) for `query` over n bytes at device
+    address d_ptr (the sample to time on; `sample` is a host copy of its
+    first bytes, for the halo rule and the cache key).  Returns
+    {"tile": T, "halo": H, "group_keys": K or None, "gbs": rate, "from_cache": bool}."""
+    cache_path = cache_path or default_cache_path()
+    key = shape_key(device_name(), query, sample[: 1 << 20])
+    cache = load_cache(cache_path) if use_cache else {}
+    if use_cache and key in cache:
+        return dict(cache[key], from_cache=True)
+    Q = Query(query)
+    t0, h = Q.autotile(sample[: 1 << 20])
+    tiles = sorted(set(t for t in TILES if t + h <= 65535 - 64) | {t0})
+    timings = {}
+    for t in tiles:
+        Q.set_tiling(t, h)
+        timings[t] = _time(Q, d_ptr, n, reps)
+    best_t = min(timings, key=timings.get)
+    Q.set_tiling(best_t, h)
+    best_keys, best_ms = None, timings[best_t]
+    if Q.is_grouped:
+        for k in GROUP_KEYS:
+            Q.set_group_capacity(k)
+            ms = _time(Q, d_ptr, n, reps)
+            if ms < best_ms:
+                best_keys, best_ms = k, ms
+    Q.close()
+    res = {"tile": best_t, "halo": h, "group_keys": best_keys, "gbs": round(n / (best_ms / 1e3) / 1e9, 2),
+           "autotile": t0, "autotile_gbs": round(n / (timings[t0] / 1e3) / 1e9, 2),
+           "swept": {str(t): round(n / (ms / 1e3) / 1e9, 2) for t, ms in timings.items()}}
+    if use_cache:
+        cache[key] = res
+        save_cache(cache_path, cache)
+    return dict(res, from_cache=False)
+
+
+def apply(Q: Query, choice: dict):
+    """Sets a tuned choice on a query's context."""
+    Q.set_tiling(choice["tile"], choice["halo"])
+    if choice.get("group_keys"):
+        Q.set_group_capacity(choice["group_keys"])
