@@ -48,15 +48,19 @@ struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
   // Grows to at least `want`; a buffer that grows again takes 1.5x its old
-  // size, so inputs of varying size reallocate (and synchronise the device
-  // in cudaFree) only a few times.
-  cudaError_t ensure(size_t want) {
+  // size, so inputs of varying size reallocate only a few times.  Growth is
+  // stream-ordered on `st` (the launch stream, whose earlier runs on this
+  // buffer have been collected): the old block returns to the device's
+  // memory pool and the new one comes from it without synchronising the
+  // device, so other streams' work runs on.  Never during a graph capture.
+  cudaError_t ensure(size_t want, cudaStream_t st, bool capturing) {
     if (want <= n && p) return cudaSuccess;
+    if (capturing) return cudaErrorStreamCaptureUnsupported;
     const size_t grown = n ? std::max(want, n + n / 2) : want;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     n = 0;
-    cudaError_t e = cudaMalloc((void **)&p, std::max<size_t>(grown, 1) * sizeof(T));
+    cudaError_t e = cudaMallocAsync((void **)&p, std::max<size_t>(grown, 1) * sizeof(T), st);
     if (e == cudaSuccess) n = grown;
     return e;
   }
@@ -235,40 +239,40 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
 
 // Sizes the buffers of `s` for an input of n bytes (first use, or growth).
 warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
-                          unsigned long long n_tiles, char *err, size_t err_len) {
+                          unsigned long long n_tiles, cudaStream_t st, bool cap, char *err, size_t err_len) {
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
   if (n_tiles == 0) n_tiles = 1;
-  CK(rb.ctr.ensure(1), "alloc counters");
-  CK(rb.tiles.ensure(n_tiles), "alloc tiles");
-  CK(rb.tile_fsum.ensure(n_tiles), "alloc tile sums");
-  CK(rb.block_f.ensure(kReduceBlocks), "alloc reduce");
-  CK(rb.block_lines.ensure(2 * kReduceBlocks), "alloc reduce");
+  CK(rb.ctr.ensure(1, st, cap), "alloc counters");
+  CK(rb.tiles.ensure(n_tiles, st, cap), "alloc tiles");
+  CK(rb.tile_fsum.ensure(n_tiles, st, cap), "alloc tile sums");
+  CK(rb.block_f.ensure(kReduceBlocks, st, cap), "alloc reduce");
+  CK(rb.block_lines.ensure(2 * kReduceBlocks, st, cap), "alloc reduce");
   if (!rb.deep_levels) rb.deep_levels = 1u << 16;
-  CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32)), "alloc deep stack");
+  CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32), st, cap), "alloc deep stack");
   if (P.needs_rows) {
-    CK(rb.row_tiles.ensure(n_tiles), "alloc row tiles");
-    CK(rb.row_bsum.ensure(3 * ((n_tiles + 31) / 32)), "alloc row prefixes");
+    CK(rb.row_tiles.ensure(n_tiles, st, cap), "alloc row tiles");
+    CK(rb.row_bsum.ensure(3 * ((n_tiles + 31) / 32), st, cap), "alloc row prefixes");
     // Records accumulate over all of a CTA's tiles: room for a row per KiB
     // of input, grown on overflow; output and row capacities follow the
     // input's size too (a larger input than the last does not overflow
     // for that reason alone).
     rb.rec_cap_per_cta = std::max(rb.rec_cap_per_cta, n / 1024 / std::max(1u, c->grid) + 1024);
-    CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * P.rec_stride), "alloc records");
+    CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * P.rec_stride, st, cap), "alloc records");
     rb.out_cap = std::max(rb.out_cap, n + n / 4 + (1u << 20));
-    CK(rb.out.ensure(rb.out_cap), "alloc output");
+    CK(rb.out.ensure(rb.out_cap, st, cap), "alloc output");
     rb.rows_cap = std::max(rb.rows_cap, n / 32 + 4096);
-    CK(rb.row_off.ensure(rb.rows_cap + 1), "alloc row offsets");
-    CK(rb.line_idx.ensure(rb.rows_cap), "alloc line index");
+    CK(rb.row_off.ensure(rb.rows_cap + 1, st, cap), "alloc row offsets");
+    CK(rb.line_idx.ensure(rb.rows_cap, st, cap), "alloc line index");
   }
   if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
     if (!rb.g_cap) {
       rb.g_key_cap = c->group_keys0;
       rb.g_cap = 2 * c->group_keys0;
     }
-    CK(rb.g_slots.ensure(rb.g_cap), "alloc group table");
-    CK(rb.g_keys.ensure(rb.g_key_cap), "alloc group keys");
-    CK(rb.g_acc.ensure(rb.g_key_cap), "alloc group accumulators");
+    CK(rb.g_slots.ensure(rb.g_cap, st, cap), "alloc group table");
+    CK(rb.g_keys.ensure(rb.g_key_cap, st, cap), "alloc group keys");
+    CK(rb.g_acc.ensure(rb.g_key_cap, st, cap), "alloc group accumulators");
   }
   return WARPJQ_OK;
 }
@@ -291,21 +295,21 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
                           cudaStream_t st, char *err, size_t err_len,
                           const warpjq_ctx::Batch *b = nullptr) {
   const unsigned long long n_tiles = b ? b->n_tiles : (n + c->tile_bytes - 1) / c->tile_bytes;
-  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, err, err_len);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(st, &cap), "capture status");
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, st, capturing, err, err_len);
   if (rc != WARPJQ_OK) return rc;
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
   bool groups = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
   const uint32_t n_inputs = b ? (uint32_t)b->start.size() : 0;
-  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-  CK(cudaStreamIsCapturing(st, &cap), "capture status");
-  const bool capturing = cap != cudaStreamCaptureStatusNone;
   if (b && !b->tables_on_device) {
-    CK(rb.b_in_start.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
-    CK(rb.b_in_end.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
-    CK(rb.b_in_tile0.ensure(n_inputs + 1), "alloc batch tables");
-    CK(rb.b_in_ctr.ensure(std::max<uint32_t>(n_inputs, 1)), "alloc batch tables");
-    CK(rb.b_tile_input.ensure(std::max<unsigned long long>(n_tiles, 1)), "alloc batch tables");
+    CK(rb.b_in_start.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch tables");
+    CK(rb.b_in_end.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch tables");
+    CK(rb.b_in_tile0.ensure(n_inputs + 1, st, capturing), "alloc batch tables");
+    CK(rb.b_in_ctr.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch tables");
+    CK(rb.b_tile_input.ensure(std::max<unsigned long long>(n_tiles, 1), st, capturing), "alloc batch tables");
     // pageable sources: staged by the driver before the calls return
     CK(cudaMemcpyAsync(rb.b_in_start.p, b->start.data(), n_inputs * 8ull, cudaMemcpyHostToDevice, st),
        "H2D batch tables");
@@ -570,6 +574,16 @@ warpjq_status warpjq_ctx_create(const warpjq_program *prog, uint64_t max_chunk_b
   if (rc != WARPJQ_OK) return rc;
   CK(cudaGetDevice(&c->device), "cudaGetDevice");
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+  {
+    // Run buffers grow from the device's default memory pool
+    // (stream-ordered); keep up to 8 GiB of what they give back cached in
+    // the pool instead of returning it to the driver at every
+    // synchronisation.
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, c->device), "memory pool");
+    uint64_t keep = 8ull << 30;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
+  }
   CK(cudaMalloc((void **)&c->d_plan, sizeof(DevPlan)), "alloc plan");
   CK(cudaMemcpy(c->d_plan, &c->plan, sizeof(DevPlan), cudaMemcpyHostToDevice), "upload plan");
   rc = configure_grid(c.get(), err, err_len);
@@ -584,9 +598,10 @@ warpjq_status warpjq_ctx_create(const warpjq_program *prog, uint64_t max_chunk_b
     CK(cudaMalloc((void **)&s.d_chunk, max_chunk_bytes + 16), "device chunk");
     CK(cudaHostAlloc((void **)&s.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
     if (max_chunk_bytes) {
-      rc = ensure_bufs(c.get(), s, max_chunk_bytes,
-                       (max_chunk_bytes + c->tile_bytes - 1) / c->tile_bytes, err, err_len);
+      rc = ensure_bufs(c.get(), s, max_chunk_bytes, (max_chunk_bytes + c->tile_bytes - 1) / c->tile_bytes,
+                       s.stream, false, err, err_len);
       if (rc != WARPJQ_OK) return rc;
+      CK(cudaStreamSynchronize(s.stream), "stream sync");
     }
   }
   CK(cudaHostAlloc((void **)&c->dev.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
