@@ -29,7 +29,7 @@
 namespace wjq {
 
 constexpr int kThreads = 32;                 // one warp per CTA; each warp owns its tile
-constexpr uint32_t kMaxLinesPerPass = 512;   // line-start list capacity per pass
+constexpr uint32_t kMaxLinesPerPass = 128;   // line-start list capacity per pass
 constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
 constexpr int kScanBlocksPerSM = 24;         // register budget of k_scan: 24 warps per SM
 
