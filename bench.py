@@ -516,6 +516,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batch and serving legs")
     ap.add_argument("--csv-only", type=int, default=0, metavar="BYTES",
                     help="only the device-resident CSV leg, on BYTES of CSV (for profiling)")
+    ap.add_argument("--nested-only", type=int, default=0, metavar="BYTES",
+                    help="only the nested-schema leg, on BYTES of input (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -532,6 +534,9 @@ def main():
     import warpjq_b200 as wjq
     if args.csv_only:
         print(json.dumps({"csv": measure_csv(wjq, args.csv_only, reps=args.steps, e2e=False)}), flush=True)
+        return
+    if args.nested_only:
+        print(json.dumps({"nested": measure_nested(wjq, args.nested_only, reps=args.steps)}), flush=True)
         return
 
     torch.cuda.set_device(local)
