@@ -288,6 +288,8 @@ typedef struct warpjq_csv warpjq_csv;
 
 #define WARPJQ_CSV_FINAL 1u      /* the input ends with this chunk */
 #define WARPJQ_CSV_HOST_INPUT 2u /* `src` is host memory (copied to the device first) */
+#define WARPJQ_CSV_AFTER_STAGE0 4u /* wait for staging buffer 0's last copy first */
+#define WARPJQ_CSV_AFTER_STAGE1 8u /* wait for staging buffer 1's last copy first */
 
 warpjq_status warpjq_csv_create(warpjq_csv **out);
 void warpjq_csv_destroy(warpjq_csv *c);
@@ -308,6 +310,25 @@ void warpjq_csv_reset(warpjq_csv *c);
 warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, uint32_t flags,
                                  void *stream, const uint8_t **d_ndjson, uint64_t *ndjson_len,
                                  uint64_t *consumed, uint64_t *records, char *err, size_t err_len);
+
+/* Staging for a pipelined host input: copies n bytes of host memory
+ * (page-locked, for the copy to be asynchronous) to offset `at` of the
+ * converter's device staging buffer `buf` (0 or 1) on the converter's own
+ * copy stream, and returns the buffer's device address in *d_buf.  A
+ * conversion passed WARPJQ_CSV_AFTER_STAGE0/1 waits on the device for that
+ * buffer's last staging, so the next chunk can be copied while this one is
+ * converted and scanned.  Growing a buffer drops its bytes.  The host bytes
+ * must stay unchanged until warpjq_csv_stage_wait on the buffer returns or a
+ * conversion that waited on it has returned. */
+warpjq_status warpjq_csv_stage(warpjq_csv *c, uint32_t buf, uint64_t at, const uint8_t *h_src,
+                               uint64_t n, uint8_t **d_buf, char *err, size_t err_len);
+warpjq_status warpjq_csv_stage_wait(warpjq_csv *c, uint32_t buf, char *err, size_t err_len);
+
+/* Copies n bytes of device memory (e.g. the unconsumed end of a chunk: a
+ * row to be continued) to offset `at` of staging buffer `buf` on `stream`;
+ * [at, at + n) must lie inside the buffer. */
+warpjq_status warpjq_csv_carry(warpjq_csv *c, const uint8_t *d_src, uint64_t n, uint32_t buf,
+                               uint64_t at, void *stream, char *err, size_t err_len);
 
 /* Copies the device byte slices d_src[offsets[i], + lengths[i]), i < n, to
  * host memory h_dst back to back (d_src may be NULL: offsets are then

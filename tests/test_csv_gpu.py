@@ -148,3 +148,28 @@ def test_empty_and_header_only_csv():
         r = Q.run_csv(src)
         assert r.rc == 0 and r.out == orc.run("count", b"").out
         Q.close()
+
+
+def test_pipelined_chunks_carry_long_rows():
+    """warpjq_query_run_csv copies chunk k + 1 while chunk k is converted;
+    rows longer than the room kept for a carried row (64 KiB), and a row
+    longer than a whole 1 MiB chunk, must come out the same as in one piece,
+    from page-locked and from ordinary host memory."""
+    import torch
+    rng = random.Random(17)
+    rows = [b"k,v"]
+    for i in range(400):
+        n = rng.choice([10, 100, 1000, 90_000, 300_000]) if i != 200 else 2_500_000
+        rows.append(b'"' + (b"x" * n).replace(b"xxxxxxxxxx", b'x""x,x\nxxx', 1) + b'",' + str(i).encode())
+    src = b"\n".join(rows) + b"\n"
+    nd = csv_map.csv_to_ndjson(src)
+    pinned = torch.empty(len(src), dtype=torch.uint8).pin_memory()
+    pinned.numpy()[:] = np.frombuffer(src, dtype=np.uint8)
+    for q in ["count", "sum(.v)", "select(.v > 390) | {v: .v, k: .k}"]:
+        want = orc.run(q, nd).out
+        for data in (src, pinned.numpy()):
+            Q = wjq.Query(q, chunk_bytes=1 << 20)
+            r = Q.run_csv(data)
+            assert r.rc == 0, r.err
+            assert r.out == want, (q, r.out[:200], want[:200])
+            Q.close()

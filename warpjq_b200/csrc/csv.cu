@@ -328,7 +328,17 @@ struct warpjq_csv {
   bool have_header = false;  // header names taken from an earlier chunk
   std::string key_text;
   std::vector<uint32_t> key_offs, key_words, key_meta;
+  // chunks staged from host memory on a copy stream of their own
+  DBuf<uint8_t> stage[2];
+  cudaStream_t copy = nullptr;
+  cudaEvent_t staged[2] = {nullptr, nullptr};
   ~warpjq_csv() {
+    if (copy) cudaStreamSynchronize(copy);
+    for (int b = 0; b < 2; b++) {
+      stage[b].release();
+      if (staged[b]) cudaEventDestroy(staged[b]);
+    }
+    if (copy) cudaStreamDestroy(copy);
     in.release();
     run_stat.release();
     tile_state.release();
@@ -382,6 +392,9 @@ warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, 
   if (records) *records = 0;
   if (n == 0) return WARPJQ_OK;
   const uint8_t *d = src;
+  for (int b = 0; b < 2; b++)
+    if ((flags & (WARPJQ_CSV_AFTER_STAGE0 << b)) && c->staged[b])
+      CSV_CK(cudaStreamWaitEvent(st, c->staged[b], 0), "wait for a staged chunk");
   if (flags & WARPJQ_CSV_HOST_INPUT) {
     CSV_CK(c->in.ensure(n + 16), "device memory for the CSV input");
     CSV_CK(cudaMemcpyAsync(c->in.p, src, n, cudaMemcpyHostToDevice, st), "copy of the CSV input");
@@ -453,6 +466,44 @@ warpjq_status warpjq_csv_convert(warpjq_csv *c, const uint8_t *src, uint64_t n, 
   CSV_CK(cudaGetLastError(), "CSV to NDJSON");
   *d_ndjson = c->out.p;
   *ndjson_len = total;
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_csv_stage(warpjq_csv *c, uint32_t buf, uint64_t at, const uint8_t *h_src, uint64_t n,
+                               uint8_t **d_buf, char *err, size_t err_len) {
+  if (!c || buf > 1 || (!h_src && n) || !d_buf) {
+    csv_err(err, err_len, "invalid argument");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  if (!c->copy) {
+    CSV_CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking), "copy stream");
+    for (int b = 0; b < 2; b++) CSV_CK(cudaEventCreateWithFlags(&c->staged[b], cudaEventDisableTiming), "copy event");
+  }
+  if (c->stage[buf].n < at + n + 16) {  // the buffer's bytes do not survive growth
+    CSV_CK(cudaStreamSynchronize(c->copy), "copy stream");
+    CSV_CK(c->stage[buf].ensure(at + n + 16), "device memory for a staged chunk");
+  }
+  if (n) CSV_CK(cudaMemcpyAsync(c->stage[buf].p + at, h_src, n, cudaMemcpyHostToDevice, c->copy), "staging copy");
+  CSV_CK(cudaEventRecord(c->staged[buf], c->copy), "staging copy");
+  *d_buf = c->stage[buf].p;
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_csv_stage_wait(warpjq_csv *c, uint32_t buf, char *err, size_t err_len) {
+  if (!c || buf > 1) return WARPJQ_ERR_INVALID_ARG;
+  if (c->staged[buf]) CSV_CK(cudaEventSynchronize(c->staged[buf]), "staging copy");
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_csv_carry(warpjq_csv *c, const uint8_t *d_src, uint64_t n, uint32_t buf, uint64_t at,
+                               void *stream, char *err, size_t err_len) {
+  if (!c || buf > 1 || (!d_src && n) || at + n + 16 > c->stage[buf].n) {
+    csv_err(err, err_len, "invalid argument");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  if (n)
+    CSV_CK(cudaMemcpyAsync(c->stage[buf].p + at, d_src, n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream),
+           "carried row copy");
   return WARPJQ_OK;
 }
 

@@ -45,6 +45,9 @@
 #pragma weak warpjq_csv_reset
 #pragma weak warpjq_csv_convert
 #pragma weak warpjq_csv_gather
+#pragma weak warpjq_csv_stage
+#pragma weak warpjq_csv_stage_wait
+#pragma weak warpjq_csv_carry
 #pragma weak warpjq_device_read
 #include "query.h"
 
@@ -434,10 +437,11 @@ struct warpjq_query {
   std::vector<uint64_t> rcaps;
   bool rpinned = false;
   std::unique_ptr<ReadPool> pool;
-  // CSV input: the converter and a page-locked staging buffer
+  // CSV input: the converter and, for input that is not page-locked, two
+  // page-locked buffers its chunks are copied through
   warpjq_csv *csv = nullptr;
-  uint8_t *csv_stage = nullptr;
-  uint64_t csv_stage_cap = 0;
+  uint8_t *csv_pin[2] = {nullptr, nullptr};
+  uint64_t csv_pin_cap[2] = {0, 0};
   void free_read_bufs() {
     for (auto &b : rbufs) {
       if (!b) continue;
@@ -449,7 +453,8 @@ struct warpjq_query {
   }
   ~warpjq_query() {
     free_read_bufs();
-    if (csv_stage) warpjq_host_free_pinned(csv_stage);
+    for (auto &b : csv_pin)
+      if (b) warpjq_host_free_pinned(b);
     if (csv) warpjq_csv_destroy(csv);
   }
 };
@@ -934,7 +939,8 @@ int warpjq_query_run_csv(warpjq_query *q, const uint8_t *data, size_t len, uint3
     put_err(err, err_len, m);
     return 1;
   };
-  if (!warpjq_csv_convert || !warpjq_launch_device || !warpjq_collect_device || !warpjq_host_alloc_pinned)
+  if (!warpjq_csv_convert || !warpjq_csv_stage || !warpjq_csv_carry || !warpjq_launch_device ||
+      !warpjq_collect_device || !warpjq_host_alloc_pinned)
     return fail("this device backend has no CSV input");
   if (!q->ctx) return fail("the query has no device context");
   if (!q->csv && warpjq_csv_create(&q->csv) != WARPJQ_OK) return fail("out of memory for the CSV converter");
@@ -952,30 +958,51 @@ int warpjq_query_run_csv(warpjq_query *q, const uint8_t *data, size_t len, uint3
   std::vector<uint64_t> k_off;
   std::vector<uint32_t> k_len;
   std::vector<uint8_t> k_bytes, rows;
-  uint64_t pos = 0;
-  for (;;) {
-    const uint64_t n = std::min<uint64_t>(cap, len - pos);
-    const bool final_ = pos + n == len;
-    const uint8_t *src = data + pos;
-    if (!pinned && n) {
-      if (q->csv_stage_cap < n) {
-        if (q->csv_stage) warpjq_host_free_pinned(q->csv_stage);
-        q->csv_stage = (uint8_t *)warpjq_host_alloc_pinned(n);
-        q->csv_stage_cap = q->csv_stage ? n : 0;
-        if (!q->csv_stage) return fail("out of page-locked host memory for the CSV input");
-      }
-      copy_to_pinned(q->csv_stage, src, n);
-      src = q->csv_stage;
+  // Chunk k on the device: the row carried over from chunk k - 1 (`carry`
+  // bytes just below offset `room` of its staging buffer), then its new
+  // bytes from `room` on.  Chunk k + 1's new bytes are copied to the other
+  // staging buffer while chunk k is converted and scanned.
+  uint64_t room = 64 << 10;
+  auto host_bytes = [&](uint32_t x, uint64_t hpos, uint64_t n, const uint8_t **src) -> bool {
+    if (pinned || !n) {
+      *src = data + hpos;
+      return true;
     }
+    if (q->csv_pin_cap[x] < n) {
+      if (q->csv_pin[x]) warpjq_host_free_pinned(q->csv_pin[x]);
+      const uint64_t want = std::max<uint64_t>(n, cap);
+      q->csv_pin[x] = (uint8_t *)warpjq_host_alloc_pinned(want);
+      q->csv_pin_cap[x] = q->csv_pin[x] ? want : 0;
+      if (!q->csv_pin[x]) return false;
+    }
+    copy_to_pinned(q->csv_pin[x], data + hpos, n);
+    *src = q->csv_pin[x];
+    return true;
+  };
+  uint8_t *dbuf[2] = {nullptr, nullptr};
+  auto stage = [&](uint32_t x, uint64_t at, uint64_t hpos, uint64_t n) -> int {
+    const uint8_t *hs = nullptr;
+    if (!host_bytes(x, hpos, n, &hs)) return fail("out of page-locked host memory for the CSV input");
+    if (warpjq_csv_stage(q->csv, x, at, hs, n, &dbuf[x], e, sizeof e) != WARPJQ_OK)
+      return fail(std::string("CUDA error in copying CSV to the device: ") + e);
+    return 0;
+  };
+  uint64_t pos = 0, carry = 0, n_new = std::min<uint64_t>(cap, len);
+  uint32_t b = 0;
+  if (len && stage(0, room, 0, n_new)) return 1;
+  while (len) {
+    const uint64_t next = pos + n_new;
+    const bool final_ = next == len;
+    const uint64_t n_next = final_ ? 0 : std::min<uint64_t>(cap, len - next);
+    if (!final_ && stage(b ^ 1, room, next, n_next)) return 1;
+    const uint8_t *src = dbuf[b] + room - carry;
+    const uint64_t n = carry + n_new;
     const uint8_t *d_nd = nullptr;
     uint64_t nd_len = 0, used = 0, recs = 0;
-    if (warpjq_csv_convert(q->csv, src, n, WARPJQ_CSV_HOST_INPUT | (final_ ? WARPJQ_CSV_FINAL : 0u), nullptr,
-                           &d_nd, &nd_len, &used, &recs, e, sizeof e) != WARPJQ_OK)
+    if (warpjq_csv_convert(q->csv, src, n,
+                           (final_ ? WARPJQ_CSV_FINAL : 0u) | (b ? WARPJQ_CSV_AFTER_STAGE1 : WARPJQ_CSV_AFTER_STAGE0),
+                           nullptr, &d_nd, &nd_len, &used, &recs, e, sizeof e) != WARPJQ_OK)
       return fail(std::string("CUDA error in converting CSV: ") + e);
-    if (!final_ && used == 0) {  // one row longer than a chunk
-      cap *= 2;
-      continue;
-    }
     if (nd_len && !q->tiled && warpjq_autotile) {  // tiles shaped by the converted lines
       std::vector<uint8_t> sample((size_t)std::min<uint64_t>(nd_len, 1 << 20));
       if (warpjq_device_read(sample.data(), d_nd, sample.size(), nullptr, e, sizeof e) != WARPJQ_OK ||
@@ -1031,8 +1058,22 @@ int warpjq_query_run_csv(warpjq_query *q, const uint8_t *data, size_t len, uint3
       }
     }
     records += recs;
-    pos += used;
     if (final_) break;
+    // the unconsumed end (a row that continues) goes in front of chunk k + 1
+    const uint64_t tail = n - used;
+    if (tail + 16 <= room) {
+      if (warpjq_csv_carry(q->csv, src + used, tail, b ^ 1, room - tail, nullptr, e, sizeof e) != WARPJQ_OK)
+        return fail(std::string("CUDA error in carrying a CSV row: ") + e);
+    } else {  // longer than the room before a chunk: stage it again, from the host
+      while (room < tail + 16) room *= 2;
+      if (warpjq_csv_stage_wait && warpjq_csv_stage_wait(q->csv, b ^ 1, e, sizeof e) != WARPJQ_OK)
+        return fail(std::string("CUDA error in copying CSV to the device: ") + e);
+      if (stage(b ^ 1, room - tail, next - tail, tail + n_next)) return 1;
+    }
+    carry = tail;
+    pos = next;
+    n_new = n_next;
+    b ^= 1;
   }
   if (P.is_aggregate()) {
     if (!P.has_group) {
