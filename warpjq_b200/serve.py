@@ -177,9 +177,18 @@ class Server:
         return finished
 
     def drain(self) -> list:
+        """Polls until every submitted request is done; when a turn neither
+        completes nor admits anything, it waits on the oldest busy slot's
+        event instead of spinning."""
         out = []
         while self.pending():
-            out += self.poll()
+            waiting = len(self.waiting)
+            got = self.poll()
+            out += got
+            if not got and len(self.waiting) == waiting:
+                busy = [s for s in self.slots if s.busy()]
+                if busy:
+                    busy[0].event.synchronize()
         return out
 
     def close(self):
