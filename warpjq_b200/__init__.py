@@ -296,10 +296,6 @@ class Query:
     def is_grouped(self) -> bool:
         return bool(self._h.warpjq_query_is_grouped(self._q))
 
-    @property
-    def is_aggregate(self) -> bool:
-        return bool(self._h.warpjq_query_is_aggregate(self._q))
-
     def run(self, data, on_invalid: str = "skip", max_line_bytes: int = 0,
             copy_out: bool = True) -> RunResult:
         """Runs over host memory: `data` is bytes, or a numpy uint8 array.
@@ -432,9 +428,10 @@ class Query:
         or keys gathered from the device)."""
         import numpy as np
         n = len(items)
+        # the collected array itself when `items` views it (the usual case),
+        # else a contiguous copy
         arr = getattr(self, "_b_items", None)
-        if arr is None or len(arr) < n or any(ctypes.addressof(a) != ctypes.addressof(b)
-                                              for a, b in zip(items[:1], arr[:1])):
+        if arr is None or len(arr) < n or (n and ctypes.addressof(items[0]) != ctypes.addressof(arr[0])):
             arr = (BatchItem * max(1, n))(*items)
         rows_p = row_off_p = None
         keep = []
