@@ -161,6 +161,21 @@ warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const 
                                   const uint64_t *lengths, uint32_t n_inputs, void *stream,
                                   char *err, size_t err_len);
 
+/* A mixed batch: like warpjq_batch_launch, but input i runs the query of
+ * input_ctx[i], so inputs with different queries share one launch of the
+ * persistent scan kernel (each tile takes its input's plan from device
+ * memory).  Aggregate queries only (count, sum, min, max, avg, group_by,
+ * with or without select): every input_ctx[i], and `ctx`, must hold one;
+ * WARPJQ_ERR_INVALID_ARG otherwise.  `ctx` supplies the buffers, tiling and
+ * stream order, and is collected with warpjq_batch_collect; each item's
+ * aggregate and groups are then rendered by its own query (its host
+ * formatter knows the aggregate kind).  The input contexts are only read
+ * during this call.  No reference counterpart. */
+warpjq_status warpjq_batch_launch_mixed(warpjq_ctx *ctx, warpjq_ctx *const *input_ctx,
+                                        const uint8_t *d_data, const uint64_t *offsets,
+                                        const uint64_t *lengths, uint32_t n_inputs, void *stream,
+                                        char *err, size_t err_len);
+
 /* Waits for the batch (repeating it once with larger buffers if one
  * overflowed) and fills items[0 .. n_inputs).  `all` (may be null) describes
  * the whole batch: its rows in input order in device memory (d_out_bytes,

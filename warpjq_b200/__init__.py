@@ -39,6 +39,7 @@ EXT_SYMBOLS = [
     "warpjq_host_free_pinned", "warpjq_csv_create", "warpjq_csv_destroy", "warpjq_csv_reset",
     "warpjq_csv_convert", "warpjq_csv_gather", "warpjq_device_read", "warpjq_batch_graph_create",
     "warpjq_batch_graph_launch", "warpjq_batch_graph_destroy", "warpjq_set_group_capacity",
+    "warpjq_batch_launch_mixed",
 ]
 HOST_SYMBOLS = [
     "warpjq_query_open", "warpjq_query_close", "warpjq_query_ctx", "warpjq_query_is_aggregate",
@@ -87,6 +88,9 @@ def _load():
     k.warpjq_autotile.restype = ctypes.c_int
     k.warpjq_batch_launch.argtypes = [vp, vp, ctypes.POINTER(u64), ctypes.POINTER(u64), u32, vp, cp, sz]
     k.warpjq_batch_launch.restype = ctypes.c_int
+    k.warpjq_batch_launch_mixed.argtypes = [vp, ctypes.POINTER(vp), vp, ctypes.POINTER(u64), ctypes.POINTER(u64),
+                                            u32, vp, cp, sz]
+    k.warpjq_batch_launch_mixed.restype = ctypes.c_int
     k.warpjq_batch_collect.argtypes = [vp, vp, vp, cp, sz]
     k.warpjq_batch_collect.restype = ctypes.c_int
     h.warpjq_query_open.argtypes = [cp, u32, u64, ctypes.POINTER(vp), cp, sz]
@@ -406,6 +410,23 @@ class Query:
         if rc:
             raise RuntimeError(err.value.decode(errors="replace"))
 
+    def batch_launch_mixed(self, queries, d_ptr: int, offsets, lengths, stream: int = 0):
+        """Enqueues one mixed batch on this (aggregate) query's context:
+        input i is d_ptr[offsets[i], + lengths[i]) and runs queries[i] (all
+        aggregate queries; each tile takes its input's plan).  Collect with
+        batch_collect() and render with batch_outputs_mixed()."""
+        k, _ = _load()
+        n = len(offsets)
+        self._b_off = (ctypes.c_uint64 * max(1, n))(*offsets)
+        self._b_len = (ctypes.c_uint64 * max(1, n))(*lengths)
+        ctxs = (ctypes.c_void_p * max(1, n))(*[q.ctx for q in queries])
+        self._b_n = n
+        err = ctypes.create_string_buffer(1024)
+        rc = k.warpjq_batch_launch_mixed(self.ctx, ctxs, ctypes.c_void_p(d_ptr), self._b_off, self._b_len, n,
+                                         ctypes.c_void_p(stream), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+
     def batch_collect(self):
         """(items, all): one BatchItem per input, and the batch's
         DeviceResult (rows and groups of every input)."""
@@ -472,6 +493,22 @@ class Query:
         self._h.warpjq_query_render_device(self._q, ctypes.byref(r), addr, ctypes.byref(out),
                                            ctypes.byref(n))
         return _take(out, n)
+
+
+def batch_outputs_mixed(queries, items, all_, host_data) -> list:
+    """Each input's output of a collected mixed batch, rendered by its own
+    query (queries[i] for input i); `host_data` holds the bytes the groups'
+    key_off values index, as for Query.batch_outputs."""
+    out = [b""] * len(items)
+    by_q = {}
+    for i, q in enumerate(queries):
+        by_q.setdefault(id(q), (q, []))[1].append(i)
+    for q, idx in by_q.values():
+        sub = [items[i] for i in idx]
+        q._b_items = None  # render from a contiguous copy of this query's items
+        for i, o in zip(idx, q.batch_outputs(sub, all_, host_data)):
+            out[i] = o
+    return out
 
 
 class BatchGraph:

@@ -81,6 +81,9 @@ struct RunBufs {
   DevBuf<uint32_t> b_tile_input;
   DevBuf<unsigned long long> b_in_start, b_in_end, b_in_tile0;
   DevBuf<RunCounters> b_in_ctr;
+  // mixed batches: the inputs' distinct plans and each input's plan index
+  DevBuf<DevPlan> b_plans;
+  DevBuf<uint32_t> b_in_plan;
   DevBuf<uint8_t> recs;
   DevBuf<uint8_t> out;
   DevBuf<unsigned long long> row_off, line_idx;
@@ -105,6 +108,8 @@ struct RunBufs {
     ctr.release(); tiles.release(); row_tiles.release(); row_bsum.release();
     b_tile_input.release(); b_in_start.release(); b_in_end.release(); b_in_tile0.release();
     b_in_ctr.release();
+    b_plans.release();
+    b_in_plan.release();
     recs.release(); out.release(); row_off.release(); line_idx.release(); tile_fsum.release();
     block_f.release(); block_lines.release(); deep.release(); g_slots.release();
     g_keys.release(); g_acc.release();
@@ -193,6 +198,10 @@ struct warpjq_ctx {
   struct Batch {
     bool active = false;
     bool tables_on_device = false;  // enqueue without uploading the tables (graph capture)
+    // a mixed batch: input i runs plans[in_plan[i]] (aggregate plans only)
+    bool mixed = false, any_grouped = false;
+    std::vector<DevPlan> plans;
+    std::vector<uint32_t> in_plan;
     uint64_t epoch = 0;             // bumped whenever a plain batch replaces the device tables
     const uint8_t *d_data = nullptr;
     cudaStream_t stream = nullptr;
@@ -227,6 +236,8 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
      "cudaFuncSetAttribute(scan rows)");
   CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan agg)");
+  CK(cudaFuncSetAttribute(k_scan<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
+     "cudaFuncSetAttribute(scan mixed)");
   int a = 0, b = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_scan<true>, kThreads, c->scan_smem),
      "occupancy");
@@ -239,7 +250,8 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
 
 // Sizes the buffers of `s` for an input of n bytes (first use, or growth).
 warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
-                          unsigned long long n_tiles, cudaStream_t st, bool cap, char *err, size_t err_len) {
+                          unsigned long long n_tiles, cudaStream_t st, bool cap, char *err, size_t err_len,
+                          bool grouped) {
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
   if (n_tiles == 0) n_tiles = 1;
@@ -265,7 +277,7 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
     CK(rb.row_off.ensure(rb.rows_cap + 1, st, cap), "alloc row offsets");
     CK(rb.line_idx.ensure(rb.rows_cap, st, cap), "alloc line index");
   }
-  if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
+  if (grouped) {
     if (!rb.g_cap) {
       rb.g_key_cap = c->group_keys0;
       rb.g_cap = 2 * c->group_keys0;
@@ -275,6 +287,13 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
     CK(rb.g_acc.ensure(rb.g_key_cap, st, cap), "alloc group accumulators");
   }
   return WARPJQ_OK;
+}
+
+// Whether a run keeps a group table: the context's plan groups, or (a mixed
+// batch) one of the inputs' plans does.
+bool run_grouped(const warpjq_ctx *c, const warpjq_ctx::Batch *b) {
+  if (b && b->mixed) return b->any_grouped;
+  return c->plan.output_kind == WARPJQ_OUT_AGG && c->plan.group_slot >= 0;
 }
 
 GroupTable group_view(RunBufs &rb, bool on) {
@@ -298,11 +317,11 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(st, &cap), "capture status");
   const bool capturing = cap != cudaStreamCaptureStatusNone;
-  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, st, capturing, err, err_len);
+  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, st, capturing, err, err_len, run_grouped(c, b));
   if (rc != WARPJQ_OK) return rc;
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
-  bool groups = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
+  const bool groups = run_grouped(c, b);
   const uint32_t n_inputs = b ? (uint32_t)b->start.size() : 0;
   if (b && !b->tables_on_device) {
     CK(rb.b_in_start.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch tables");
@@ -310,6 +329,16 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     CK(rb.b_in_tile0.ensure(n_inputs + 1, st, capturing), "alloc batch tables");
     CK(rb.b_in_ctr.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch tables");
     CK(rb.b_tile_input.ensure(std::max<unsigned long long>(n_tiles, 1), st, capturing), "alloc batch tables");
+    if (b->mixed) {
+      CK(rb.b_plans.ensure(b->plans.size(), st, capturing), "alloc batch plans");
+      CK(rb.b_in_plan.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch plans");
+      CK(cudaMemcpyAsync(rb.b_plans.p, b->plans.data(), b->plans.size() * sizeof(DevPlan), cudaMemcpyHostToDevice,
+                         st),
+         "H2D batch plans");
+      if (n_inputs)
+        CK(cudaMemcpyAsync(rb.b_in_plan.p, b->in_plan.data(), n_inputs * 4ull, cudaMemcpyHostToDevice, st),
+           "H2D batch plans");
+    }
     // pageable sources: staged by the driver before the calls return
     CK(cudaMemcpyAsync(rb.b_in_start.p, b->start.data(), n_inputs * 8ull, cudaMemcpyHostToDevice, st),
        "H2D batch tables");
@@ -345,6 +374,11 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.g = g;
     sp.deep_words = rb.deep.p;
     sp.deep_levels_per_cta = rb.deep_levels;
+    if (b && b->mixed) {
+      sp.plans = rb.b_plans.p;
+      sp.in_plan = rb.b_in_plan.p;
+      sp.any_grouped = b->any_grouped ? 1u : 0u;
+    }
     if (b) {
       sp.tile_input = rb.b_tile_input.p;
       sp.in_start = rb.b_in_start.p;
@@ -359,7 +393,10 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     }
     s.timed = !capturing;  // a captured sequence is not timed
     if (s.timed) CK(cudaEventRecord(s.scan_t0, st), "event record");
-    if (P.needs_rows)
+    if (b && b->mixed)  // the inputs' plans may group where the context's does not
+      k_scan<false, true><<<grid, kThreads, scan_smem_bytes(c->tile_bytes, c->halo_bytes, b->any_grouped), st>>>(
+          sp, c->plan);
+    else if (P.needs_rows)
       k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     else
       k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
@@ -599,7 +636,7 @@ warpjq_status warpjq_ctx_create(const warpjq_program *prog, uint64_t max_chunk_b
     CK(cudaHostAlloc((void **)&s.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
     if (max_chunk_bytes) {
       rc = ensure_bufs(c.get(), s, max_chunk_bytes, (max_chunk_bytes + c->tile_bytes - 1) / c->tile_bytes,
-                       s.stream, false, err, err_len);
+                       s.stream, false, err, err_len, run_grouped(c.get(), nullptr));
       if (rc != WARPJQ_OK) return rc;
       CK(cudaStreamSynchronize(s.stream), "stream sync");
     }
@@ -993,9 +1030,11 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
   return WARPJQ_OK;
 }
 
-warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const uint64_t *offsets,
-                                  const uint64_t *lengths, uint32_t n_inputs, void *stream,
-                                  char *err, size_t err_len) {
+// The batch tables of warpjq_batch_launch(_mixed); the batch is left
+// inactive until enqueued.
+static warpjq_status batch_prepare(warpjq_ctx *ctx, const uint8_t *d_data, const uint64_t *offsets,
+                                   const uint64_t *lengths, uint32_t n_inputs, void *stream, char *err,
+                                   size_t err_len) {
   // d_data may be null: offsets are then device addresses, and the inputs
   // may lie in different allocations.
   if (!ctx || (n_inputs && (!offsets || !lengths))) return WARPJQ_ERR_INVALID_ARG;
@@ -1026,7 +1065,55 @@ warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const 
   }
   b.tile0[n_inputs] = tiles;
   b.n_tiles = tiles;
-  warpjq_status rc = enqueue_run(ctx, ctx->dev, d_data, b.total, b.stream, err, err_len, &b);
+  b.mixed = b.any_grouped = false;
+  b.plans.clear();
+  b.in_plan.clear();
+  return WARPJQ_OK;
+}
+
+warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const uint64_t *offsets,
+                                  const uint64_t *lengths, uint32_t n_inputs, void *stream,
+                                  char *err, size_t err_len) {
+  warpjq_status rc = batch_prepare(ctx, d_data, offsets, lengths, n_inputs, stream, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  warpjq_ctx::Batch &b = ctx->batch;
+  rc = enqueue_run(ctx, ctx->dev, d_data, b.total, b.stream, err, err_len, &b);
+  if (rc == WARPJQ_OK) b.active = true;
+  return rc;
+}
+
+warpjq_status warpjq_batch_launch_mixed(warpjq_ctx *ctx, warpjq_ctx *const *input_ctx, const uint8_t *d_data,
+                                        const uint64_t *offsets, const uint64_t *lengths, uint32_t n_inputs,
+                                        void *stream, char *err, size_t err_len) {
+  if (!ctx || (n_inputs && !input_ctx)) return WARPJQ_ERR_INVALID_ARG;
+  if (ctx->plan.output_kind != WARPJQ_OUT_AGG) {
+    set_err(err, err_len, "a mixed batch runs on an aggregate query's context");
+    return WARPJQ_ERR_INVALID_ARG;
+  }
+  std::vector<const warpjq_ctx *> distinct;
+  std::vector<uint32_t> in_plan(n_inputs);
+  for (uint32_t i = 0; i < n_inputs; i++) {
+    const warpjq_ctx *q = input_ctx[i];
+    if (!q || q->plan.output_kind != WARPJQ_OUT_AGG) {
+      set_err(err, err_len, "input %u of a mixed batch does not have an aggregate query", i);
+      return WARPJQ_ERR_INVALID_ARG;
+    }
+    uint32_t k = 0;
+    while (k < distinct.size() && distinct[k] != q) k++;
+    if (k == distinct.size()) distinct.push_back(q);
+    in_plan[i] = k;
+  }
+  warpjq_status rc = batch_prepare(ctx, d_data, offsets, lengths, n_inputs, stream, err, err_len);
+  if (rc != WARPJQ_OK) return rc;
+  warpjq_ctx::Batch &b = ctx->batch;
+  b.mixed = true;
+  for (const warpjq_ctx *q : distinct) {
+    b.plans.push_back(q->plan);
+    b.any_grouped = b.any_grouped || q->plan.group_slot >= 0;
+  }
+  if (b.plans.empty()) b.plans.push_back(ctx->plan);
+  b.in_plan = std::move(in_plan);
+  rc = enqueue_run(ctx, ctx->dev, d_data, b.total, b.stream, err, err_len, &b);
   if (rc == WARPJQ_OK) b.active = true;
   return rc;
 }
@@ -1046,7 +1133,7 @@ warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
     CK(cudaMemcpy(b.h_ctr.data(), s.rb.b_in_ctr.p, n * sizeof(RunCounters), cudaMemcpyDeviceToHost),
        "D2H batch counters");
   const DevPlan &P = ctx->plan;
-  const bool grouped = P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0;
+  const bool grouped = run_grouped(ctx, &b);
   // Groups ordered by input (stable within an input).
   std::vector<uint32_t> first(n + 1, 0);
   if (grouped) {

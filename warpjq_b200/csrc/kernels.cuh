@@ -132,6 +132,11 @@ struct ScanParams {
   const unsigned long long *in_end;
   const unsigned long long *in_tile0;
   RunCounters *in_ctr;
+  // Mixed batches (k_scan<false, true>): input i runs plans[in_plan[i]];
+  // any_grouped when one of them groups.
+  const DevPlan *plans;
+  const uint32_t *in_plan;
+  uint32_t any_grouped;
 };
 
 // Rows emission.
@@ -580,7 +585,9 @@ __device__ __forceinline__ uint32_t chunk_newlines(const uint8_t *win, uint32_t 
 
 // The plan is a kernel parameter (constant bank): fields at fixed offsets
 // are instruction operands, and no plan read goes through global memory.
-template <bool kRows>
+// kMulti (aggregates only): a mixed batch, each input with its own plan,
+// taken per tile from sp.plans in device memory instead of `plan`.
+template <bool kRows, bool kMulti = false>
 __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -612,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
-  const bool grouped = !kRows && P.group_slot >= 0;
+  const bool grouped = !kRows && (kMulti ? sp.any_grouped != 0 : P.group_slot >= 0);
   if (grouped) {
     for (int k = lane; k < kGroupCache; k += 32) {
       gcache->tag[k] = 0xFFFFFFFFu;
@@ -646,6 +653,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
       ts = data_start + (tile - sp.in_tile0[input]) * T;
       ctr_in = sp.in_ctr + input;
     }
+    // The tile's plan (a mixed batch: its input's own).
+    const DevPlan &P = kMulti ? sp.plans[sp.in_plan[input]] : plan;
     const unsigned long long te = min(ts + T, data_end);
     const uint32_t tlen = (uint32_t)(te - ts);
     const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, data_end - ts);
