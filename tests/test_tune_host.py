@@ -13,6 +13,8 @@ def test_shape_key_groups_line_lengths_by_power_of_two():
     c = tune.shape_key("B200", "count", b"z" * 99 + b"\n")
     assert a == b != c
     assert tune.shape_key("B200", "sum(.a)", b"x\n") != tune.shape_key("B200", "count", b"x\n")
+    assert tune.shape_key("B200", "count", b"x\n", "1-2") != tune.shape_key("B200", "count", b"x\n", "1-3")
+    assert tune.library_id() != "unbuilt"  # the tests run against a built library
 
 
 def test_cache_round_trip_and_damage(tmp_path):

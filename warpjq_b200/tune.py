@@ -12,9 +12,10 @@ Swept, each timed with CUDA events around the device-resident run (best of
 Lines per round are fixed at 32 by the design (one line per lane), so they
 are not swept.
 
-The cache is a JSON file keyed by device name, query and the sample's mean
-line length (rounded to a power of two), so inputs of the same shape reuse
-a choice without measuring again.  warpjq_autotile's analytic choice is
+The cache is a JSON file keyed by device name, the device library's build,
+query and the sample's mean line length (rounded to a power of two), so
+inputs of the same shape reuse a choice without measuring again, and a
+rebuilt library measures afresh.  warpjq_autotile's analytic choice is
 always one of the candidates, so a tuned choice is never slower on the
 sample than the default.
 """
@@ -36,10 +37,21 @@ def default_cache_path() -> str:
     return os.path.join(base, "warpjq_b200", "tune.json")
 
 
-def shape_key(device: str, query: str, sample: bytes) -> str:
+def library_id() -> str:
+    """Identity of the built device library (size and modification time):
+    a rebuilt kernel may want other tiles, so its choices are kept apart."""
+    from . import KERNELS_SO
+    try:
+        st = os.stat(KERNELS_SO)
+        return f"{st.st_size}-{int(st.st_mtime)}"
+    except OSError:
+        return "unbuilt"
+
+
+def shape_key(device: str, query: str, sample: bytes, library: str = "") -> str:
     lines = sample.count(b"\n")
     mean = len(sample) / max(1, lines)
-    return f"{device}|{query}|{2 ** round(math.log2(max(1.0, mean)))}"
+    return f"{device}|{library}|{query}|{2 ** round(math.log2(max(1.0, mean)))}"
 
 
 def load_cache(path: str) -> dict:
@@ -82,7 +94,7 @@ def tune(query: str, d_ptr: int, n: int, sample: bytes, reps: int = 3, cache_pat
     first bytes, for the halo rule and the cache key).  Returns
     {"tile": T, "halo": H, "group_keys": K or None, "gbs": rate, "from_cache": bool}."""
     cache_path = cache_path or default_cache_path()
-    key = shape_key(device_name(), query, sample[: 1 << 20])
+    key = shape_key(device_name(), query, sample[: 1 << 20], library_id())
     cache = load_cache(cache_path) if use_cache else {}
     if use_cache and key in cache:
         return dict(cache[key], from_cache=True)
