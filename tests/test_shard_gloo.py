@@ -142,3 +142,67 @@ def test_two_gloo_ranks_merge_to_the_single_input_result():
                 got = f.read()
             want = orc.run(q, data).out
             assert got == want, (q, got[:200], want[:200])
+
+
+def make_csv() -> bytes:
+    """The nginx records as CSV, with quoted newlines and doubled quotes put
+    into some ua fields, so cuts must find row ends outside quotes."""
+    buf, used, _ = wjq.gen_nginx_csv(1 << 20, seed=9)
+    rows = bytes(buf[:used]).split(b"\n")[:-1]
+    out = [rows[0]]
+    for i, r in enumerate(rows[1:]):
+        if i % 7 == 3:
+            r = r.replace(b',"', b',"line one\nline "" two\n', 1)
+        out.append(r)
+    return b"\n".join(out) + b"\n"
+
+
+def test_csv_shard_bounds_cut_at_row_ends():
+    from oracle import csv_map
+    from tests.test_csv_gpu import fuzz_csv
+    for data in [make_csv(), fuzz_csv(3, 2000, crlf=True, bom=True), fuzz_csv(4, 500),
+                 b"k\n" + b'"' + b"x\n" * 5000 + b'"\n1\n']:
+        whole = csv_map.csv_to_ndjson(data).split(b"\n")[:-1]
+        for world in (1, 2, 3, 5):
+            h_end, b = shard.csv_shard_bounds(data, world)
+            assert b[0][0] == h_end and b[-1][1] == len(data) and len(b) == world
+            parts = []
+            for (a0, a1), nxt in zip(b, b[1:] + [(len(data), len(data))]):
+                assert a1 == nxt[0]
+                assert data[:a1].count(b'"') % 2 == 0  # each cut is outside quotes
+                parts += csv_map.csv_to_ndjson(data[:h_end] + data[a0:a1]).split(b"\n")[:-1]
+            assert parts == whole, world
+
+
+def _rank_main_csv(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from oracle import csv_map
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        data = make_csv()
+        h_end, bounds = shard.csv_shard_bounds(data, world)
+        lo, hi = bounds[rank]
+        mine = csv_map.csv_to_ndjson(data[:h_end] + data[lo:hi])
+        for i, q in enumerate(ROW_QUERIES + list(AGG_QUERIES)):
+            parts = shard.gather(cpu_partial(q, mine), rank, world)
+            if rank == 0:
+                with open(os.path.join(out_dir, f"{i}.out"), "wb") as f:
+                    f.write(shard.render(q, shard.merge(parts)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_merge_csv_shards_to_the_single_input_result():
+    from oracle import csv_map
+    world = 2
+    with tempfile.TemporaryDirectory() as out_dir:
+        mp.start_processes(_rank_main_csv, args=(world, _free_port(), out_dir), nprocs=world,
+                           start_method="spawn", join=True)
+        nd = csv_map.csv_to_ndjson(make_csv())
+        for i, q in enumerate(ROW_QUERIES + list(AGG_QUERIES)):
+            with open(os.path.join(out_dir, f"{i}.out"), "rb") as f:
+                got = f.read()
+            want = orc.run(q, nd).out
+            assert got == want, (q, got[:200], want[:200])

@@ -35,3 +35,19 @@ def test_hostile_corpus_groups_merge_by_decoded_key(golden):
     for q in ["group_by(.host) | count", "group_by(.msg) | count", "count"]:
         parts = [shard.device_partial(q, data[lo:hi]) for lo, hi in bounds]
         assert shard.render(q, shard.merge(parts)) == orc.run(q, data).out, q
+
+
+@pytest.mark.parametrize("world", [1, 3])
+def test_csv_device_partials_merge_to_the_whole_input_result(world):
+    """CSV cut for several ranks (shard.csv_shard_bounds): each range runs
+    behind a copy of the header, converted and scanned on the device, and the
+    merge renders what the oracle prints for the whole input's NDJSON."""
+    from oracle import csv_map
+    from tests.test_shard_gloo import make_csv
+    data = make_csv()
+    nd = csv_map.csv_to_ndjson(data)
+    h_end, bounds = shard.csv_shard_bounds(data, world)
+    for q in ["select(.status == 500) | count", "sum(.bytes)", "group_by(.host) | sum(.bytes)",
+              "group_by(.path) | count", "select(.status >= 500) | {p: .path, b: .bytes}", ".ua"]:
+        parts = [shard.csv_device_partial(q, data[:h_end], data[lo:hi]) for lo, hi in bounds]
+        assert shard.render(q, shard.merge(parts)) == orc.run(q, nd).out, q

@@ -47,6 +47,48 @@ def shard_bounds(data, world: int) -> List[Tuple[int, int]]:
     return list(zip(cuts[:-1], cuts[1:]))
 
 
+def csv_row_end(mv, pos: int, inside: bool) -> int:
+    """Offset just past the first row end at or after `pos` (a '\n' with an
+    even number of '"' before it in the input), given whether `pos` itself
+    lies inside quotes; len(mv) when none follows."""
+    n = len(mv)
+    while pos < n:
+        window = bytes(mv[pos:min(n, pos + (1 << 20))])
+        k = 0
+        while True:
+            q = window.find(b'"', k)
+            nl = window.find(b"\n", k)
+            if nl < 0 and q < 0:
+                break
+            if nl >= 0 and (q < 0 or nl < q):
+                if not inside:
+                    return pos + nl + 1
+                k = nl + 1
+            else:
+                inside = not inside
+                k = q + 1
+        pos += len(window)
+    return n
+
+
+def csv_shard_bounds(data, world: int) -> Tuple[int, List[Tuple[int, int]]]:
+    """CSV input cut for `world` ranks: (header end, [start, end) of each
+    rank's rows).  Cuts fall just after row ends (newlines outside quotes,
+    whose quote count from the input's start is even), so a quoted field's
+    newlines never split; every rank runs its rows behind a copy of the
+    header row [0, header end)."""
+    mv = memoryview(data).cast("B")
+    n = len(mv)
+    h_end = csv_row_end(mv, 0, False)
+    cuts = [h_end]
+    for r in range(1, world):
+        t = max(cuts[-1], h_end + (n - h_end) * r // world)
+        inside = bytes(mv[:t]).count(b'"') % 2 == 1
+        cuts.append(max(csv_row_end(mv, t, inside), cuts[-1]))
+    cuts.append(n)
+    return h_end, list(zip(cuts[:-1], cuts[1:]))
+
+
 def decode_key(kind: int, raw: bytes) -> bytes:
     """Group-key identity: string keys compare by their decoded bytes (escapes
     resolved, a lone surrogate becomes U+FFFD; json.rs:594-654), every
@@ -239,6 +281,53 @@ def device_partial(query: str, shard_host, fmt: str = "ndjson") -> Partial:
     part = partial_from_device(q.collect_device(), shard_np)
     q.close()
     return part
+
+
+def csv_device_partial(query: str, header: bytes, rows_host, fmt: str = "ndjson") -> Partial:
+    """One CSV range's partial: the header and the range's rows converted to
+    NDJSON on the current GPU, scanned there; group keys are gathered from
+    the converted bytes on the device."""
+    import numpy as np
+    import torch
+    from . import CsvConverter
+    src = bytes(header) + bytes(memoryview(rows_host).cast("B"))
+    dev = torch.zeros(len(src) + 16, dtype=torch.uint8, device="cuda")
+    if src:
+        dev[:len(src)].copy_(torch.frombuffer(bytearray(src), dtype=torch.uint8))
+    conv = CsvConverter()
+    stream = torch.cuda.current_stream().cuda_stream
+    d, nd, _, _ = conv.convert(dev.data_ptr(), len(src), stream=stream)
+    q = Query(query, fmt)
+    q.launch_device(d, nd, stream)
+    r = q.collect_device()
+    keys = np.zeros(1, dtype=np.uint8)
+    if r.n_groups:
+        g = np.ctypeslib.as_array(r.groups, shape=(r.n_groups,))
+        offs = np.ascontiguousarray(g["key_off"], dtype=np.uint64)
+        lens = np.ascontiguousarray(g["key_len"], dtype=np.uint32)
+        keys = np.zeros(int(lens.sum()) + 1, dtype=np.uint8)
+        conv.gather(d, offs, lens, r.n_groups, keys, stream)
+        at = np.zeros(r.n_groups, dtype=np.uint64)
+        np.cumsum(lens[:-1], out=at[1:])
+        g["key_off"] = at
+    part = partial_from_device(r, keys)
+    q.close()
+    conv.close()
+    return part
+
+
+def run_sharded_csv(query: str, host_data, rank: int, world: int, fmt: str = "ndjson",
+                    group=None) -> Optional[bytes]:
+    """run_sharded for CSV input: every rank converts its rows, behind the
+    header, on its own GPU."""
+    h_end, bounds = csv_shard_bounds(host_data, world)
+    mv = memoryview(host_data).cast("B")
+    lo, hi = bounds[rank]
+    part = csv_device_partial(query, bytes(mv[:h_end]), mv[lo:hi], fmt)
+    parts = gather(part, rank, world, group)
+    if rank != 0:
+        return None
+    return render(query, merge(parts), fmt)
 
 
 def run_sharded(query: str, host_data, rank: int, world: int, fmt: str = "ndjson",
