@@ -65,6 +65,8 @@ def matches(got, q, data, fmt):
 
 
 def test_each_result_is_the_same_alone_and_in_the_mix():
+    import warpjq_b200.serve as serve
+    serve.MIXED_MIN = 2  # exercise the mixed batches on these small slots too
     reqs = workload()
     srv = Server(QUERIES, n_slots=3)
     handles = []
@@ -84,6 +86,7 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
         assert r.out == h.out, (h.id, q)  # exact: an input's tiles and order do not depend on the mix
     alone.close()
     srv.close()
+    serve.MIXED_MIN = 16
 
 
 def test_device_resident_requests():

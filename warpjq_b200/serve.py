@@ -26,7 +26,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import CsvConverter, Query
+from . import CsvConverter, Query, batch_outputs_mixed
 
 
 @dataclass
@@ -47,6 +47,12 @@ class Request:
     @property
     def latency(self) -> float:
         return self.t_done - self.t_arrive
+
+
+# A slot's aggregate requests go into one mixed batch from this many on
+# (a few requests gain little from it, and a batch per query is the
+# faster kernel).
+MIXED_MIN = 16
 
 
 def footprint(nbytes: int, fmt: str) -> int:
@@ -76,6 +82,9 @@ class _Slot:
         import torch
         self.stream = torch.cuda.Stream()
         self.qs = {q: Query(q, fmt=fmt_out, chunk_bytes=chunk_bytes) for q in queries}
+        # runs a slot's aggregate requests of several queries as one mixed batch
+        self.driver = Query("count", fmt=fmt_out, chunk_bytes=chunk_bytes)
+        self.mixed: list = []  # (request, address, bytes) of the mixed batch in flight
         self.arena = torch.empty(0, dtype=torch.uint8, device="cuda")
         self.conv = CsvConverter()
         self.event = None
@@ -90,6 +99,7 @@ class _Slot:
     def close(self):
         for q in self.qs.values():
             q.close()
+        self.driver.close()
         self.conv.close()
 
 
@@ -101,11 +111,15 @@ class Server:
     every submitted request is done.  `budget_bytes` caps the device memory
     that admitted requests may hold at once (a request alone over the budget
     is refused with an error); `max_batch` caps the requests a slot takes
-    (1 with one slot serves requests one at a time)."""
+    (1 with one slot serves requests one at a time); with `mixed`, a slot's
+    aggregate requests of two or more queries, MIXED_MIN or more of them,
+    run as one mixed batch (one launch sequence and one collect, each input
+    with its own plan) instead of one batch per query."""
 
     def __init__(self, queries, n_slots: int = 3, budget_bytes: int = 120 << 30, fmt_out: str = "ndjson",
-                 chunk_bytes: int = 1 << 20, max_batch: int = 0):
+                 chunk_bytes: int = 1 << 20, max_batch: int = 0, mixed: bool = True):
         self.max_batch = max_batch  # requests per slot at most (0: no limit)
+        self.mixed = mixed          # a slot's aggregate requests of several queries in one launch
         self.queries = list(dict.fromkeys(queries))
         self.slots = [_Slot(self.queries, fmt_out, chunk_bytes) for _ in range(n_slots)]
         self.budget = budget_bytes
@@ -156,6 +170,12 @@ class Server:
                     Q.batch_launch(small.data_ptr(), [0], [len(line)], s.stream.cuda_stream)
                     items, all_ = Q.batch_collect()
                     Q.batch_outputs(items, all_, self._gather_keys(s, all_, base=small.data_ptr()))
+                # the mixed path: every aggregate query over the blank lines
+                aggs = [Q for Q in s.qs.values() if Q.is_aggregate]
+                if self.mixed and len(aggs) > 1:
+                    s.driver.batch_launch_mixed(aggs, buf.data_ptr(), [0] * len(aggs), [reserve_bytes] * len(aggs),
+                                                s.stream.cuda_stream)
+                    s.driver.batch_collect()
                 # the CSV kernels and the converter's buffers
                 s.conv.reset()
                 s.conv.convert(csv.data_ptr(), len(rows), stream=s.stream.cuda_stream)
@@ -248,6 +268,13 @@ class Server:
             by_q = {}
             for r, (addr, n) in zip(take, addrs):
                 by_q.setdefault(r.query, []).append((r, addr, n))
+            agg = [q for q in by_q if s.qs[q].is_aggregate]
+            s.mixed = []
+            if self.mixed and len(agg) > 1 and sum(len(by_q[q]) for q in agg) >= MIXED_MIN:
+                s.mixed = [x for q in agg for x in by_q.pop(q)]
+                s.driver.batch_launch_mixed([s.qs[r.query] for r, _, _ in s.mixed], 0,
+                                            [a for _, a, _ in s.mixed], [n for _, _, n in s.mixed],
+                                            s.stream.cuda_stream)
             for q, lst in by_q.items():
                 s.qs[q].batch_launch(0, [a for _, a, _ in lst], [n for _, _, n in lst], s.stream.cuda_stream)
             s.event = torch.cuda.Event()
@@ -272,6 +299,16 @@ class Server:
     def _complete(self, s: _Slot) -> list:
         done_at = time.perf_counter()
         out = []
+        if s.mixed:
+            items, all_ = s.driver.batch_collect()
+            keys = self._gather_keys(s, all_)
+            outs = batch_outputs_mixed([s.qs[r.query] for r, _, _ in s.mixed], items, all_, keys)
+            for (r, _, _), it, o in zip(s.mixed, items, outs):
+                r.out = o
+                r.n_lines = it.n_lines - it.n_blank
+                r.t_done = done_at
+                out.append(r)
+            s.mixed = []
         for q, lst in s.used_queries.items():
             Q = s.qs[q]
             items, all_ = Q.batch_collect()
