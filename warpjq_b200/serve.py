@@ -7,7 +7,9 @@ slot is free, it takes every waiting request that fits the device-memory
 budget, finds each one's NDJSON a 16-byte aligned device address (device
 inputs in place, CSV converted on the device, host inputs copied into the
 arena), and runs one batch per query among them (warpjq_batch_launch, by
-device address) on its stream, then returns to the loop: requests
+device address; from MIXED_MIN aggregate requests of two or more queries
+on, those go into one mixed batch, warpjq_batch_launch_mixed) on its
+stream, then returns to the loop: requests
 arriving meanwhile are admitted into the next free slot, so several slots'
 work overlaps on the device.  A finished slot is collected when its event
 has completed; each request's output is exactly what a run over its input
