@@ -276,7 +276,7 @@ typedef struct {
  * calls that overlap on the GPU race -- order them on one stream.  The first
  * call on each device does a one-time set-up (it looks up the array's device
  * address); make that first call before any stream capture.  Lines nesting
- * deeper than 65,600 levels exceed the fixed nesting stack and set status 1. */
+ * deeper than 16,448 levels exceed the fixed nesting stack and set status 1. */
 warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, const uint8_t *d_data,
                                        uint64_t n_bytes, void *stream,
                                        warpjq_noalloc_result *d_result, char *err, size_t err_len);

@@ -64,9 +64,9 @@ def matches(got, q, data, fmt):
     return got == want or ("avg(" in q and close_enough(got, want))
 
 
-def test_each_result_is_the_same_alone_and_in_the_mix():
+def test_each_result_is_the_same_alone_and_in_the_mix(monkeypatch):
     import warpjq_b200.serve as serve
-    serve.MIXED_MIN = 2  # exercise the mixed batches on these small slots too
+    monkeypatch.setattr(serve, "MIXED_MIN", 2)  # exercise the mixed batches on these small slots too
     reqs = workload()
     srv = Server(QUERIES, n_slots=3)
     handles = []
@@ -86,7 +86,6 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
         assert r.out == h.out, (h.id, q)  # exact: an input's tiles and order do not depend on the mix
     alone.close()
     srv.close()
-    serve.MIXED_MIN = 16
 
 
 def test_device_resident_requests():

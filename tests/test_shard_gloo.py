@@ -47,12 +47,25 @@ def make_data() -> bytes:
     return b"\n".join(out) + b"\n"
 
 
+def first_invalid(data: bytes):
+    """Index of the first physical line that is neither blank nor valid JSON
+    (the nginx-schema test data has no other kind of bad line)."""
+    for i, ln in enumerate(data.split(b"\n")[:-1]):
+        if ln.strip():
+            try:
+                json.loads(ln)
+            except ValueError:
+                return i
+    return None
+
+
 def cpu_partial(query: str, data: bytes) -> shard.Partial:
+    base = dict(n_lines=data.count(b"\n"), first_invalid=first_invalid(data))
     if query in ROW_QUERIES:
         r = orc.run(query, data)
-        return shard.Partial(rows=r.out)
+        return shard.Partial(rows=r.out, **base)
     flt, agg, grp = AGG_QUERIES[query]
-    p = shard.Partial()
+    p = shard.Partial(**base)
     groups = {}
     for ln in data.split(b"\n"):
         if not ln.strip():
@@ -88,19 +101,43 @@ def cpu_partial(query: str, data: bytes) -> shard.Partial:
     return p
 
 
+def make_data_late_bad() -> bytes:
+    """Valid lines, blank lines, and malformed lines only in the second half,
+    so with two ranks the first bad line lies in rank 1's range."""
+    buf, used, _ = wjq.gen_nginx(1 << 19, seed=5)
+    lines = bytes(buf[:used]).split(b"\n")[:-1]
+    out = []
+    for i, ln in enumerate(lines):
+        if i % 17 == 4:
+            out.append(b"")
+        if i > len(lines) * 3 // 4 and i % 29 == 11:
+            out.append(b'{"status":500,')
+        out.append(ln)
+    return b"\n".join(out) + b"\n"
+
+
 def _rank_main(rank, world, port, out_dir):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        data = make_data()
-        lo, hi = shard.shard_bounds(data, world)[rank]
-        for i, q in enumerate(ROW_QUERIES + list(AGG_QUERIES)):
-            parts = shard.gather(cpu_partial(q, data[lo:hi]), rank, world)
-            if rank == 0:
-                with open(os.path.join(out_dir, f"{i}.out"), "wb") as f:
-                    f.write(shard.render(q, shard.merge(parts)))
+        for tag, data in (("a", make_data()), ("b", make_data_late_bad())):
+            lo, hi = shard.shard_bounds(data, world)[rank]
+            for i, q in enumerate(ROW_QUERIES + list(AGG_QUERIES)):
+                part = cpu_partial(q, data[lo:hi])
+                if q in ROW_QUERIES and rank % 2:
+                    # rows handed over as a tensor, as a device-resident run does
+                    import torch
+                    part.rows = torch.frombuffer(bytearray(part.rows), dtype=torch.uint8) if part.rows \
+                        else torch.empty(0, dtype=torch.uint8)
+                parts = shard.gather(part, rank, world)
+                if rank == 0:
+                    m = shard.merge(parts)
+                    with open(os.path.join(out_dir, f"{tag}{i}.out"), "wb") as f:
+                        f.write(shard.render(q, m))
+                    with open(os.path.join(out_dir, f"{tag}{i}.json"), "w") as f:
+                        json.dump({"first_invalid": m.first_invalid, "n_lines": m.n_lines}, f)
     finally:
         dist.destroy_process_group()
 
@@ -131,17 +168,24 @@ def test_decoded_string_keys_merge_across_ranks():
     assert shard.decode_key(4, b"\\ud83d\\ude00\\ud800x") == "😀�x".encode()
 
 
-def test_two_gloo_ranks_merge_to_the_single_input_result():
-    world = 2
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_merge_to_the_single_input_result(world):
     with tempfile.TemporaryDirectory() as out_dir:
         mp.start_processes(_rank_main, args=(world, _free_port(), out_dir), nprocs=world,
                            start_method="spawn", join=True)
-        data = make_data()
-        for i, q in enumerate(ROW_QUERIES + list(AGG_QUERIES)):
-            with open(os.path.join(out_dir, f"{i}.out"), "rb") as f:
-                got = f.read()
-            want = orc.run(q, data).out
-            assert got == want, (q, got[:200], want[:200])
+        for tag, data in (("a", make_data()), ("b", make_data_late_bad())):
+            fi = first_invalid(data)
+            assert fi is not None
+            if tag == "b":  # the first bad line is past rank 0's range
+                assert fi >= data[:shard.shard_bounds(data, world)[0][1]].count(b"\n")
+            for i, q in enumerate(ROW_QUERIES + list(AGG_QUERIES)):
+                with open(os.path.join(out_dir, f"{tag}{i}.out"), "rb") as f:
+                    got = f.read()
+                want = orc.run(q, data).out
+                assert got == want, (tag, q, got[:200], want[:200])
+                with open(os.path.join(out_dir, f"{tag}{i}.json")) as f:
+                    st = json.load(f)
+                assert st["first_invalid"] == fi and st["n_lines"] == data.count(b"\n"), (tag, q, st, fi)
 
 
 def make_csv() -> bytes:

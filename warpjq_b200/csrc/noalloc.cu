@@ -189,9 +189,14 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (e != cudaSuccess) {
     set_err(err, err_len, "cudaGetDevice: %s", cudaGetErrorString(e));
     return WARPJQ_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_err(err, err_len, "device %d is beyond the %d devices the no-allocation scan sets up", dev,
+            kMaxDevices);
+    return WARPJQ_ERR_INVALID_ARG;
   }
   DeviceSetup *s = nullptr;
   rc = noalloc_setup(dev, s, err, err_len);
@@ -206,7 +211,12 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
   unsigned long long *block_lines = (unsigned long long *)(base + kOffBlockLines);
   uint32_t *deep = (uint32_t *)(base + kOffDeep);
 
-  k_noalloc_reset<<<1, 32, 0, st>>>(ctr);
+  // Each launch's own status is checked (cudaLaunchKernel returns it), so an
+  // earlier, unrelated error of the caller is neither reported nor cleared.
+  {
+    void *args[] = {&ctr};
+    e = cudaLaunchKernel((const void *)k_noalloc_reset, dim3(1), dim3(32), args, 0, st);
+  }
   unsigned long long n_tiles = (n_bytes + kNoAllocTile - 1) / kNoAllocTile;
   if (n_bytes > 0) {
     ScanParams sp;
@@ -222,13 +232,25 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     sp.deep_words = deep;
     sp.deep_levels_per_cta = kNoAllocDeepLevels;
     unsigned grid = (unsigned)(n_tiles < s->grid ? n_tiles : s->grid);
-    k_scan<false><<<grid, kThreads, s->smem, st>>>(sp, plan);
-    k_reduce_tiles<<<kNoAllocReduceBlocks, kReduceThreads, 0, st>>>(tile_fsum, n_tiles, block_f,
-                                                                    tiles, ctr, block_lines);
-    k_finalize<<<1, 32, 0, st>>>(block_f, block_lines, kNoAllocReduceBlocks, tiles, ctr);
+    if (e == cudaSuccess) {
+      void *args[] = {&sp, &plan};
+      e = cudaLaunchKernel((const void *)k_scan<false>, dim3(grid), dim3(kThreads), args, s->smem, st);
+    }
+    if (e == cudaSuccess) {
+      unsigned nb = kNoAllocReduceBlocks;
+      void *args[] = {&tile_fsum, &n_tiles, &block_f, &tiles, &ctr, &block_lines};
+      e = cudaLaunchKernel((const void *)k_reduce_tiles, dim3(nb), dim3(kReduceThreads), args, 0, st);
+    }
+    if (e == cudaSuccess) {
+      unsigned nb = kNoAllocReduceBlocks;
+      void *args[] = {&block_f, &block_lines, &nb, &tiles, &ctr};
+      e = cudaLaunchKernel((const void *)k_finalize, dim3(1), dim3(32), args, 0, st);
+    }
   }
-  k_noalloc_result<<<1, 32, 0, st>>>(ctr, d_result);
-  e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    void *args[] = {&ctr, &d_result};
+    e = cudaLaunchKernel((const void *)k_noalloc_result, dim3(1), dim3(32), args, 0, st);
+  }
   if (e != cudaSuccess) {
     set_err(err, err_len, "launch: %s", cudaGetErrorString(e));
     return WARPJQ_ERR_CUDA;

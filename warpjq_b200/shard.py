@@ -71,6 +71,14 @@ def csv_row_end(mv, pos: int, inside: bool) -> int:
     return n
 
 
+def _count_quotes(mv, lo: int, hi: int) -> int:
+    """'"' bytes in mv[lo, hi), counted a window at a time."""
+    n = 0
+    for a in range(lo, hi, 1 << 24):
+        n += bytes(mv[a:min(hi, a + (1 << 24))]).count(b'"')
+    return n
+
+
 def csv_shard_bounds(data, world: int) -> Tuple[int, List[Tuple[int, int]]]:
     """CSV input cut for `world` ranks: (header end, [start, end) of each
     rank's rows).  Cuts fall just after row ends (newlines outside quotes,
@@ -83,7 +91,9 @@ def csv_shard_bounds(data, world: int) -> Tuple[int, List[Tuple[int, int]]]:
     cuts = [h_end]
     for r in range(1, world):
         t = max(cuts[-1], h_end + (n - h_end) * r // world)
-        inside = bytes(mv[:t]).count(b'"') % 2 == 1
+        # every cut lies outside quotes, so the parity at t is that of the
+        # quotes between the previous cut and t
+        inside = _count_quotes(mv, cuts[-1], t) % 2 == 1
         cuts.append(max(csv_row_end(mv, t, inside), cuts[-1]))
     cuts.append(n)
     return h_end, list(zip(cuts[:-1], cuts[1:]))
@@ -152,8 +162,14 @@ class Partial:
     min: float = math.inf
     max: float = -math.inf
     saw_non_numeric: bool = False
+    # lowest malformed / type-error line index within the rank's range (None:
+    # none); after merge(), within the whole input
+    first_invalid: Optional[int] = None
+    first_type_error: Optional[int] = None
     groups: List[GroupPart] = field(default_factory=list)
-    rows: bytes = b""
+    # the rank's rows: bytes, or a uint8 torch tensor (on the rank's device
+    # for a device-resident run); gather() moves them without pickling
+    rows: object = b""
 
 
 class _DeviceBytes:
@@ -168,10 +184,13 @@ class _DeviceBytes:
 def partial_from_device(r: DeviceResult, shard_host) -> Partial:
     """The rank's partial from a collected device-resident run; group key
     bytes are read from the rank's host copy of its shard."""
+    none = (1 << 64) - 1
     p = Partial(n_lines=r.n_lines, n_blank=r.n_blank, n_invalid=r.n_invalid,
                 n_type_error=r.n_type_error, n_selected=r.n_selected, count=r.count,
                 numeric=r.numeric, isum=r.isum(), n_int=r.n_int, fsum=r.fsum, min=r.min, max=r.max,
-                saw_non_numeric=bool(r.saw_non_numeric))
+                saw_non_numeric=bool(r.saw_non_numeric),
+                first_invalid=None if r.first_invalid == none else int(r.first_invalid),
+                first_type_error=None if r.first_type_error == none else int(r.first_type_error))
     mv = memoryview(shard_host).cast("B")
     for k in range(r.n_groups):
         g = r.groups[k]
@@ -182,8 +201,8 @@ def partial_from_device(r: DeviceResult, shard_host) -> Partial:
                                   fsum=g.fsum, min=g.min, max=g.max))
     if r.out_len and r.d_out_bytes:
         import torch
-        t = torch.as_tensor(_DeviceBytes(r.d_out_bytes, r.out_len), device="cuda")
-        p.rows = t.cpu().numpy().tobytes()
+        # a device copy the rank owns (the run's buffer is reused by its next run)
+        p.rows = torch.as_tensor(_DeviceBytes(r.d_out_bytes, r.out_len), device="cuda").clone()
     return p
 
 
@@ -194,6 +213,12 @@ def merge(parts: Sequence[Partial]) -> Partial:
     groups = {}
     rows = []
     for p in parts:
+        # first bad lines: the first rank that has one, offset by the lines
+        # of the ranks before it
+        if m.first_invalid is None and p.first_invalid is not None:
+            m.first_invalid = m.n_lines + p.first_invalid
+        if m.first_type_error is None and p.first_type_error is not None:
+            m.first_type_error = m.n_lines + p.first_type_error
         m.n_lines += p.n_lines
         m.n_blank += p.n_blank
         m.n_invalid += p.n_invalid
@@ -221,8 +246,14 @@ def merge(parts: Sequence[Partial]) -> Partial:
             acc.min = min(acc.min, g.min)
             acc.max = max(acc.max, g.max)
     m.groups = list(groups.values())
-    m.rows = b"".join(rows)
+    m.rows = b"".join(_host_bytes(r) for r in rows)
     return m
+
+
+def _host_bytes(rows) -> bytes:
+    if isinstance(rows, (bytes, bytearray)):
+        return bytes(rows)
+    return rows.cpu().numpy().tobytes()
 
 
 def _sum(isum: int, n_int: int, fsum: float) -> float:
@@ -258,13 +289,46 @@ def render(query: str, merged: Partial, fmt: str = "ndjson") -> bytes:
 
 
 def gather(partial: Partial, rank: int, world: int, group=None) -> Optional[List[Partial]]:
-    """Rank 0 receives every rank's partial, in rank order (others: None)."""
+    """Rank 0 receives every rank's partial, in rank order (others: None).
+
+    The small part (counts, aggregate state, groups) travels as one object
+    per rank.  Rows do not: the ranks' row byte counts are all-gathered, an
+    exclusive scan of them gives each rank's offset in the output, and rank
+    0 receives each rank's rows straight into its slice of one output tensor
+    (on the ranks' devices with NCCL, in host memory with gloo).  Every rank
+    takes the same collective steps in the same order."""
     if world == 1:
         return [partial]
+    import torch
     import torch.distributed as dist
-    out = [None] * world if rank == 0 else None
-    dist.gather_object(partial, out, dst=0, group=group)
-    return out
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    rows = partial.rows
+    if isinstance(rows, (bytes, bytearray)):
+        rows = torch.frombuffer(bytearray(rows), dtype=torch.uint8) if rows else torch.empty(0, dtype=torch.uint8)
+    rows = rows.to(dev)
+    head = Partial(**{k: v for k, v in partial.__dict__.items() if k != "rows"})
+    heads = [None] * world if rank == 0 else None
+    dist.gather_object(head, heads, dst=0, group=group)
+    sizes = torch.zeros(world, dtype=torch.int64, device=dev)
+    mine = torch.tensor([rows.numel()], dtype=torch.int64, device=dev)
+    dist.all_gather_into_tensor(sizes, mine, group=group)
+    sz = [int(x) for x in sizes.cpu()]
+    offs = [0]
+    for x in sz:
+        offs.append(offs[-1] + x)  # exclusive scan: rank r's rows start at offs[r]
+    if rank == 0:
+        out = torch.empty(offs[-1], dtype=torch.uint8, device=dev)
+        out[: sz[0]].copy_(rows)
+        for r in range(1, world):
+            if sz[r]:
+                dist.recv(out[offs[r]:offs[r + 1]], src=r, group=group)
+        for r in range(world):
+            heads[r].rows = out[offs[r]:offs[r + 1]]
+        return heads
+    if sz[rank]:
+        dist.send(rows.contiguous(), dst=0, group=group)
+    return None
 
 
 def device_partial(query: str, shard_host, fmt: str = "ndjson") -> Partial:
@@ -330,13 +394,20 @@ def run_sharded_csv(query: str, host_data, rank: int, world: int, fmt: str = "nd
     return render(query, merge(parts), fmt)
 
 
+def run_sharded_partial(query: str, host_data, rank: int, world: int, fmt: str = "ndjson",
+                        group=None) -> Optional[Partial]:
+    """run_sharded's merged result on rank 0 (None on the others): counts,
+    the first malformed / type-error line of the whole input, aggregate
+    state, groups and rows."""
+    lo, hi = shard_bounds(host_data, world)[rank]
+    part = device_partial(query, memoryview(host_data).cast("B")[lo:hi], fmt)
+    parts = gather(part, rank, world, group)
+    return merge(parts) if rank == 0 else None
+
+
 def run_sharded(query: str, host_data, rank: int, world: int, fmt: str = "ndjson",
                 group=None) -> Optional[bytes]:
     """Runs `query` over `host_data` on `world` GPUs (this process: `rank`,
     on the current CUDA device).  Returns the output bytes on rank 0."""
-    lo, hi = shard_bounds(host_data, world)[rank]
-    part = device_partial(query, memoryview(host_data).cast("B")[lo:hi], fmt)
-    parts = gather(part, rank, world, group)
-    if rank != 0:
-        return None
-    return render(query, merge(parts), fmt)
+    m = run_sharded_partial(query, host_data, rank, world, fmt, group)
+    return None if m is None else render(query, m, fmt)
