@@ -137,14 +137,71 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(data: bytes, queries, threads=0):
+def cpu_baseline(data, queries, threads=0):
+    """Seconds the oracle (all host threads) takes for `queries` over `data`
+    (bytes or a uint8 numpy array), and each query's output bytes."""
     from oracle import pyoracle as orc
     t = time.perf_counter()
+    outs = []
     for q in queries:
         r = orc.run(q, data, threads=threads)
         if r.rc != 0:
             raise RuntimeError(r.err)
-    return time.perf_counter() - t
+        outs.append(r.out)
+    return time.perf_counter() - t, outs
+
+
+def same_output(got: bytes, want: bytes, rel: float = 1e-9) -> bool:
+    """Byte-identical, or (aggregates of fractional values) equal line by
+    line with numbers within `rel` relative: the device sums exactly and
+    rounds once, the oracle adds in line order."""
+    if got == want:
+        return True
+    a, b = got.split(b"\n"), want.split(b"\n")
+    if len(a) != len(b):
+        return False
+    for x, y in zip(a, b):
+        if x == y:
+            continue
+        try:
+            jx, jy = json.loads(x), json.loads(y)
+        except ValueError:
+            return False
+        if not _close(jx, jy, rel):
+            return False
+    return True
+
+
+def _close(x, y, rel):
+    if isinstance(x, dict) and isinstance(y, dict):
+        return x.keys() == y.keys() and all(_close(x[k], y[k], rel) for k in x)
+    if isinstance(x, list) and isinstance(y, list):
+        return len(x) == len(y) and all(_close(p, q, rel) for p, q in zip(x, y))
+    if isinstance(x, (int, float)) and isinstance(y, (int, float)) and not isinstance(x, bool):
+        return x == y or abs(x - y) <= rel * max(abs(x), abs(y))
+    return x == y
+
+
+class _DevView:
+    """n bytes of device memory at ptr, described for torch.as_tensor."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 2}
+
+
+def _d2h(ptr: int, n: int) -> bytes:
+    import torch
+    return torch.as_tensor(_DevView(ptr, n), device="cuda").cpu().numpy().tobytes()
+
+
+def device_output(Q, r, host_data) -> bytes:
+    """A device-resident run's output bytes: aggregates rendered by the host
+    library (group keys read from the host copy of the input), rows copied
+    from device memory."""
+    if Q.is_aggregate:
+        return Q.render_device(r, host_data)
+    return _d2h(r.d_out_bytes, r.out_len) if r.out_len else b""
 
 
 def batch_workload(hnp, n, n_inputs=4096, lo=4096, hi=4 << 20, seed=7):
@@ -373,7 +430,7 @@ NESTED_QUERIES = [
 ]
 
 
-def measure_nested(wjq, n_bytes=2_000_000_000, reps=3):
+def measure_nested(wjq, n_bytes=2_000_000_000, reps=3, check=True):
     """Device-resident GB/s of the nested workload's two queries (best of
     `reps` after a warm-up run; CUDA events around all kernels of a run)."""
     import torch
@@ -386,6 +443,7 @@ def measure_nested(wjq, n_bytes=2_000_000_000, reps=3):
     out = {"bytes": n, "lines": lines, "residency": "device",
            "sizes": "2 GB (rescaled from 4 GB for the bench's time budget), 1M Zipf(0.9) user ids",
            "per_query_gbs": {}}
+    outs = []
     for q in NESTED_QUERIES:
         Q = wjq.Query(q, chunk_bytes=1 << 20)
         Q.autotile(host.numpy()[: 1 << 20])
@@ -401,17 +459,21 @@ def measure_nested(wjq, n_bytes=2_000_000_000, reps=3):
             ms = e0.elapsed_time(e1)
             best = ms if best is None else min(best, ms)
         out["per_query_gbs"][q] = round(n / (best / 1e3) / 1e9, 2)
+        outs.append(device_output(Q, r, host.numpy()))
         if Q.is_grouped:
             out["groups"] = r.n_groups
         Q.close()
     del dev
+    if check:  # the oracle over the same bytes (skip-invalid, as the device runs)
+        _, want = cpu_baseline(host.numpy()[:n], NESTED_QUERIES)
+        out["parity"] = {q: same_output(g, w) for q, g, w in zip(NESTED_QUERIES, outs, want)}
     return out
 
 
 CSV_QUERY = "group_by(.path) | max(.latency_ms)"
 
 
-def measure_csv(wjq, n_bytes=2_000_000_000, reps=3, e2e=True):
+def measure_csv(wjq, n_bytes=2_000_000_000, reps=3, e2e=True, check=True):
     """The nginx records as 2 GB of CSV (RFC 4180 quoting on ua), query
     group_by(.path) | max(.latency_ms).  Device-resident GB/s of CSV bytes
     (conversion to NDJSON on the device plus the scan; CUDA events around
@@ -440,6 +502,16 @@ def measure_csv(wjq, n_bytes=2_000_000_000, reps=3, e2e=True):
         if best is None or t[0] < best[0]:
             best = t
     assert recs == rows and r.n_groups == 32, (recs, rows, r.n_groups)
+    parity = None
+    if check:
+        # the oracle over the NDJSON rendering of exactly these CSV records;
+        # group keys of the device result index the converted NDJSON
+        conv_np = torch.as_tensor(_DevView(d, nd), device="cuda").cpu().numpy()
+        got = Q.render_device(r, conv_np)
+        exp, eu, _ = wjq.gen_nginx_csv_as_ndjson(n_bytes, seed=6)
+        _, want = cpu_baseline(exp[:eu], [CSV_QUERY])
+        parity = {CSV_QUERY: same_output(got, want[0])}
+        del conv_np, exp
     Q.close()
     conv.close()
     del dev
@@ -459,7 +531,8 @@ def measure_csv(wjq, n_bytes=2_000_000_000, reps=3, e2e=True):
             "convert_gbs": round(n / (best[1] / 1e3) / 1e9, 2),
             "scan_gbs_of_ndjson": round(nd / (best[2] / 1e3) / 1e9, 2),
             "ms": [round(x, 3) for x in best],
-            "e2e_gbs": round(n / el / 1e9, 3) if el else None}
+            "e2e_gbs": round(n / el / 1e9, 3) if el else None,
+            "parity": parity}
 
 
 def measure_file(wjq, hnp, n, n_bytes=2_000_000_000):
@@ -493,36 +566,40 @@ def measure_file(wjq, hnp, n, n_bytes=2_000_000_000):
 
 def run_reference(args, rank):
     """The reference arm: the reference's CPU engine, as restated by the
-    oracle (the Rust crate cannot be built here), on all host cores."""
+    oracle (the Rust crate cannot be built here), on all host cores, over
+    the same input as the product's arm: the seeded 8 GB of nginx NDJSON
+    (generated by the oracle library's copy of the generator, so no product
+    library is loaded).  Each timed step runs one of the four queries over
+    the whole input, cycling through them; warm-up steps run them over the
+    input's first 256 MB.  Under torchrun only rank 0 runs."""
     if rank != 0:
         return
-    import numpy as np
-    import warpjq_b200 as wjq
+    from oracle import pyoracle as orc
     cores = os.cpu_count() or 1
-    # Size each step to ~120 s / (steps + warmup) of CPU work in total.
-    probe, used, _ = wjq.gen_nginx(64 << 20, seed=1)
-    data = bytes(probe[:used])
-    dt = cpu_baseline(data, QUERIES)
-    rate = len(data) * len(QUERIES) / dt
-    per_step = 120.0 / max(1, args.steps + args.warmup)
-    sample = int(min(1 << 30, max(16 << 20, rate * per_step / len(QUERIES))))
-    buf, used, lines = wjq.gen_nginx(sample, seed=1)
-    data = bytes(buf[:used])
-    for _ in range(args.warmup):
-        cpu_baseline(data, QUERIES)
+    buf, n, lines = orc.gen_nginx(args.bytes, seed=1)
+    data = buf[:n]
+    warm_n = bytes(data[: 256 << 20]).rfind(b"\n") + 1
+    for k in range(args.warmup):
+        cpu_baseline(data[:warm_n], [QUERIES[k % len(QUERIES)]])
     t = 0.0
-    for _ in range(args.steps):
-        t += cpu_baseline(data, QUERIES)
-    value = len(data) * len(QUERIES) * args.steps / t / 1e9
+    per_q = {}
+    for k in range(args.steps):
+        q = QUERIES[k % len(QUERIES)]
+        dt, _ = cpu_baseline(data, [q])
+        t += dt
+        per_q.setdefault(q, []).append(dt)
+    value = n * args.steps / t / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_bytes_per_query": used, "sample_lines": lines,
-                   "queries": QUERIES},
+        "config": {"workload": WORKLOAD, "input_bytes": n, "lines": lines, "queries": QUERIES,
+                   "same_config": True,
+                   "step": "one query over the whole input, cycling through the four",
+                   "per_query_gbs": {q: round(n * len(v) / sum(v) / 1e9, 4) for q, v in per_q.items()}},
         "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": "port",
-                         "sample": f"{used} bytes x {len(QUERIES)} queries per step"},
+                         "sample": f"the whole {n}-byte input per step, one query per step"},
         "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -537,7 +614,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bytes", type=int, default=8_000_000_000, help="input bytes per GPU")
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch and serving legs")
     ap.add_argument("--csv-only", type=int, default=0, metavar="BYTES",
@@ -635,6 +711,8 @@ def main():
     for i, r in enumerate(results):
         scan_ms[i] = r.scan_ms
         assert (r.n_selected, r.count, r.out_len, r.isum(), r.n_groups) == first[i], "results changed"
+    # the last timed run's outputs, for the parity check against the oracle
+    device_outs = [device_output(Q, r, hnp) for Q, r in zip(qs, results)] if rank == 0 else []
 
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -710,15 +788,19 @@ def main():
         csv_leg = measure_csv(wjq)
         e2e_file = measure_file(wjq, hnp, n)
 
-    cpu = None
+    # CPU baseline and parity: the oracle on all host cores over the whole
+    # input, each query once after a warm-up pass over the first 256 MB; its
+    # outputs are the expected bytes for the device runs' outputs.
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sample = bytes(hnp[: min(args.cpu_sample, n)])
-        cut = sample.rfind(b"\n") + 1
-        sample = sample[:cut]
-        ct = cpu_baseline(sample, QUERIES)
-        cpu = {"value": round(len(sample) * len(QUERIES) / ct / 1e9, 4), "unit": "GB/s",
+        warm_n = bytes(hnp[: min(256 << 20, n)]).rfind(b"\n") + 1
+        cpu_baseline(hnp[:warm_n], QUERIES)
+        ct, want = cpu_baseline(hnp[:n], QUERIES)
+        cpu = {"value": round(n * len(QUERIES) / ct / 1e9, 4), "unit": "GB/s",
                "cores": os.cpu_count(), "kind": "port",
-               "sample": f"first {len(sample)} bytes of the input, 4 queries"}
+               "sample": f"the whole {n}-byte input, each of the 4 queries once, after a warm-up "
+                         f"pass over its first {warm_n} bytes"}
+        parity = {q: same_output(g, w) for q, g, w in zip(QUERIES, device_outs, want)}
 
     if rank == 0:
         line = {
@@ -746,6 +828,7 @@ def main():
                     "host_link_h2d_gbs": link_gbs},
             "gpu_launches": kernels_per_step * args.steps,
             "clocks": clk,
+            "parity": parity,
             "cpu_baseline": cpu,
             "e2e_file": e2e_file,
             "batch": batch,

@@ -31,7 +31,8 @@ typedef struct {
   uint64_t isum_lo;   /* exact sum of integer-literal values, two's complement */
   uint64_t isum_hi;
   uint64_t n_int;     /* how many values went into the exact sum */
-  double fsum;        /* fixed-order FP64 sum of the other numbers */
+  double fsum;        /* exact sum of the other numbers, rounded once to FP64 (independent of
+                         tiling and of the order work runs in) */
   double min;
   double max;
   double sum;         /* isum + fsum rounded once to FP64 */
@@ -251,10 +252,10 @@ typedef struct {
   uint64_t isum_lo;       /* exact sum of integer-literal values, two's complement */
   uint64_t isum_hi;
   uint64_t n_int;
-  double fsum;            /* fixed-order FP64 sum of the other numbers */
+  double fsum;            /* exact sum of the other numbers, rounded once to FP64 */
   double min;
   double max;
-  double sum;             /* isum + fsum; exact while |isum| < 2^53 and fsum == 0 */
+  double sum;             /* isum + the other numbers, summed exactly and rounded once */
   uint32_t saw_non_numeric;
   uint32_t status;        /* 0 complete; 1 a fixed limit was hit, do not use the counts */
 } warpjq_noalloc_result;

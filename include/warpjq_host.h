@@ -115,6 +115,11 @@ uint64_t warpjq_gen_nginx_csv(uint64_t seed, uint8_t *out, uint64_t target, uint
                               unsigned threads, uint64_t *total_lines);
 uint64_t warpjq_gen_nginx_csv_block(uint64_t seed, uint64_t block, uint64_t first_line, uint8_t *out,
                                     uint64_t cap, uint64_t *n_lines);
+/* The NDJSON lines of exactly the records warpjq_gen_nginx_csv writes with
+ * the same seed, target and block size, in order; `out` holds 2 * target
+ * bytes.  Returns the bytes written. */
+uint64_t warpjq_gen_nginx_csv_as_ndjson(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                                        unsigned threads, uint64_t *total_lines);
 
 /* The same for a nested, dirty schema: objects 3-5 levels deep with shuffled
  * key order (req.user.{id, tier, geo{cc, lat, lon}}, req.method, req.path,

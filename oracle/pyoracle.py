@@ -77,17 +77,33 @@ class OracleResult:
         return f"OracleResult(rc={self.rc}, out={self.out[:80]!r}, stats={self.stats}, err={self.err!r})"
 
 
-def run(query: str, data: bytes, fmt: str = "ndjson", on_invalid: str = "skip",
+def _input(data):
+    """(pointer argument, length, keep-alive) for bytes or a uint8 numpy array
+    (the array is passed without a copy)."""
+    if isinstance(data, bytes):
+        return data, len(data), None
+    if isinstance(data, bytearray):
+        b = bytes(data)
+        return b, len(b), b
+    import numpy as np
+    a = np.ascontiguousarray(data, dtype=np.uint8)
+    return a.ctypes.data_as(ctypes.c_char_p), a.size, a
+
+
+def run(query: str, data, fmt: str = "ndjson", on_invalid: str = "skip",
         chunk_bytes: int = 0, threads: int = 0, max_line_bytes: int = 0) -> OracleResult:
-    """Runs a query the way the reference CPU engine's run_bytes does."""
+    """Runs a query the way the reference CPU engine's run_bytes does; `data`
+    is bytes or a uint8 numpy array."""
     L = lib()
     out = ctypes.c_void_p()
     n = ctypes.c_size_t()
     stats = (ctypes.c_uint64 * 5)()
     err = ctypes.create_string_buffer(4096)
-    rc = L.oracle_run(query.encode(), data, len(data), FORMATS[fmt], ON_INVALID[on_invalid],
+    ptr, ln, keep = _input(data)
+    rc = L.oracle_run(query.encode(), ptr, ln, FORMATS[fmt], ON_INVALID[on_invalid],
                       chunk_bytes, threads, max_line_bytes, ctypes.byref(out), ctypes.byref(n),
                       stats, err, len(err))
+    del keep
     body = _take(out, n)
     st = dict(zip(["bytes_in", "lines_in", "lines_out", "malformed", "type_errors"], list(stats)))
     return OracleResult(rc, body, st, err.value.decode(errors="replace"))
@@ -139,3 +155,19 @@ def eval_select(line: bytes, query: str) -> bool:
 
 def parse_f64(text: bytes) -> float:
     return lib().oracle_parse_f64(text, len(text))
+
+
+def gen_nginx(n_bytes: int, seed: int = 1, threads: int = 0, into=None):
+    """The benchmark's seeded nginx-style NDJSON, from the generator compiled
+    into the oracle library (the same source as the product's generator),
+    so a CPU-only measurement builds its input without the product's
+    libraries.  Returns (buffer, used_bytes, n_lines)."""
+    import numpy as np
+    L = lib()
+    L.warpjq_gen_nginx.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                   ctypes.c_uint, ctypes.POINTER(ctypes.c_uint64)]
+    L.warpjq_gen_nginx.restype = ctypes.c_uint64
+    buf = into if into is not None else np.empty(n_bytes, dtype=np.uint8)
+    lines = ctypes.c_uint64()
+    used = L.warpjq_gen_nginx(seed, buf.ctypes.data, n_bytes, 1 << 20, threads, ctypes.byref(lines))
+    return buf, int(used), int(lines.value)

@@ -40,9 +40,10 @@ using namespace wjq;
 extern "C" {
 
 // One output line per physical input line (mode 0: the bounded walker
-// walk_line; mode 1: the window walker walk_window, with the line copied at
-// a varying alignment into a window whose bytes past the newline are
-// quotes, backslashes and digits):
+// walk_line; mode 1: the window walker walk_masked, with the line copied at
+// a varying offset into a window whose bytes past the newline are quotes,
+// backslashes and digits, and the window's special mask made by the
+// kernel's chunk classifier):
 //   blank | invalid | type | filtered | selected<TAB>kind:raw<TAB>...
 // Returns 0, or 2 for a query error, 3 for a plan error.
 int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char **out,
@@ -59,7 +60,7 @@ int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char *
   DeepStack deep{deep_words.data(), (uint64_t)deep_words.size() * 32};
   static NodeVals nv;
   std::string o;
-  std::vector<uint32_t> winbuf;
+  std::vector<uint32_t> winbuf, smask;
   size_t pos = 0, line_no = 0;
   while (pos < len) {
     const uint8_t *nl = (const uint8_t *)std::memchr(data + pos, '\n', len - pos);
@@ -69,14 +70,20 @@ int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char *
     pos = end + 1;
     int st;
     if (mode == 1) {
-      uint32_t s = (uint32_t)(line_no++ * 7 % 16);
-      winbuf.assign((s + n + 64) / 4 + 1, 0);
+      // the line at a varying offset (across 32-byte chunk boundaries), its
+      // newline, then quotes, backslashes and digits; the special mask of
+      // the whole window is made by the kernel's own chunk classifier
+      uint32_t s = (uint32_t)(line_no++ * 7 % 48);
+      const uint32_t W = (s + n + 64 + 31) / 32 * 32;
+      winbuf.assign(W / 4 + 8, 0);
       uint8_t *w = (uint8_t *)winbuf.data();
       std::memcpy(w + s, line, n);
       w[s + n] = '\n';
       for (uint32_t k = 1; k < 40; k++) w[s + n + k] = "\"\\9"[k % 3];
+      smask.assign(W / 32 + 1, 0);
+      for (uint32_t c = 0; c < W / 32; c++) classify_chunk(winbuf.data() + 8 * c, &smask[c]);
       line = w + s;
-      st = walk_window(P, w, s, s + n, nv);
+      st = walk_masked(P, w, smask.data(), s, s + n, nv);
     } else {
       st = walk_line(P, line, n, nv, nullptr);
     }

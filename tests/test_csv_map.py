@@ -15,6 +15,7 @@ import random
 import pytest
 
 from oracle import csv_map
+import warpjq_b200 as wjq
 
 HAND = [
     (b"", b""),
@@ -117,3 +118,14 @@ def test_nginx_csv_rendering_maps_to_the_ndjson_rendering():
     lines = bytes(nbuf[:nused]).split(b"\n")
     assert len(mapped) > 2000
     assert mapped == lines[:len(mapped)]
+
+
+def test_csv_records_rendered_as_ndjson_match_the_mapping():
+    """warpjq_gen_nginx_csv_as_ndjson (the expected input of a query over the
+    bench's CSV) is exactly the mapping of the CSV rows of the same seed and
+    size, so the oracle over it checks the CSV leg at its full size."""
+    for size, seed in ((1 << 20, 6), (5 << 20, 7), (200_000, 2)):
+        c, cu, cl = wjq.gen_nginx_csv(size, seed=seed)
+        n, nu, nl = wjq.gen_nginx_csv_as_ndjson(size, seed=seed)
+        assert cl == nl
+        assert csv_map.csv_to_ndjson(bytes(c[:cu])) == bytes(n[:nu])

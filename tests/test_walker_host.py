@@ -1,5 +1,5 @@
 """The device line walkers (the bounded walk_line and the window walker
-walk_window) and evaluator (warpjq_b200/csrc/walker.cuh), compiled for the
+walk_masked) and evaluator (warpjq_b200/csrc/walker.cuh), compiled for the
 host, against the oracle's per-line semantics
 (exec/cpu.rs:299-371): same verdict per line -- blank, invalid, type error,
 filtered, selected -- and, for selected lines, the same resolved value of
@@ -52,7 +52,7 @@ def check(harness, data, queries, label):
     L, o = harness
     for q in queries:
         ref = _run(o.oracle_eval_lines, o.oracle_free, q, data)
-        for mode, name in ((0, "walk_line"), (1, "walk_window")):
+        for mode, name in ((0, "walk_line"), (1, "walk_masked")):
             dev = _run(L.wh_eval, L.wh_free, q, data, mode)
             assert len(dev) == len(ref), (label, q, name)
             for i, (a, b) in enumerate(zip(dev, ref)):

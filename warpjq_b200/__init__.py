@@ -46,7 +46,8 @@ HOST_SYMBOLS = [
     "warpjq_query_run", "warpjq_run_bytes", "warpjq_query_render_device", "warpjq_host_free",
     "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
     "warpjq_gen_nested", "warpjq_gen_nested_block", "warpjq_query_run_file", "warpjq_query_run_csv",
-    "warpjq_gen_nginx_csv", "warpjq_gen_nginx_csv_block", "warpjq_query_render_batch",
+    "warpjq_gen_nginx_csv", "warpjq_gen_nginx_csv_block", "warpjq_gen_nginx_csv_as_ndjson",
+    "warpjq_query_render_batch",
 ]
 
 
@@ -130,6 +131,8 @@ def _load():
     h.warpjq_query_run_csv.restype = ctypes.c_int
     h.warpjq_gen_nginx_csv.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
     h.warpjq_gen_nginx_csv.restype = u64
+    h.warpjq_gen_nginx_csv_as_ndjson.argtypes = [u64, vp, u64, u64, ctypes.c_uint, ctypes.POINTER(u64)]
+    h.warpjq_gen_nginx_csv_as_ndjson.restype = u64
     h.warpjq_run_bytes.argtypes = [cp, cp, sz, u32, u32, u64, u64, ctypes.POINTER(vp),
                                    ctypes.POINTER(sz), ctypes.POINTER(u64), cp, sz]
     h.warpjq_run_bytes.restype = ctypes.c_int
@@ -650,6 +653,18 @@ def gen_nginx_csv(n_bytes: int, seed: int = 1, threads: int = 0, into=None):
     buf = into if into is not None else np.empty(n_bytes, dtype=np.uint8)
     lines = ctypes.c_uint64()
     used = h.warpjq_gen_nginx_csv(seed, buf.ctypes.data, n_bytes, 1 << 20, threads, ctypes.byref(lines))
+    return buf, int(used), int(lines.value)
+
+
+def gen_nginx_csv_as_ndjson(n_bytes: int, seed: int = 1, threads: int = 0):
+    """The NDJSON lines of exactly the records gen_nginx_csv(n_bytes, seed)
+    writes as CSV rows; returns (buffer, used_bytes, n_lines)."""
+    import numpy as np
+    _, h = _load()
+    buf = np.empty(2 * n_bytes + 16, dtype=np.uint8)
+    lines = ctypes.c_uint64()
+    used = h.warpjq_gen_nginx_csv_as_ndjson(seed, buf.ctypes.data, n_bytes, 1 << 20, threads,
+                                            ctypes.byref(lines))
     return buf, int(used), int(lines.value)
 
 

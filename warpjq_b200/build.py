@@ -5,7 +5,6 @@
                                             reference's Rust crate links
   warpjq_b200/_lib/libwarpjq_host.so     -- the C++ host driver (query front-end,
                                             pipeline, formatting)
-  warpjq_b200/_lib/warpjq                -- the command-line tool
 
 Run: python -m warpjq_b200.build   (nvcc cross-compiles; no GPU needed)
 """
@@ -25,9 +24,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 KERNEL_SRCS = [os.path.join(CSRC, "backend.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "csv.cu")]
-KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "plan.h", "csv_rows.cuh")]
+KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "fixsum.cuh", "plan.h",
+                                               "plan_build.h", "csv_rows.cuh")]
 HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc")]
-CLI_SRCS = [os.path.join(CSRC, "host", "cli.cc")]
 HEADERS = [os.path.join(ROOT, "include", f) for f in ("warpjq_kernels.h", "warpjq_ext.h", "warpjq_host.h")]
 EXPORTS = os.path.join(CSRC, "exports.map")  # only the C ABI is exported
 
@@ -70,10 +69,6 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> None:
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wl,--version-script=" + EXPORTS, "-o", host,
               *HOST_SRCS,
               "-L" + LIB, "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN", "-lpthread"])
-    cli = os.path.join(LIB, "warpjq")
-    if all(os.path.exists(s) for s in CLI_SRCS) and (force or _stale(cli, CLI_SRCS + [host])):
-        _run(["g++", "-O2", "-std=c++17", "-o", cli, *CLI_SRCS, "-L" + LIB, "-lwarpjq_host",
-              "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN", "-lpthread"])
 
 
 if __name__ == "__main__":

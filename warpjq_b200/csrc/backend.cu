@@ -87,8 +87,6 @@ struct RunBufs {
   DevBuf<uint8_t> recs;
   DevBuf<uint8_t> out;
   DevBuf<unsigned long long> row_off, line_idx;
-  DevBuf<double> tile_fsum;
-  DevBuf<double> block_f;
   DevBuf<unsigned long long> block_lines;
   DevBuf<uint32_t> deep;
   // group table
@@ -110,8 +108,8 @@ struct RunBufs {
     b_in_ctr.release();
     b_plans.release();
     b_in_plan.release();
-    recs.release(); out.release(); row_off.release(); line_idx.release(); tile_fsum.release();
-    block_f.release(); block_lines.release(); deep.release(); g_slots.release();
+    recs.release(); out.release(); row_off.release(); line_idx.release();
+    block_lines.release(); deep.release(); g_slots.release();
     g_keys.release(); g_acc.release();
   }
 };
@@ -133,14 +131,7 @@ __global__ void k_reset_run(RunCounters *ctr, GroupTable g, uint32_t g_cap, uint
   }
   if (g.slots) {
     for (unsigned long long i = tid; i < g_cap; i += stride) g.slots[i] = 0;
-    for (unsigned long long i = tid; i < key_cap; i += stride) {
-      GroupAcc a;
-      a.count = a.numeric = a.isum_lo = a.isum_hi = a.n_int = 0;
-      a.min_bits = ~0ull;
-      a.max_bits = 0;
-      a.fsum = 0.0;
-      g.acc[i] = a;
-    }
+    for (unsigned long long i = tid; i < key_cap; i += stride) group_acc_init(g.acc[i]);
   }
 }
 
@@ -257,8 +248,6 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
   if (n_tiles == 0) n_tiles = 1;
   CK(rb.ctr.ensure(1, st, cap), "alloc counters");
   CK(rb.tiles.ensure(n_tiles, st, cap), "alloc tiles");
-  CK(rb.tile_fsum.ensure(n_tiles, st, cap), "alloc tile sums");
-  CK(rb.block_f.ensure(kReduceBlocks, st, cap), "alloc reduce");
   CK(rb.block_lines.ensure(2 * kReduceBlocks, st, cap), "alloc reduce");
   if (!rb.deep_levels) rb.deep_levels = 1u << 16;
   CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32), st, cap), "alloc deep stack");
@@ -370,7 +359,6 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.row_tiles = rb.row_tiles.p;
     sp.rec_scratch = rb.recs.p;
     sp.rec_cap_per_cta = rb.rec_cap_per_cta;
-    sp.tile_fsum = rb.tile_fsum.p;
     sp.g = g;
     sp.deep_words = rb.deep.p;
     sp.deep_levels_per_cta = rb.deep_levels;
@@ -429,18 +417,15 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       s.kernels += 3;
       CK(cudaGetLastError(), "launch rows");
     }
-    k_reduce_tiles<<<kReduceBlocks, kReduceThreads, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
-                                                       n_tiles, rb.block_f.p, rb.tiles.p,
-                                                       rb.ctr.p, rb.block_lines.p);
+    k_reduce_tiles<<<kReduceBlocks, kReduceThreads, 0, st>>>(n_tiles, rb.tiles.p, rb.ctr.p,
+                                                             rb.block_lines.p);
     s.kernels++;
     CK(cudaGetLastError(), "launch reduce");
-    k_finalize<<<1, 32, 0, st>>>(rb.block_f.p, rb.block_lines.p, kReduceBlocks, rb.tiles.p,
-                                 rb.ctr.p);
+    k_finalize<<<1, 32, 0, st>>>(rb.block_lines.p, kReduceBlocks, rb.tiles.p, rb.ctr.p);
     s.kernels++;
     CK(cudaGetLastError(), "launch finalize");
     if (b && n_inputs) {
-      k_batch_finalize<<<(n_inputs + 7) / 8, 256, 0, st>>>(P.needs_rows ? nullptr : rb.tile_fsum.p,
-                                                          rb.tiles.p, rb.b_in_tile0.p, rb.b_in_ctr.p,
+      k_batch_finalize<<<(n_inputs + 7) / 8, 256, 0, st>>>(rb.tiles.p, rb.b_in_tile0.p, rb.b_in_ctr.p,
                                                           n_inputs);
       s.kernels++;
       CK(cudaGetLastError(), "launch batch finalize");
@@ -536,17 +521,12 @@ uint64_t bufs_signature(const warpjq_ctx *c) {
   mix((uintptr_t)rb.recs.p); mix(rb.recs.n);
   mix((uintptr_t)rb.out.p); mix(rb.out.n);
   mix((uintptr_t)rb.row_off.p); mix((uintptr_t)rb.line_idx.p);
-  mix((uintptr_t)rb.tile_fsum.p); mix((uintptr_t)rb.block_f.p); mix((uintptr_t)rb.block_lines.p);
+  mix((uintptr_t)rb.block_lines.p);
   mix((uintptr_t)rb.deep.p); mix(rb.deep.n);
   mix((uintptr_t)rb.g_slots.p); mix((uintptr_t)rb.g_keys.p); mix((uintptr_t)rb.g_acc.p);
   mix(rb.rec_cap_per_cta); mix(rb.out_cap); mix(rb.rows_cap); mix(rb.g_cap); mix(rb.g_key_cap);
   mix(rb.deep_levels); mix(c->tile_bytes); mix(c->halo_bytes); mix(c->grid); mix(c->scan_smem);
   return h;
-}
-
-double i128_to_double(unsigned long long lo, unsigned long long hi) {
-  __int128 v = (__int128)(((unsigned __int128)hi << 64) | lo);
-  return (double)v;
 }
 
 }  // namespace
@@ -796,10 +776,11 @@ static warpjq_status fetch_groups(warpjq_ctx *ctx, Slot &s, const RunCounters &h
     g.isum_lo = a.isum_lo;
     g.isum_hi = a.isum_hi;
     g.n_int = a.n_int;
-    g.fsum = a.fsum;
+    // exact sums, rounded once (fixsum.cuh)
+    g.fsum = fix_to_double(a.fix, 0, 0) + a.fbig;
     g.min = a.numeric ? from_order_bits(a.min_bits) : 1.0 / 0.0;
     g.max = a.numeric ? from_order_bits(a.max_bits) : -1.0 / 0.0;
-    g.sum = (a.n_int ? i128_to_double(a.isum_lo, a.isum_hi) : 0.0) + a.fsum;
+    g.sum = fix_to_double(a.fix, a.isum_lo, a.isum_hi) + a.fbig;
     out.push_back(g);
     if (inputs) inputs->push_back(keys[k].input);
   }
@@ -831,7 +812,7 @@ warpjq_status warpjq_wait(warpjq_ctx *ctx, uint32_t slot, warpjq_chunk_result *o
     if (P.group_slot < 0) {
       out->agg.count = h.agg_count;
       out->agg.numeric = h.agg_numeric;
-      out->agg.sum = (h.agg_n_int ? i128_to_double(h.agg_isum_lo, h.agg_isum_hi) : 0.0) + h.fsum_total;
+      out->agg.sum = h.sum_total;
       out->agg.min = h.agg_numeric ? from_order_bits(h.agg_min_bits) : 1.0 / 0.0;
       out->agg.max = h.agg_numeric ? from_order_bits(h.agg_max_bits) : -1.0 / 0.0;
       out->agg.saw_non_numeric = h.agg_saw_non_numeric;
@@ -1013,7 +994,7 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
   out->fsum = h.fsum_total;
   out->min = h.agg_numeric ? from_order_bits(h.agg_min_bits) : 1.0 / 0.0;
   out->max = h.agg_numeric ? from_order_bits(h.agg_max_bits) : -1.0 / 0.0;
-  out->sum = (h.agg_n_int ? i128_to_double(h.agg_isum_lo, h.agg_isum_hi) : 0.0) + h.fsum_total;
+  out->sum = h.sum_total;
   out->saw_non_numeric = h.agg_saw_non_numeric;
   if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
     rc = fetch_groups(ctx, s, h, ctx->dev_groups, err, err_len);
@@ -1173,7 +1154,7 @@ warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
     it.fsum = c.fsum_total;
     it.min = c.agg_numeric ? from_order_bits(c.agg_min_bits) : 1.0 / 0.0;
     it.max = c.agg_numeric ? from_order_bits(c.agg_max_bits) : -1.0 / 0.0;
-    it.sum = (c.agg_n_int ? i128_to_double(c.agg_isum_lo, c.agg_isum_hi) : 0.0) + c.fsum_total;
+    it.sum = c.sum_total;
     it.saw_non_numeric = c.agg_saw_non_numeric;
     it.group_begin = first[i];
     it.n_groups = first[i + 1] - first[i];

@@ -63,6 +63,52 @@ __device__ __forceinline__ uint32_t swar_movemask(uint32_t m) {
 }
 
 // ---------------------------------------------------------------------------
+// Structural classification of 32-byte chunks (the scan's first stage)
+// ---------------------------------------------------------------------------
+
+// Exact per-byte flags (0x80 in each byte lane) of the bytes of x that are
+// '"', '\\' or below 0x20.  Each test adds to the low seven bits, which never
+// carries across a byte lane; bytes >= 0x80 are never flagged.
+__host__ __device__ __forceinline__ uint32_t flags_special(uint32_t x) {
+  const uint32_t t = x & 0x7F7F7F7Fu;
+  const uint32_t sq = (t ^ 0x22222222u) + 0x7F7F7F7Fu;  // bit 7 clear iff '"'
+  const uint32_t sb = (t ^ 0x5C5C5C5Cu) + 0x7F7F7F7Fu;  // bit 7 clear iff '\\'
+  const uint32_t sc = t + 0x60606060u;                  // bit 7 clear iff < 0x20
+  return ~((sq & sb & sc) | x) & 0x80808080u;
+}
+
+// Exact per-byte flags of the '\n' bytes of x.
+__host__ __device__ __forceinline__ uint32_t flags_newline(uint32_t x) {
+  const uint32_t sn = ((x ^ 0x0A0A0A0Au) & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+  return ~(sn | x) & 0x80808080u;
+}
+
+// Moves the four flags of word k (0..7) of a chunk to bits 4k..4k+3.  The
+// multiply by 1 + 2^7 + 2^14 + 2^21 lands byte j's flag (bit 8j + 7) on bit
+// 28 + j; no two partial products share a bit, so nothing carries.
+__host__ __device__ __forceinline__ uint32_t flags_to_bits(uint32_t f, int k) {
+  const uint32_t prod = f * 0x00204081u;
+  return k == 7 ? (prod & 0xF0000000u) : ((prod >> (28 - 4 * k)) & (0xFu << (4 * k)));
+}
+
+// Classifies one 32-byte chunk given as eight little-endian words: returns
+// the newline mask (bit j: byte j is '\n') and stores the special mask (bit
+// j: byte j is '"', '\\' or below 0x20) in *special.  The special mask is
+// what string scanning needs: a string ends at its first unescaped '"', a
+// '\\' starts an escape, and any byte below 0x20 (the line's own newline
+// too) ends a malformed string.
+__host__ __device__ __forceinline__ uint32_t classify_chunk(const uint32_t w[8], uint32_t *special) {
+  uint32_t s = 0, nl = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    s |= flags_to_bits(flags_special(w[k]), k);
+    nl |= flags_to_bits(flags_newline(w[k]), k);
+  }
+  *special = s;
+  return nl;
+}
+
+// ---------------------------------------------------------------------------
 // Order-preserving float encoding (agg.rs:205-212)
 // ---------------------------------------------------------------------------
 

@@ -395,6 +395,51 @@ uint64_t warpjq_gen_nested(uint64_t seed, uint8_t *out, uint64_t target, uint64_
   return gen_parallel(seed, out, target, block_bytes, threads, total_lines, n_users, 1);
 }
 
+// The NDJSON rendering of exactly the records warpjq_gen_nginx_csv(seed,
+// .., target, block_bytes, ..) writes as CSV rows, in order (the expected
+// input of a query over that CSV).  `out` must hold 2 * target bytes: a
+// record's NDJSON line is under twice its CSV row.
+uint64_t warpjq_gen_nginx_csv_as_ndjson(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,
+                                        unsigned threads, uint64_t *total_lines) {
+  static const uint64_t h = 47;  // the CSV header row's length
+  if (target < h) {
+    if (total_lines) *total_lines = 0;
+    return 0;
+  }
+  target -= h;
+  if (block_bytes < 4096) block_bytes = 4096;
+  const uint64_t nb = (target + block_bytes - 1) / block_bytes;
+  std::vector<uint64_t> len(nb), lines(nb);
+  if (!threads) threads = std::max(1u, std::thread::hardware_concurrency());
+  std::vector<std::thread> ws;
+  for (unsigned t = 0; t < threads; t++) {
+    ws.emplace_back([&, t] {
+      std::vector<uint8_t> tmp(block_bytes);
+      for (uint64_t b = t; b < nb; b += threads) {
+        const uint64_t cap = std::min<uint64_t>(block_bytes, target - b * block_bytes);
+        const uint64_t first = b * (block_bytes / 64);
+        uint64_t k = 0;
+        warpjq_gen_nginx_csv_block(seed, b, first, tmp.data(), cap, &k);  // the block's row count
+        // the same draws rendered as NDJSON
+        Rng r(seed * 0x100000001B3ull ^ (b * 0xD1B54A32D192ED03ull));
+        char *p = (char *)out + 2 * b * block_bytes;
+        for (uint64_t i = 0; i < k; i++) p = nginx_line(p, r, first + i);
+        len[b] = (uint64_t)(p - ((char *)out + 2 * b * block_bytes));
+        lines[b] = k;
+      }
+    });
+  }
+  for (auto &w : ws) w.join();
+  uint64_t w = 0, total = 0;
+  for (uint64_t b = 0; b < nb; b++) {
+    if (w != 2 * b * block_bytes) memmove(out + w, out + 2 * b * block_bytes, len[b]);
+    w += len[b];
+    total += lines[b];
+  }
+  if (total_lines) *total_lines = total;
+  return w;
+}
+
 // About `target` bytes of the nginx records as CSV: a header row naming the
 // columns (ts,host,method,path,status,bytes,latency_ms,ua), then the rows.
 uint64_t warpjq_gen_nginx_csv(uint64_t seed, uint8_t *out, uint64_t target, uint64_t block_bytes,

@@ -5,12 +5,16 @@
 // 1117-1849) as one scan pass plus, for row output, two small passes:
 //
 //   k_scan      One warp per CTA.  A warp takes the next tile from a work
-//               ticket, stages tile + halo into shared memory with
-//               asynchronous 16-byte copies, marks its newlines, lists the
-//               lines that start in the tile, and walks them one line per
-//               lane (walker.cuh): validation, path resolution, the filter,
-//               and either the aggregate or a compact record per selected
-//               row (line offset, row length, field spans).
+//               ticket and stages tile + halo into shared memory with one
+//               bulk (TMA) copy.  Stage 1 is lane-parallel over 32-byte
+//               chunks: each chunk becomes two bit masks, its newlines and
+//               its "special" bytes ('"', '\\', < 0x20).  The lines that
+//               start in the tile are listed from the newline masks, and
+//               stage 2 walks them one line per lane (walker.cuh), jumping
+//               through strings by the special mask: validation, path
+//               resolution, the filter, and either the aggregate or a
+//               compact record per selected row (line offset, row length,
+//               field spans).
 //   k_rows_*    Rows only: block sums and an exclusive prefix over the
 //               per-tile (rows, bytes, lines) totals, then the rows are
 //               copied in line order from the input to the output.
@@ -23,6 +27,7 @@
 #include <stdint.h>
 
 #include "devutil.cuh"
+#include "fixsum.cuh"
 #include "plan.h"
 #include "walker.cuh"
 
@@ -35,12 +40,24 @@ constexpr int kScanBlocksPerSM = 24;         // register budget of k_scan: 24 wa
 
 constexpr int kGroupCache = 16;  // per-CTA group accumulators kept in shared memory
 
-// Dynamic shared memory of k_scan for tile T and halo H (the layout is at the
-// top of k_scan), plus the group cache for grouped aggregates.
+// Readable bytes kept past a window's data: the end sentinel, the walker's
+// word reads after a line's newline, and the last chunk's 32-byte read.
+constexpr uint32_t kWinSlack = 64;
+
+// Shared-memory layout of k_scan for tile T and halo H: the window bytes,
+// then the special and newline masks (one word per 32-byte chunk, the
+// sentinel's chunk included), the CTA's exact FP sum, the line-start list,
+// and for grouped aggregates the group cache.
+__host__ __device__ inline uint32_t scan_win_bytes(uint32_t T, uint32_t H) {
+  return (T + H + kWinSlack + 15u) & ~15u;
+}
+__host__ __device__ inline uint32_t scan_chunk_words(uint32_t T, uint32_t H) {
+  return ((T + H) / 32 + 2 + 3) & ~3u;
+}
 __host__ __device__ inline size_t scan_smem_base(uint32_t T, uint32_t H) {
-  size_t nchunk_max = (T + H) / 32 + 1;
-  size_t s = T + H + 32;
-  s += ((nchunk_max + 3) & ~(size_t)3) * sizeof(uint32_t);
+  size_t s = scan_win_bytes(T, H);
+  s += 2 * (size_t)scan_chunk_words(T, H) * sizeof(uint32_t);
+  s += kFixDigits * sizeof(long long);
   s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
   return (s + 15) & ~(size_t)15;
 }
@@ -57,13 +74,76 @@ struct RowRec {
 };
 static_assert(sizeof(RowRec) == kRowRecBytes, "row record header size");
 
-// One group key's accumulators: a 64-byte record, so all updates of a key
-// land on one line of memory.
+// One group key's accumulators, 128 bytes: the counts, the exact integer
+// sum and min/max in the first 64, the exact sum of the non-integer values
+// (fixsum.cuh) in the second.
 struct GroupAcc {
   unsigned long long count, numeric, isum_lo, isum_hi, n_int, min_bits, max_bits;
-  double fsum;
+  double fbig;                // non-integer values of magnitude >= 2^128
+  long long fix[kFixDigits];  // the other non-integer values, exactly
 };
-static_assert(sizeof(GroupAcc) == 64, "group accumulator record");
+static_assert(sizeof(GroupAcc) == 128, "group accumulator record");
+
+__device__ __forceinline__ void group_acc_init(GroupAcc &a) {
+  a.count = a.numeric = a.isum_lo = a.isum_hi = a.n_int = 0;
+  a.min_bits = ~0ull;
+  a.max_bits = 0;
+  a.fbig = 0.0;
+#pragma unroll
+  for (int k = 0; k < kFixDigits; k++) a.fix[k] = 0;
+}
+
+// Adds a non-integer value to exact limbs (global or shared memory) with
+// independent atomics; values too large for the limbs go to *big.
+__device__ __forceinline__ void fix_atomic_add(long long *limbs, double *big, double v) {
+  const FixParts pr = fix_split(v);
+  if (pr.d == -2) {
+    atomicAdd(big, v);
+    return;
+  }
+  if (pr.d < 0) return;
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    if (pr.part[k] && pr.d + k < kFixDigits)
+      atomicAdd((unsigned long long *)&limbs[pr.d + k], (unsigned long long)pr.part[k]);
+}
+
+// A lane's running exact sum of non-integer values: three limbs from `d`
+// (consecutive values of similar magnitude share them), spilled into the
+// CTA's shared limbs when a value needs other limbs, and at each flush.
+struct LaneFix {
+  long long l0, l1, l2;
+  int d;       // first limb held, -1 when empty
+  double big;  // values of magnitude >= 2^128
+  __device__ void init() {
+    l0 = l1 = l2 = 0;
+    d = -1;
+    big = 0.0;
+  }
+  __device__ void spill(long long *cta) {
+    if (d < 0) return;
+    if (l0) atomicAdd((unsigned long long *)&cta[d], (unsigned long long)l0);
+    if (l1 && d + 1 < kFixDigits) atomicAdd((unsigned long long *)&cta[d + 1], (unsigned long long)l1);
+    if (l2 && d + 2 < kFixDigits) atomicAdd((unsigned long long *)&cta[d + 2], (unsigned long long)l2);
+    l0 = l1 = l2 = 0;
+    d = -1;
+  }
+  __device__ void add(double v, long long *cta) {
+    const FixParts pr = fix_split(v);
+    if (pr.d == -2) {
+      big += v;
+      return;
+    }
+    if (pr.d < 0) return;
+    if (pr.d != d) {
+      spill(cta);
+      d = pr.d;
+    }
+    l0 += pr.part[0];
+    l1 += pr.part[1];
+    l2 += pr.part[2];
+  }
+};
 
 // Where a group key's bytes are (the first line that inserted it).
 struct GroupKeyDesc {
@@ -118,8 +198,6 @@ struct ScanParams {
   RowTile *row_tiles;
   uint8_t *rec_scratch;
   unsigned long long rec_cap_per_cta;
-  // per-tile FP partial sums (fixed-order reduction)
-  double *tile_fsum;
   GroupTable g;
   // deep-nesting scratch, per CTA
   uint32_t *deep_words;
@@ -448,6 +526,43 @@ struct ThreadAgg {
   }
 };
 
+// One-CTA mbarrier (a tile's bulk copy completes on it) and the 1-D bulk
+// (TMA) copy from this GPU's own global memory into shared memory.  The
+// copy is single-CTA, with no cluster multicast.
+constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait rounds before a wait gives up
+
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// Issued by one lane: expects `bytes` (a multiple of 16, src and dst 16-byte
+// aligned) on the barrier, then starts the copy.  The proxy fence orders the
+// warp's earlier generic reads of `dst` before the copy's writes.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint32_t bar) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// Waits (bounded) for the barrier's phase of parity `phase` to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (uint32_t it = 0; it < kWaitLimit; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // 16-byte global -> shared copy that does not go through registers; bytes
 // past `src_bytes` (0..16) are zero-filled and not read.
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
@@ -490,11 +605,13 @@ __device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uin
 
 // Adds the warp's counts and (ungrouped) aggregate to `dst` and clears them;
 // `also` (a batch's totals, may be null) receives the line counts too.
+// The non-integer values' exact sum goes through the CTA's shared limbs
+// `cta_fix` (cleared again) into dst's limbs.
 __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, const DevPlan &P,
-                                          bool rows, int lane,
-                                             unsigned long long &c_lines, unsigned long long &c_blank,
-                                             unsigned long long &c_invalid, unsigned long long &c_type,
-                                             unsigned long long &c_sel, ThreadAgg &agg) {
+                                          bool rows, int lane, unsigned long long &c_lines,
+                                          unsigned long long &c_blank, unsigned long long &c_invalid,
+                                          unsigned long long &c_type, unsigned long long &c_sel,
+                                          ThreadAgg &agg, LaneFix &fx, long long *cta_fix) {
   const unsigned long long nl = warp_sum_u64(c_lines), nb = warp_sum_u64(c_blank),
                            ni = warp_sum_u64(c_invalid), nt = warp_sum_u64(c_type),
                            ns = warp_sum_u64(c_sel);
@@ -529,6 +646,21 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
       mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
     }
     const unsigned int saw = __any_sync(0xffffffffu, agg.saw);
+    if (__any_sync(0xffffffffu, fx.d >= 0 || fx.big != 0.0)) {
+      fx.spill(cta_fix);
+      double big = fx.big;
+      fx.big = 0.0;
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) big += __shfl_down_sync(0xffffffffu, big, d);
+      __syncwarp();
+      if (lane < kFixDigits) {
+        const long long v = cta_fix[lane];
+        cta_fix[lane] = 0;
+        if (v) atomicAdd((unsigned long long *)&dst->fix[lane], (unsigned long long)v);
+      }
+      if (lane == 0 && big != 0.0) atomicAdd(&dst->fbig, big);
+      __syncwarp();
+    }
     if (lane == 0) {
       if (cnt) atomicAdd(&dst->agg_count, cnt);
       if (num) atomicAdd(&dst->agg_numeric, num);
@@ -551,38 +683,6 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
   agg.init();
 }
 
-// Natural-order newline mask of window chunk c (bytes 32c .. 32c+31); bytes
-// at or past `wlen` do not count.  A cheap has-a-newline test runs first;
-// the exact per-byte flags are worked out only for chunks holding one.
-__device__ __forceinline__ uint32_t chunk_newlines(const uint8_t *win, uint32_t c, uint32_t wlen) {
-  const uint4 a = ((const uint4 *)win)[2 * c];
-  const uint4 b = ((const uint4 *)win)[2 * c + 1];
-  const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-  uint32_t any = 0;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    uint32_t t = w[k] ^ 0x0A0A0A0Au;
-    any |= (t - 0x01010101u) & ~t;  // nonzero iff a byte of t is zero (flags above it may be spurious)
-  }
-  if (!(any & 0x80808080u)) return 0;
-  // Exact flags, gathered in a permuted order (bit 8j+k = byte 4k+j), then
-  // put in byte order.
-  uint32_t nl = 0;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    uint32_t t = w[k] ^ 0x0A0A0A0Au;
-    nl |= (~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u) >> (7 - k);
-  }
-  uint32_t nat = 0;
-  while (nl) {
-    uint32_t bit = (uint32_t)__ffs(nl) - 1u;
-    nl &= nl - 1u;
-    nat |= 1u << (((bit & 7u) << 2) | (bit >> 3));
-  }
-  if (wlen - c * 32 < 32) nat &= (1u << (wlen - c * 32)) - 1u;
-  return nat;
-}
-
 // The plan is a kernel parameter (constant bank): fields at fixed offsets
 // are instruction operands, and no plan read goes through global memory.
 // kMulti (aggregates only): a mixed batch, each input with its own plan,
@@ -591,15 +691,16 @@ template <bool kRows, bool kMulti = false>
 __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ __align__(8) unsigned long long s_bar;  // completes each tile's bulk copy
   const DevPlan &P = plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
-  // Shared layout: window bytes (+32 readable bytes past the end for the
-  // walker's word reads), per-32-byte-chunk newline masks, line starts.
-  const uint32_t nchunk_max = (T + H) / 32 + 1;
-  uint8_t *win = smem;                                                 // T + H + 32
-  uint32_t *nlmask = (uint32_t *)(smem + T + H + 32);                  // nchunk_max (+pad)
-  uint16_t *lstart = (uint16_t *)(nlmask + ((nchunk_max + 3) & ~3u));  // kMaxLinesPerPass + 2
-  GroupCache *gcache = (GroupCache *)(smem + scan_smem_base(T, H));     // grouped aggregates only
+  const uint32_t nwords = scan_chunk_words(T, H);
+  uint8_t *win = smem;                                              // window bytes (+ slack)
+  uint32_t *smask = (uint32_t *)(smem + scan_win_bytes(T, H));      // special bytes per chunk
+  uint32_t *nlmask = smask + nwords;                                // newlines per chunk
+  long long *cta_fix = (long long *)(nlmask + nwords);              // the CTA's exact FP sum
+  uint16_t *lstart = (uint16_t *)(cta_fix + kFixDigits);            // kMaxLinesPerPass + 2
+  GroupCache *gcache = (GroupCache *)(smem + scan_smem_base(T, H));  // grouped aggregates only
 
   const int lane = threadIdx.x;
   const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
@@ -608,30 +709,28 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
   DeepStack deep;
   deep.words = sp.deep_words + (unsigned long long)blockIdx.x * (sp.deep_levels_per_cta / 32);
   deep.cap_levels = sp.deep_levels_per_cta;
-  // Lane l lists the newlines of tile chunks [l*K, l*K + K).
-  const uint32_t K = (T / 32 + 31) / 32;
-  const uint32_t c0 = lane * K;
 
   ThreadAgg agg;
   agg.init();
+  LaneFix fx;
+  fx.init();
   unsigned long long c_lines = 0, c_blank = 0, c_invalid = 0, c_type = 0, c_sel = 0;
   unsigned long long cta_recs = 0;  // records this CTA has appended (rows mode)
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
+  if (lane < kFixDigits) cta_fix[lane] = 0;
   const bool grouped = !kRows && (kMulti ? sp.any_grouped != 0 : P.group_slot >= 0);
   if (grouped) {
     for (int k = lane; k < kGroupCache; k += 32) {
       gcache->tag[k] = 0xFFFFFFFFu;
-      GroupAcc z;
-      z.count = z.numeric = z.isum_lo = z.isum_hi = z.n_int = 0;
-      z.min_bits = ~0ull;
-      z.max_bits = 0;
-      z.fsum = 0.0;
-      gcache->acc[k] = z;
+      group_acc_init(gcache->acc[k]);
     }
-    __syncwarp();
   }
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_bar);
+  if (lane == 0) mbar_init(bar);
+  __syncwarp();
+  uint32_t phase = 0;  // parity of the barrier's current phase
 
   // Tickets are taken one tile ahead, so the atomic's latency overlaps a
   // tile's work.
@@ -660,22 +759,35 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, data_end - ts);
     const bool win_reaches_end = ts + wlen == data_end;
 
-    // 1. Stage tile + halo with asynchronous 16-byte copies.
-    const uint32_t n16 = (wlen + 15) >> 4;
-    for (uint32_t k = lane; k < n16; k += 32)
-      cp_async16(win + k * 16, sp.data + ts + k * 16, min(16u, wlen - k * 16));
+    // 1. Stage tile + halo: the window's 16-byte multiple by one bulk copy
+    //    (inputs and tiles start 16-byte aligned), its last 0-15 bytes by
+    //    plain loads, so nothing past the input is read.
+    const uint32_t body = wlen & ~15u;
+    __syncwarp();  // the previous tile's reads of the window are done
+    if (lane == 0 && body) bulk_load(win, sp.data + ts, body, bar);
+    if (lane < (wlen & 15u)) win[body + lane] = sp.data[ts + body + lane];
     const uint32_t prev_nl = (ts == data_start || sp.data[ts - 1] == '\n') ? 1u : 0u;
-    cp_async_wait_all();
+    if (body) {
+      if (!mbar_wait(bar, phase)) {
+        // the copy did not complete within the wait limit: report, give it
+        // another bounded wait (it writes this CTA's shared memory), stop
+        if (lane == 0) atomicOr(&sp.ctr->error, 2u);
+        mbar_wait(bar, phase);
+        return;
+      }
+      phase ^= 1u;
+    }
+    if (lane == 0 && win_reaches_end) win[wlen] = '\n';  // ends the last line for the walker
     __syncwarp();
 
-    if (lane == 0 && win_reaches_end) win[wlen] = '\n';  // ends the last line for the walker
-
-    // 2. Newline masks of the tile's chunks (lane l owns [l*K, l*K + K)),
-    //    counted as they are made; chunks past the tile are classified only
-    //    when the tile's last line is looked for there.
-    const uint32_t nchunks = (wlen + 31) >> 5;
-    const uint32_t tchunks = (tlen + 31) >> 5;
-    const uint32_t nl_limit = tlen ? tlen - 1 : 0;  // newlines below this start a line in the tile
+    // 2. Stage 1, lane-parallel: every 32-byte chunk of the window (the end
+    //    sentinel's too) becomes its special and newline masks; lane l owns
+    //    chunks [l*K, l*K + K) and counts the line starts among them.
+    const uint32_t limit = wlen + (win_reaches_end ? 1u : 0u);  // classified bytes
+    const uint32_t nchunks = (limit + 31) >> 5;
+    const uint32_t K = (nchunks + 31) >> 5;
+    const uint32_t c0 = lane * K;
+    const uint32_t nl_limit = tlen - 1;  // newlines below this start a line in the tile
     auto listed = [&](uint32_t c, uint32_t m) -> uint32_t {
       const uint32_t base = c * 32;
       if (base >= nl_limit) return 0u;
@@ -686,10 +798,20 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     unsigned long long nz = 0;  // bit k: chunk c0 + k lists a line start
     for (uint32_t k = 0; k < K; k++) {
       const uint32_t c = c0 + k;
-      if (c >= tchunks) break;
-      const uint32_t m = chunk_newlines(win, c, wlen);
-      nlmask[c] = m;
-      const uint32_t lm = listed(c, m);
+      if (c >= nchunks) break;
+      const uint4 u = ((const uint4 *)win)[2 * c];
+      const uint4 v = ((const uint4 *)win)[2 * c + 1];
+      const uint32_t w8[8] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w};
+      uint32_t sm_c;
+      uint32_t nl_c = classify_chunk(w8, &sm_c);
+      const uint32_t rem = limit - c * 32;
+      if (rem < 32) {  // bytes past the window's data are stale
+        sm_c &= (1u << rem) - 1u;
+        nl_c &= (1u << rem) - 1u;
+      }
+      smask[c] = sm_c;
+      nlmask[c] = nl_c;
+      const uint32_t lm = listed(c, nl_c);
       if (lm) {
         my_nl += __popc(lm);
         nz |= 1ull << k;
@@ -707,7 +829,6 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     // 4. Walk the lines, one per lane, in passes of the list's capacity.
     unsigned long long tile_rows = 0, tile_bytes = 0;
     const unsigned long long tile_rec0 = cta_recs;
-    double fsum_lane = 0.0;
     uint32_t tile_first_invalid = 0xFFFFFFFFu, tile_first_type = 0xFFFFFFFFu;
     for (uint32_t base = 0; base < n_lines_tile; base += kMaxLinesPerPass) {
       const uint32_t cnt = min(n_lines_tile - base, kMaxLinesPerPass);
@@ -750,23 +871,21 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
             // the pass for exactly this)
             e = (uint32_t)lstart[li + 1] - 1;
           } else {
-            // last line of the tile: its newline is at or after te - 1
-            uint32_t q = tlen ? tlen - 1 : 0;
+            // last line of the tile: its newline is at or after te - 1 (the
+            // sentinel's, when the window reaches the data's end)
+            uint32_t q = tlen - 1;
             if (q < s) q = s;
             uint32_t c = q >> 5;
-            uint32_t m = (c < tchunks ? nlmask[c] : chunk_newlines(win, c, wlen)) &
-                         (0xFFFFFFFFu << (q & 31));
-            while (!m && ++c < nchunks) m = c < tchunks ? nlmask[c] : chunk_newlines(win, c, wlen);
-            q = m ? c * 32 + (uint32_t)__ffs(m) - 1 : wlen;
-            if (q < wlen) e = q;
-            else if (win_reaches_end) e = wlen;
+            uint32_t m = c < nchunks ? (nlmask[c] & (0xFFFFFFFFu << (q & 31))) : 0u;
+            while (!m && ++c < nchunks) m = nlmask[c];
+            if (m) e = c * 32 + (uint32_t)__ffs(m) - 1;
             else found = false;
           }
           line_abs = ts + s;
           if (found) {
             lp = win + s;
             line_len = e - s;
-            status = walk_window(P, win, s, e, nv);
+            status = walk_masked(P, win, smask, s, e, nv);
           } else {
             // longer than the window: walk it from global memory
             unsigned long long q = ts + wlen;
@@ -882,7 +1001,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
               agg.add_int(iv);
               agg.n_int++;
             } else {
-              fsum_lane += fv;
+              fx.add(fv, cta_fix);
             }
           }
         }
@@ -929,7 +1048,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
                 if (hi) atomicAdd(&a.isum_hi, hi);
                 atomicAdd(&a.n_int, 1ull);
               } else {
-                atomicAdd(&a.fsum, fv);
+                fix_atomic_add(a.fix, &a.fbig, fv);
               }
             } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0) {
               sp.g.keys[kid].saw_non_numeric = 1;
@@ -994,16 +1113,11 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
         rt.pad = 0;
         sp.row_tiles[tile] = rt;
       }
-    } else {
-      // fixed-order tree over the lanes
-      double f = fsum_lane;
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) f += __shfl_down_sync(0xffffffffu, f, d);
-      if (lane == 0) sp.tile_fsum[tile] = f;
     }
     // A batch input's counts and aggregate go to its own record, tile by tile.
     if (sp.tile_input)
-      flush_counts(ctr_in, sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
+      flush_counts(ctr_in, sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, fx,
+                   cta_fix);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
@@ -1026,74 +1140,76 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
         if (c.isum_hi + carry) atomicAdd(&a.isum_hi, c.isum_hi + carry);
         atomicAdd(&a.n_int, c.n_int);
       }
-      if (c.numeric > c.n_int) atomicAdd(&a.fsum, c.fsum);
+      if (c.numeric > c.n_int) {
+        for (int d = 0; d < kFixDigits; d++)
+          if (c.fix[d]) atomicAdd((unsigned long long *)&a.fix[d], (unsigned long long)c.fix[d]);
+        if (c.fbig != 0.0) atomicAdd(&a.fbig, c.fbig);
+      }
     }
   }
 
   // Flush this CTA's counters (a batch's were flushed per tile).
-  flush_counts(sp.ctr, nullptr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg);
+  flush_counts(sp.ctr, nullptr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, fx,
+               cta_fix);
 }
 
-// Fixed-order reduction of the per-tile FP partials (pass 1: contiguous
-// blocks; pass 2: one CTA over the block partials), plus the first invalid
-// line index.
-__global__ void k_reduce_tiles(const double *tile_fsum, unsigned long long n_tiles,
-                               double *block_out, const TileDesc *tiles, RunCounters *ctr,
+// The index of the first invalid / type-error line: lines of the tiles
+// before the first tile holding one, summed in two passes (contiguous blocks
+// of tiles, then one warp over the block sums).
+__global__ void k_reduce_tiles(unsigned long long n_tiles, const TileDesc *tiles, RunCounters *ctr,
                                unsigned long long *block_lines) {
-  __shared__ double s_f[kReduceThreads];
   __shared__ unsigned long long s_l[kReduceThreads], s_t[kReduceThreads];
   unsigned long long per = (n_tiles + gridDim.x - 1) / gridDim.x;
   unsigned long long b0 = blockIdx.x * per, b1 = min(b0 + per, n_tiles);
   unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
-  double f = 0.0;
   unsigned long long lines = 0, lines_t = 0;
   unsigned long long chunk = (b1 > b0 ? b1 - b0 : 0);
   unsigned long long cper = (chunk + kReduceThreads - 1) / kReduceThreads;
   unsigned long long c0 = b0 + threadIdx.x * cper, c1 = min(c0 + cper, b1);
-  for (unsigned long long t = c0; t < c1; t++) {
-    if (tile_fsum) f += tile_fsum[t];
+  for (unsigned long long t = c0; t < c1 && (t < cut || t < cut_t); t++) {
     if (t < cut) lines += tiles[t].n_lines;
     if (t < cut_t) lines_t += tiles[t].n_lines;
   }
-  s_f[threadIdx.x] = f;
   s_l[threadIdx.x] = lines;
   s_t[threadIdx.x] = lines_t;
   __syncthreads();
   for (int d = kReduceThreads / 2; d > 0; d >>= 1) {
     if (threadIdx.x < d) {
-      s_f[threadIdx.x] += s_f[threadIdx.x + d];
       s_l[threadIdx.x] += s_l[threadIdx.x + d];
       s_t[threadIdx.x] += s_t[threadIdx.x + d];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    block_out[blockIdx.x] = s_f[0];
     block_lines[2 * blockIdx.x] = s_l[0];
     block_lines[2 * blockIdx.x + 1] = s_t[0];
   }
 }
 
-// One warp: lane l sums block partials l, l+32, ... in order, then a fixed
-// shuffle tree combines the lanes (the same order on every run).
-__global__ void k_finalize(const double *block_f, const unsigned long long *block_lines,
-                           unsigned nblocks, const TileDesc *tiles, RunCounters *ctr) {
+// The run's FP totals from its exact limbs (the integer sum joins them
+// before the one rounding of sum_total).
+__device__ __forceinline__ void finalize_sums(RunCounters &c) {
+  c.fsum_total = fix_to_double(c.fix, 0, 0) + c.fbig;
+  c.sum_total = fix_to_double(c.fix, c.agg_isum_lo, c.agg_isum_hi) + c.fbig;
+}
+
+// One warp: the block sums of k_reduce_tiles, then the first bad lines and
+// the FP totals.
+__global__ void k_finalize(const unsigned long long *block_lines, unsigned nblocks, const TileDesc *tiles,
+                           RunCounters *ctr) {
   const int lane = threadIdx.x;
-  double f = 0.0;
   unsigned long long lines = 0, lines_t = 0;
   for (unsigned b = lane; b < nblocks; b += 32) {
-    f += block_f[b];
     lines += block_lines[2 * b];
     lines_t += block_lines[2 * b + 1];
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) {
-    f += __shfl_down_sync(0xffffffffu, f, d);
     lines += __shfl_down_sync(0xffffffffu, lines, d);
     lines_t += __shfl_down_sync(0xffffffffu, lines_t, d);
   }
   if (lane != 0) return;
-  ctr->fsum_total = f;
+  finalize_sums(*ctr);
   unsigned long long cut = ctr->first_invalid_tile, cut_t = ctr->first_type_tile;
   ctr->first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
   ctr->first_type_error = cut_t == ~0ull ? ~0ull : lines_t + tiles[cut_t].first_type_error;
@@ -1113,12 +1229,11 @@ __global__ void k_batch_reset(RunCounters *in_ctr, uint32_t n_inputs) {
   }
 }
 
-// Batched runs, one warp per input: the input's FP sum over its tiles (lane l
-// sums a contiguous slice in order, then a fixed shuffle tree) and its first
-// invalid / type-error line.
-__global__ void k_batch_finalize(const double *tile_fsum, const TileDesc *tiles,
-                                 const unsigned long long *in_tile0, RunCounters *in_ctr,
-                                 uint32_t n_inputs) {
+// Batched runs, one warp per input: the input's first invalid / type-error
+// line (lane l sums a contiguous slice of the input's tiles' line counts)
+// and its FP totals.
+__global__ void k_batch_finalize(const TileDesc *tiles, const unsigned long long *in_tile0,
+                                 RunCounters *in_ctr, uint32_t n_inputs) {
   const int lane = threadIdx.x & 31;
   const unsigned long long i = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= n_inputs) return;  // uniform per warp
@@ -1127,21 +1242,18 @@ __global__ void k_batch_finalize(const double *tile_fsum, const TileDesc *tiles,
   const unsigned long long cut = c.first_invalid_tile, cut_t = c.first_type_tile;
   const unsigned long long per = (t1 - t0 + 31) / 32;
   const unsigned long long a = min(t0 + lane * per, t1), b = min(a + per, t1);
-  double f = 0.0;
   unsigned long long lines = 0, lines_t = 0;
-  for (unsigned long long t = a; t < b; t++) {
-    if (tile_fsum) f += tile_fsum[t];
+  for (unsigned long long t = a; t < b && (t < cut || t < cut_t); t++) {
     if (t < cut) lines += tiles[t].n_lines;
     if (t < cut_t) lines_t += tiles[t].n_lines;
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) {
-    f += __shfl_down_sync(0xffffffffu, f, d);
     lines += __shfl_down_sync(0xffffffffu, lines, d);
     lines_t += __shfl_down_sync(0xffffffffu, lines_t, d);
   }
   if (lane != 0) return;
-  c.fsum_total = f;
+  finalize_sums(c);
   c.first_invalid = cut == ~0ull ? ~0ull : lines + tiles[cut].first_invalid;
   c.first_type_error = cut_t == ~0ull ? ~0ull : lines_t + tiles[cut_t].first_type_error;
 }

@@ -60,9 +60,7 @@ constexpr unsigned kNoAllocReduceBlocks = 256;
 constexpr uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
 constexpr uint64_t kOffCtr = 0;
 constexpr uint64_t kOffTiles = align256(kOffCtr + sizeof(RunCounters));
-constexpr uint64_t kOffFsum = align256(kOffTiles + kNoAllocMaxTiles * sizeof(TileDesc));
-constexpr uint64_t kOffBlockF = align256(kOffFsum + kNoAllocMaxTiles * sizeof(double));
-constexpr uint64_t kOffBlockLines = align256(kOffBlockF + kNoAllocReduceBlocks * sizeof(double));
+constexpr uint64_t kOffBlockLines = align256(kOffTiles + kNoAllocMaxTiles * sizeof(TileDesc));
 constexpr uint64_t kOffDeep =
     align256(kOffBlockLines + 2 * kNoAllocReduceBlocks * sizeof(unsigned long long));
 constexpr uint64_t kScratchBytes =
@@ -149,12 +147,10 @@ __global__ void k_noalloc_result(const RunCounters *ctr, warpjq_noalloc_result *
   r.isum_lo = c.agg_isum_lo;
   r.isum_hi = c.agg_isum_hi;
   r.n_int = c.agg_n_int;
-  r.fsum = c.fsum_total;
+  r.fsum = c.fsum_total;  // exact sums rounded once (fixsum.cuh)
   r.min = c.agg_numeric ? from_order_bits(c.agg_min_bits) : __longlong_as_double(0x7FF0000000000000ll);
   r.max = c.agg_numeric ? from_order_bits(c.agg_max_bits) : -__longlong_as_double(0x7FF0000000000000ll);
-  // isum as a double: exact while |isum| < 2^53, rounded twice beyond.
-  double isum = (double)(long long)c.agg_isum_hi * 18446744073709551616.0 + (double)c.agg_isum_lo;
-  r.sum = (c.agg_n_int ? isum : 0.0) + c.fsum_total;
+  r.sum = c.sum_total;
   r.saw_non_numeric = c.agg_saw_non_numeric;
   r.status = (c.overflow || c.error) ? 1u : 0u;
   *out = r;
@@ -206,8 +202,6 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
   unsigned char *base = s->scratch;
   RunCounters *ctr = (RunCounters *)(base + kOffCtr);
   TileDesc *tiles = (TileDesc *)(base + kOffTiles);
-  double *tile_fsum = (double *)(base + kOffFsum);
-  double *block_f = (double *)(base + kOffBlockF);
   unsigned long long *block_lines = (unsigned long long *)(base + kOffBlockLines);
   uint32_t *deep = (uint32_t *)(base + kOffDeep);
 
@@ -228,7 +222,6 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     sp.n_tiles = n_tiles;
     sp.ctr = ctr;
     sp.tiles = tiles;
-    sp.tile_fsum = tile_fsum;
     sp.deep_words = deep;
     sp.deep_levels_per_cta = kNoAllocDeepLevels;
     unsigned grid = (unsigned)(n_tiles < s->grid ? n_tiles : s->grid);
@@ -238,12 +231,12 @@ extern "C" warpjq_status warpjq_aggregate_noalloc(const warpjq_program *prog, co
     }
     if (e == cudaSuccess) {
       unsigned nb = kNoAllocReduceBlocks;
-      void *args[] = {&tile_fsum, &n_tiles, &block_f, &tiles, &ctr, &block_lines};
+      void *args[] = {&n_tiles, &tiles, &ctr, &block_lines};
       e = cudaLaunchKernel((const void *)k_reduce_tiles, dim3(nb), dim3(kReduceThreads), args, 0, st);
     }
     if (e == cudaSuccess) {
       unsigned nb = kNoAllocReduceBlocks;
-      void *args[] = {&block_f, &block_lines, &nb, &tiles, &ctr};
+      void *args[] = {&block_lines, &nb, &tiles, &ctr};
       e = cudaLaunchKernel((const void *)k_finalize, dim3(1), dim3(32), args, 0, st);
     }
   }

@@ -125,7 +125,12 @@ struct RunCounters {
   unsigned int n_keys;
   unsigned int overflow;     // bit0 records, bit1 output, bit2 groups, bit3 deep stack
   unsigned int error;        // nonzero: a kernel found its own state inconsistent
-  double fsum_total;         // written by the finalize kernel
+  // exact sum of the non-integer aggregate values (fixsum.cuh): limb k
+  // counts units of 2^(32 k - 128); values of magnitude >= 2^128 go to fbig
+  long long fix[8];
+  double fbig;
+  double fsum_total;         // written by the finalize kernel: the rounded fix sum + fbig
+  double sum_total;          // written by the finalize kernel: integer + fix sums rounded once, + fbig
   unsigned long long first_invalid;     // written by the finalize kernel
   unsigned long long first_type_error;  // written by the finalize kernel
 };

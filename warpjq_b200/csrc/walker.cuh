@@ -336,16 +336,6 @@ __device__ __forceinline__ uint32_t load4(const uint8_t *w, uint32_t i) {
   return __funnelshift_r(p[0], p[1], (i & 3u) * 8u);
 }
 
-// 0x80 in the byte lanes of `x` holding '"', '\\' or a byte below 0x20.  The
-// lowest flagged lane is exact; lanes above a flagged lane may be flagged
-// spuriously (a borrow), which callers check for.
-__device__ __forceinline__ uint32_t str_special(uint32_t x) {
-  uint32_t q = x ^ 0x22222222u;
-  uint32_t b = x ^ 0x5C5C5C5Cu;
-  return (((q - 0x01010101u) & ~q) | ((b - 0x01010101u) & ~b) | ((x - 0x20202020u) & ~x)) &
-         0x80808080u;
-}
-
 // Number of ASCII digits starting at w[j]; `term` receives the byte after
 // them.
 __device__ __forceinline__ uint32_t digit_run(const uint8_t *w, uint32_t j, uint32_t &term) {
@@ -370,76 +360,34 @@ __device__ __forceinline__ bool simple_escape(uint32_t e) {
 
 // Closing quote of the string opened at w[i], or 0 when the string is
 // malformed (a bad escape, a raw control byte) or reaches the newline.
-// `esc` reports whether the body holds a backslash.  Ordinary bytes are
-// skipped four at a time up to a 16-byte boundary, then 32 at a time; the
-// byte that stops a step is taken from the loaded word.
-__device__ __forceinline__ uint32_t win_string(const uint8_t *w, uint32_t i, bool &esc) {
+// `esc` reports whether the body holds a backslash.  `sm` has one bit per
+// window byte that is '"', '\\' or below 0x20 (the stage-1 special mask), so
+// the scan jumps from one such byte to the next: ordinary bytes are never
+// looked at.  The line's own newline is such a byte, so no search passes
+// it: every escape that moves past a byte has checked that byte first.
+__device__ __forceinline__ uint32_t mask_string(const uint8_t *w, const uint32_t *sm, uint32_t i,
+                                                bool &esc) {
   uint32_t p = i + 1;
   esc = false;
   for (;;) {
-    uint32_t wa = p & ~3u;
-    uint32_t x = *(const uint32_t *)(w + wa);
-    uint32_t f = str_special(x) & (0xFFFFFFFFu << ((p & 3u) * 8u));
-    if (!f) {
-      wa += 4;
-      while (wa & 15u) {
-        x = *(const uint32_t *)(w + wa);
-        f = str_special(x);
-        if (f) break;
-        wa += 4;
-      }
-      while (!f) {
-        const uint4 u = *(const uint4 *)(w + wa);
-        const uint4 v = *(const uint4 *)(w + wa + 16);
-        const uint32_t f0 = str_special(u.x), f1 = str_special(u.y), f2 = str_special(u.z),
-                       f3 = str_special(u.w);
-        const uint32_t f4 = str_special(v.x), f5 = str_special(v.y), f6 = str_special(v.z),
-                       f7 = str_special(v.w);
-        if (f0 | f1 | f2 | f3) {
-          if (f0) {
-            f = f0; x = u.x;
-          } else if (f1) {
-            f = f1; x = u.y; wa += 4;
-          } else if (f2) {
-            f = f2; x = u.z; wa += 8;
-          } else {
-            f = f3; x = u.w; wa += 12;
-          }
-        } else if (f4 | f5 | f6 | f7) {
-          if (f4) {
-            f = f4; x = v.x; wa += 16;
-          } else if (f5) {
-            f = f5; x = v.y; wa += 20;
-          } else if (f6) {
-            f = f6; x = v.z; wa += 24;
-          } else {
-            f = f7; x = v.w; wa += 28;
-          }
-        } else {
-          wa += 32;
-        }
-      }
-    }
-    const uint32_t sh = ((uint32_t)__ffs(f) - 1u) & ~7u;
-    p = wa + (sh >> 3);
-    const uint32_t c = (x >> sh) & 0xFFu;
+    uint32_t k = p >> 5;
+    uint32_t m = sm[k] & (0xFFFFFFFFu << (p & 31u));
+    while (!m) m = sm[++k];
+    p = (k << 5) + (uint32_t)__ffs(m) - 1u;
+    const uint32_t c = w[p];
     if (c == '"') return p;
-    if (c == '\\') {
-      esc = true;
-      uint32_t e = w[p + 1];
-      if (e == 'u') {
-        if (hex_val(w[p + 2]) < 0 || hex_val(w[p + 3]) < 0 || hex_val(w[p + 4]) < 0 ||
-            hex_val(w[p + 5]) < 0)
-          return 0;
-        p += 6;
-      } else {
-        if (!simple_escape(e)) return 0;
-        p += 2;
-      }
-      continue;
+    if (c != '\\') return 0;  // a byte below 0x20
+    esc = true;
+    const uint32_t e = w[p + 1];
+    if (e == 'u') {
+      if (hex_val(w[p + 2]) < 0 || hex_val(w[p + 3]) < 0 || hex_val(w[p + 4]) < 0 ||
+          hex_val(w[p + 5]) < 0)
+        return 0;
+      p += 6;
+    } else {
+      if (!simple_escape(e)) return 0;
+      p += 2;
     }
-    if (c < 0x20) return 0;
-    p++;  // a spurious flag above a masked-off lane
   }
 }
 
@@ -496,10 +444,12 @@ __device__ __forceinline__ uint8_t match_key_win(const DevPlan &P, uint8_t node,
 }  // namespace detail
 
 // Walks the line w[s, e) of a window.  w must be 4-byte aligned, w[e] must
-// be '\n' and the 32 bytes after it readable.  Offsets recorded in `v` are
-// relative to s.  Lines nesting past 64 levels return LS_DEEP.
-__device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, uint32_t s,
-                                           uint32_t e, NodeVals &v) {
+// be '\n' and the 32 bytes after it readable; `sm` is the window's special
+// mask (bit j of sm[j / 32]: byte j is '"', '\\' or below 0x20), complete at
+// least up to e.  Offsets recorded in `v` are relative to s.  Lines nesting
+// past 64 levels return LS_DEEP.
+__device__ __forceinline__ int walk_masked(const DevPlan &P, const uint8_t *w, const uint32_t *sm,
+                                           uint32_t s, uint32_t e, NodeVals &v) {
   using namespace detail;
   const uint32_t n_nodes = P.n_nodes;
   for (uint32_t k = 0; k < n_nodes; k++) v.kind[k] = JK_MISSING;
@@ -532,7 +482,7 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
     if (want_key) {
       if (c != '"') return LS_INVALID;
       bool esc;
-      const uint32_t q = win_string(w, i, esc);
+      const uint32_t q = mask_string(w, sm, i, esc);
       if (!q) return LS_INVALID;
       vn = kNoNode;
       if (cur_lm) {
@@ -588,7 +538,7 @@ __device__ __forceinline__ int walk_window(const DevPlan &P, const uint8_t *w, u
       uint32_t j;
       if (c == '"') {
         bool esc;
-        j = win_string(w, i, esc);
+        j = mask_string(w, sm, i, esc);
         if (!j) return LS_INVALID;
         j++;
         if (vn != kNoNode) v.esc[vn] = esc;

@@ -257,8 +257,12 @@ def _host_bytes(rows) -> bytes:
 
 
 def _sum(isum: int, n_int: int, fsum: float) -> float:
-    # the device's rounding: the exact integer sum to FP64, plus the FP sum
-    return (float(isum) if n_int else 0.0) + fsum
+    # the device's rounding: the integer sum and the FP sum added exactly,
+    # then rounded once
+    from fractions import Fraction
+    if not math.isfinite(fsum):
+        return float(isum) + fsum
+    return float(Fraction(isum) + Fraction(fsum))
 
 
 def render(query: str, merged: Partial, fmt: str = "ndjson") -> bytes:
