@@ -46,8 +46,10 @@ constexpr uint32_t kWinSlack = 64;
 
 // Shared-memory layout of k_scan for tile T and halo H: the window bytes,
 // then the special and newline masks (one word per 32-byte chunk, the
-// sentinel's chunk included), the CTA's exact FP sum, the line-start list,
-// and for grouped aggregates the group cache.
+// sentinel's chunk included), the CTA's exact FP sum, the mbarrier the
+// tile copies complete on, the line-start list, and for grouped aggregates
+// the group cache.  Nothing is static, so the dynamic size may be raised
+// to the device's whole opt-in limit.
 __host__ __device__ inline uint32_t scan_win_bytes(uint32_t T, uint32_t H) {
   return (T + H + kWinSlack + 15u) & ~15u;
 }
@@ -58,6 +60,7 @@ __host__ __device__ inline size_t scan_smem_base(uint32_t T, uint32_t H) {
   size_t s = scan_win_bytes(T, H);
   s += 2 * (size_t)scan_chunk_words(T, H) * sizeof(uint32_t);
   s += kFixDigits * sizeof(long long);
+  s += sizeof(unsigned long long);  // the mbarrier of the tile copies
   s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
   return (s + 15) & ~(size_t)15;
 }
@@ -691,7 +694,6 @@ template <bool kRows, bool kMulti = false>
 __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
-  __shared__ __align__(8) unsigned long long s_bar;  // completes each tile's bulk copy
   const DevPlan &P = plan;
   const uint32_t T = sp.tile_bytes, H = sp.halo_bytes;
   const uint32_t nwords = scan_chunk_words(T, H);
@@ -699,7 +701,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
   uint32_t *smask = (uint32_t *)(smem + scan_win_bytes(T, H));      // special bytes per chunk
   uint32_t *nlmask = smask + nwords;                                // newlines per chunk
   long long *cta_fix = (long long *)(nlmask + nwords);              // the CTA's exact FP sum
-  uint16_t *lstart = (uint16_t *)(cta_fix + kFixDigits);            // kMaxLinesPerPass + 2
+  unsigned long long *s_bar = (unsigned long long *)(cta_fix + kFixDigits);  // tile copies' mbarrier
+  uint16_t *lstart = (uint16_t *)(s_bar + 1);                       // kMaxLinesPerPass + 2
   GroupCache *gcache = (GroupCache *)(smem + scan_smem_base(T, H));  // grouped aggregates only
 
   const int lane = threadIdx.x;
@@ -727,7 +730,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
       group_acc_init(gcache->acc[k]);
     }
   }
-  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_bar);
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(s_bar);
   if (lane == 0) mbar_init(bar);
   __syncwarp();
   uint32_t phase = 0;  // parity of the barrier's current phase
