@@ -43,7 +43,8 @@ extern "C" {
 // walk_line; mode 1: the window walker walk_masked, with the line copied at
 // a varying offset into a window whose bytes past the newline are quotes,
 // backslashes and digits, and the window's special mask made by the
-// kernel's chunk classifier):
+// kernel's chunk classifier; mode 2: as mode 1, with the object fast path
+// walk_objects tried first, as the scan kernel does):
 //   blank | invalid | type | filtered | selected<TAB>kind:raw<TAB>...
 // Returns 0, or 2 for a query error, 3 for a plan error.
 int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char **out,
@@ -69,7 +70,7 @@ int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char *
     uint32_t n = (uint32_t)(end - pos);
     pos = end + 1;
     int st;
-    if (mode == 1) {
+    if (mode == 1 || mode == 2) {
       // the line at a varying offset (across 32-byte chunk boundaries), its
       // newline, then quotes, backslashes and digits; the special mask of
       // the whole window is made by the kernel's own chunk classifier
@@ -83,7 +84,8 @@ int wh_eval(const char *query, const uint8_t *data, size_t len, int mode, char *
       smask.assign(W / 32 + 1, 0);
       for (uint32_t c = 0; c < W / 32; c++) classify_chunk(winbuf.data() + 8 * c, &smask[c]);
       line = w + s;
-      st = walk_masked(P, w, smask.data(), s, s + n, nv);
+      st = mode == 2 ? walk_objects(P, w, smask.data(), s, s + n, nv) : LS_FALLBACK;
+      if (st == LS_FALLBACK) st = walk_masked(P, w, smask.data(), s, s + n, nv);
     } else {
       st = walk_line(P, line, n, nv, nullptr);
     }

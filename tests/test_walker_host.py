@@ -1,5 +1,5 @@
 """The device line walkers (the bounded walk_line and the window walker
-walk_masked) and evaluator (warpjq_b200/csrc/walker.cuh), compiled for the
+walk_masked, with its object fast path walk_objects) and evaluator (warpjq_b200/csrc/walker.cuh), compiled for the
 host, against the oracle's per-line semantics
 (exec/cpu.rs:299-371): same verdict per line -- blank, invalid, type error,
 filtered, selected -- and, for selected lines, the same resolved value of
@@ -52,7 +52,7 @@ def check(harness, data, queries, label):
     L, o = harness
     for q in queries:
         ref = _run(o.oracle_eval_lines, o.oracle_free, q, data)
-        for mode, name in ((0, "walk_line"), (1, "walk_masked")):
+        for mode, name in ((0, "walk_line"), (1, "walk_masked"), (2, "walk_objects")):
             dev = _run(L.wh_eval, L.wh_free, q, data, mode)
             assert len(dev) == len(ref), (label, q, name)
             for i, (a, b) in enumerate(zip(dev, ref)):
@@ -146,3 +146,30 @@ def test_walker_on_mutated_lines(harness):
     data = b"\n".join(lines) + b"\n"
     check(harness, data, [".", ".a", ".status", "select(.a)", '{a: .a, b: .b}', ".arr[1]",
                           ".nested.deep.v"], "mutated")
+
+
+def test_walker_on_the_benchmark_schemas(harness):
+    """The object fast path's common shapes: nginx-style lines (escaped
+    quotes and backslashes in ua) and the nested schema (objects 3-5 deep,
+    \\u escapes, malformed lines), as generated and with random edits, under
+    the benchmark queries."""
+    import random
+    import warpjq_b200 as wjq
+    nb, nu, _ = wjq.gen_nginx(400_000, seed=4)
+    sb, su, _ = wjq.gen_nested(400_000, seed=4, n_users=1000)
+    nginx = bytes(nb[:nu]).split(b"\n")[:-1]
+    nested = bytes(sb[:su]).split(b"\n")[:-1]
+    rng = random.Random(23)
+    mutated = []
+    for _ in range(2000):
+        b = bytearray(rng.choice(nginx + nested))
+        at = rng.randrange(len(b))
+        b[at] = rng.choice(b'"\\{}[]:, \x01ua0')
+        mutated.append(bytes(b).replace(b"\n", b" "))
+    check(harness, b"\n".join(nginx + mutated) + b"\n",
+          ["select(.status == 500) | count", "select(.status >= 500) | {p: .path, b: .bytes}",
+           "group_by(.host) | sum(.bytes)", ".ua", "select(.latency_ms > 50) | .method"], "nginx")
+    check(harness, b"\n".join(nested + mutated) + b"\n",
+          ['select(.req.user.tier == "gold" and .resp.code != 200) | {u: .req.user.id, l: .resp.latency}',
+           "group_by(.req.user.id) | avg(.resp.latency)", ".req.path", ".meta.trace.span",
+           "select(.req.user.geo.cc == \"jp\") | {c: .req.user.geo, m: .req.method}"], "nested")

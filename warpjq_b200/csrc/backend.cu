@@ -227,6 +227,8 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
      "cudaFuncSetAttribute(scan rows)");
   CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan agg)");
+  CK(cudaFuncSetAttribute(k_scan<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
+     "cudaFuncSetAttribute(scan grouped)");
   CK(cudaFuncSetAttribute(k_scan<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan mixed)");
   int a = 0, b = 0;
@@ -234,7 +236,10 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
      "occupancy");
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scan<false>, kThreads, c->scan_smem),
      "occupancy");
-  per_sm = std::max(1, std::min(a, b));
+  int g = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, k_scan<false, false, true>, kThreads, c->scan_smem),
+     "occupancy");
+  per_sm = std::max(1, std::min(a, std::min(b, g)));
   c->grid = (unsigned)(c->num_sms * per_sm);
   return WARPJQ_OK;
 }
@@ -386,6 +391,8 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
           sp, c->plan);
     else if (P.needs_rows)
       k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
+    else if (groups)
+      k_scan<false, false, true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     else
       k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     s.kernels++;

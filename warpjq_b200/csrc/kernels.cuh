@@ -111,43 +111,6 @@ __device__ __forceinline__ void fix_atomic_add(long long *limbs, double *big, do
       atomicAdd((unsigned long long *)&limbs[pr.d + k], (unsigned long long)pr.part[k]);
 }
 
-// A lane's running exact sum of non-integer values: three limbs from `d`
-// (consecutive values of similar magnitude share them), spilled into the
-// CTA's shared limbs when a value needs other limbs, and at each flush.
-struct LaneFix {
-  long long l0, l1, l2;
-  int d;       // first limb held, -1 when empty
-  double big;  // values of magnitude >= 2^128
-  __device__ void init() {
-    l0 = l1 = l2 = 0;
-    d = -1;
-    big = 0.0;
-  }
-  __device__ void spill(long long *cta) {
-    if (d < 0) return;
-    if (l0) atomicAdd((unsigned long long *)&cta[d], (unsigned long long)l0);
-    if (l1 && d + 1 < kFixDigits) atomicAdd((unsigned long long *)&cta[d + 1], (unsigned long long)l1);
-    if (l2 && d + 2 < kFixDigits) atomicAdd((unsigned long long *)&cta[d + 2], (unsigned long long)l2);
-    l0 = l1 = l2 = 0;
-    d = -1;
-  }
-  __device__ void add(double v, long long *cta) {
-    const FixParts pr = fix_split(v);
-    if (pr.d == -2) {
-      big += v;
-      return;
-    }
-    if (pr.d < 0) return;
-    if (pr.d != d) {
-      spill(cta);
-      d = pr.d;
-    }
-    l0 += pr.part[0];
-    l1 += pr.part[1];
-    l2 += pr.part[2];
-  }
-};
-
 // Where a group key's bytes are (the first line that inserted it).
 struct GroupKeyDesc {
   unsigned long long off;  // absolute input offset of the key bytes (string: body)
@@ -513,7 +476,8 @@ __device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
 // ---------------------------------------------------------------------------
 
 struct ThreadAgg {
-  unsigned long long count, numeric, isum_lo, isum_hi, n_int, min_bits, max_bits;
+  uint32_t count, numeric, n_int;  // a lane's counts (flushed per CTA, or per tile in a batch)
+  unsigned long long isum_lo, isum_hi, min_bits, max_bits;
   unsigned int saw;
   __device__ void init() {
     count = numeric = isum_lo = isum_hi = n_int = 0;
@@ -550,6 +514,12 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
+}
+
+// Hint: bring `bytes` (a multiple of 16, src 16-byte aligned) of this GPU's
+// global memory into L2; nothing waits for it.
+__device__ __forceinline__ void l2_prefetch(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
 }
 
 // Waits (bounded) for the barrier's phase of parity `phase` to complete.
@@ -608,13 +578,12 @@ __device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uin
 
 // Adds the warp's counts and (ungrouped) aggregate to `dst` and clears them;
 // `also` (a batch's totals, may be null) receives the line counts too.
-// The non-integer values' exact sum goes through the CTA's shared limbs
-// `cta_fix` (cleared again) into dst's limbs.
+// The non-integer values' exact sum, gathered in the CTA's shared limbs
+// `cta_fix`, goes into dst's limbs (and the shared limbs are cleared).
 __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, const DevPlan &P,
-                                          bool rows, int lane, unsigned long long &c_lines,
-                                          unsigned long long &c_blank, unsigned long long &c_invalid,
-                                          unsigned long long &c_type, unsigned long long &c_sel,
-                                          ThreadAgg &agg, LaneFix &fx, long long *cta_fix) {
+                                          bool rows, int lane, uint32_t &c_lines, uint32_t &c_blank,
+                                          uint32_t &c_invalid, uint32_t &c_type, uint32_t &c_sel,
+                                          ThreadAgg &agg, long long *cta_fix) {
   const unsigned long long nl = warp_sum_u64(c_lines), nb = warp_sum_u64(c_blank),
                            ni = warp_sum_u64(c_invalid), nt = warp_sum_u64(c_type),
                            ns = warp_sum_u64(c_sel);
@@ -649,21 +618,13 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
       mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
     }
     const unsigned int saw = __any_sync(0xffffffffu, agg.saw);
-    if (__any_sync(0xffffffffu, fx.d >= 0 || fx.big != 0.0)) {
-      fx.spill(cta_fix);
-      double big = fx.big;
-      fx.big = 0.0;
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) big += __shfl_down_sync(0xffffffffu, big, d);
-      __syncwarp();
-      if (lane < kFixDigits) {
-        const long long v = cta_fix[lane];
-        cta_fix[lane] = 0;
-        if (v) atomicAdd((unsigned long long *)&dst->fix[lane], (unsigned long long)v);
-      }
-      if (lane == 0 && big != 0.0) atomicAdd(&dst->fbig, big);
-      __syncwarp();
+    __syncwarp();
+    if (lane < kFixDigits) {
+      const long long v = cta_fix[lane];
+      cta_fix[lane] = 0;
+      if (v) atomicAdd((unsigned long long *)&dst->fix[lane], (unsigned long long)v);
     }
+    __syncwarp();
     if (lane == 0) {
       if (cnt) atomicAdd(&dst->agg_count, cnt);
       if (num) atomicAdd(&dst->agg_numeric, num);
@@ -690,7 +651,9 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
 // are instruction operands, and no plan read goes through global memory.
 // kMulti (aggregates only): a mixed batch, each input with its own plan,
 // taken per tile from sp.plans in device memory instead of `plan`.
-template <bool kRows, bool kMulti = false>
+// kGroups: the group-by path is compiled in (grouped aggregates, mixed
+// batches); without it the kernel is lighter for every other query.
+template <bool kRows, bool kMulti = false, bool kGroups = kMulti>
 __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -715,15 +678,13 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
 
   ThreadAgg agg;
   agg.init();
-  LaneFix fx;
-  fx.init();
-  unsigned long long c_lines = 0, c_blank = 0, c_invalid = 0, c_type = 0, c_sel = 0;
+  uint32_t c_lines = 0, c_blank = 0, c_invalid = 0, c_type = 0, c_sel = 0;  // a lane's line counts
   unsigned long long cta_recs = 0;  // records this CTA has appended (rows mode)
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
   if (lane < kFixDigits) cta_fix[lane] = 0;
-  const bool grouped = !kRows && (kMulti ? sp.any_grouped != 0 : P.group_slot >= 0);
+  const bool grouped = kGroups && !kRows && (kMulti ? sp.any_grouped != 0 : P.group_slot >= 0);
   if (grouped) {
     for (int k = lane; k < kGroupCache; k += 32) {
       gcache->tag[k] = 0xFFFFFFFFu;
@@ -821,6 +782,22 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
       }
     }
 
+    // The next tile's window is fetched into L2 now (its ticket has
+    // arrived), so its bulk copy reads from L2 rather than waiting on HBM.
+    if (lane == 0) {
+      const unsigned long long nt = next_ticket;
+      if (nt < sp.n_tiles) {
+        unsigned long long ns = nt * T, ne = sp.n;
+        if (sp.tile_input) {
+          const uint32_t ni = sp.tile_input[nt];
+          ns = sp.in_start[ni] + (nt - sp.in_tile0[ni]) * T;
+          ne = sp.in_end[ni];
+        }
+        const uint32_t nb = (uint32_t)min((unsigned long long)T + H, ne - ns) & ~15u;
+        if (nb) l2_prefetch(sp.data + ns, nb);
+      }
+    }
+
     // 3. Lines starting in the tile: ts itself (after a newline) and q+1 for
     //    every newline q in [ts, te-1).
     uint32_t first_nl, tot_nl;
@@ -888,7 +865,8 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
           if (found) {
             lp = win + s;
             line_len = e - s;
-            status = walk_masked(P, win, smask, s, e, nv);
+            status = walk_objects(P, win, smask, s, e, nv);
+            if (status == LS_FALLBACK) status = walk_masked(P, win, smask, s, e, nv);
           } else {
             // longer than the window: walk it from global memory
             unsigned long long q = ts + wlen;
@@ -951,7 +929,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
           } else {
             // aggregate (exec/cpu.rs:358-369, agg.rs:44-71)
             if (P.agg_slot >= 0) aggv = slots[P.agg_slot];
-            if (P.group_slot >= 0) {
+            if (kGroups && P.group_slot >= 0) {
               const SlotVal &g = slots[P.group_slot];
               has_group = true;
               gk.esc = 0;
@@ -1004,11 +982,11 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
               agg.add_int(iv);
               agg.n_int++;
             } else {
-              fx.add(fv, cta_fix);
+              fix_atomic_add(cta_fix, &ctr_in->fbig, fv);  // exact, in the CTA's shared limbs
             }
           }
         }
-        if (!kRows && P.group_slot >= 0) {
+        if (kGroups && !kRows && P.group_slot >= 0) {
           // Lanes whose keys hash alike compare their key bytes with the
           // lowest such lane; only lanes that differ from it look up the
           // table themselves.
@@ -1119,8 +1097,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
     }
     // A batch input's counts and aggregate go to its own record, tile by tile.
     if (sp.tile_input)
-      flush_counts(ctr_in, sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, fx,
-                   cta_fix);
+      flush_counts(ctr_in, sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, cta_fix);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
@@ -1152,8 +1129,7 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
   }
 
   // Flush this CTA's counters (a batch's were flushed per tile).
-  flush_counts(sp.ctr, nullptr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, fx,
-               cta_fix);
+  flush_counts(sp.ctr, nullptr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, cta_fix);
 }
 
 // The index of the first invalid / type-error line: lines of the tiles

@@ -27,6 +27,7 @@ enum LineStatus : int {
   LS_BLANK = 4,
   LS_DEEP = 5,       // deeper than the register stack; caller retries with a deep stack
   LS_DEEP_FULL = 6,  // deeper than the deep stack provided
+  LS_FALLBACK = 7,   // not the fast path's shape; the general walker decides
 };
 
 // Values recorded per trie node for one line; offsets are relative to the
@@ -448,7 +449,7 @@ __device__ __forceinline__ uint8_t match_key_win(const DevPlan &P, uint8_t node,
 // mask (bit j of sm[j / 32]: byte j is '"', '\\' or below 0x20), complete at
 // least up to e.  Offsets recorded in `v` are relative to s.  Lines nesting
 // past 64 levels return LS_DEEP.
-__device__ __forceinline__ int walk_masked(const DevPlan &P, const uint8_t *w, const uint32_t *sm,
+__device__ __noinline__ int walk_masked(const DevPlan &P, const uint8_t *w, const uint32_t *sm,
                                            uint32_t s, uint32_t e, NodeVals &v) {
   using namespace detail;
   const uint32_t n_nodes = P.n_nodes;
@@ -585,6 +586,124 @@ __device__ __forceinline__ int walk_masked(const DevPlan &P, const uint8_t *w, c
       i++;
       la = load4(w, i);
     }
+  }
+}
+
+namespace detail {
+
+// Four hex digits at w[i..i+3].
+__device__ __forceinline__ bool hex4_at(const uint8_t *w, uint32_t i) {
+  return hex_val(w[i]) >= 0 && hex_val(w[i + 1]) >= 0 && hex_val(w[i + 2]) >= 0 && hex_val(w[i + 3]) >= 0;
+}
+
+// Position of the next special byte (a set bit of the window's special mask)
+// from the cursor (k, m), consuming it.  The line's newline is special, so
+// a walk that reaches it stops there.
+__device__ __forceinline__ uint32_t pop_special(const uint32_t *sm, uint32_t &k, uint32_t &m) {
+  while (!m) m = sm[++k];
+  const uint32_t b = (k << 5) + (uint32_t)__ffs(m) - 1u;
+  m &= m - 1u;
+  return b;
+}
+
+}  // namespace detail
+
+// The fast path of the window walk, for the common shape of a log line: one
+// object whose members are separated by single ',' and ':' with no
+// whitespace, keys without escapes, and values that are scalars or objects
+// of the same shape, at most 8 deep (no arrays).  It steps from special byte
+// to special byte: a key is its two quotes, a string value its quotes and
+// escapes, and only the bytes right after them are read ('"' ':' value, ','
+// or '}').  Lines of that shape get exactly walk_masked's verdict and node
+// values; for any other line (whitespace, arrays, escaped keys, deeper
+// nesting, anything malformed) it returns LS_FALLBACK and records nothing
+// that walk_masked does not overwrite.  Same window contract as walk_masked.
+__device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, const uint32_t *sm,
+                                            uint32_t s, uint32_t e, NodeVals &v) {
+  using namespace detail;
+  if (w[s] != '{') return LS_FALLBACK;
+  const uint32_t n_nodes = P.n_nodes;
+  for (uint32_t k = 0; k < n_nodes; k++) v.kind[k] = JK_MISSING;
+  uint32_t cur = n_nodes ? 0u : kNoNode;  // trie node of the innermost open object
+  unsigned long long lm = 0;             // its key_len_mask (0: no key is looked up)
+  if (cur != kNoNode) {
+    v.kind[0] = JK_OBJ;
+    v.off[0] = 0;
+    v.esc[0] = 0;
+    lm = P.nodes[0].key_len_mask;
+  }
+  unsigned long long stack = 0;  // trie nodes of the enclosing objects, 8 bits a level
+  uint32_t depth = 1;
+  uint32_t k = (s + 1) >> 5;
+  uint32_t m = sm[k] & (0xFFFFFFFFu << ((s + 1) & 31u));
+  uint32_t p = s + 1;  // where the next key's opening quote must be
+  for (;;) {
+    const uint32_t q0 = pop_special(sm, k, m);
+    if (q0 != p || w[q0] != '"') return LS_FALLBACK;
+    const uint32_t q1 = pop_special(sm, k, m);
+    if (w[q1] != '"') return LS_FALLBACK;
+    uint32_t vn = kNoNode;
+    const uint32_t kl = q1 - q0 - 1;
+    if ((lm >> (kl < 63u ? kl : 63u)) & 1ull) vn = match_key_win(P, (uint8_t)cur, w, q0 + 1, kl, false);
+    const uint32_t la = load4(w, q1 + 1);
+    if ((la & 0xFFu) != ':') return LS_FALLBACK;
+    const uint32_t c = (la >> 8) & 0xFFu;
+    const uint32_t vs = q1 + 2;
+    if (vn != kNoNode) {
+      for (uint32_t x = vn + 1u; x < P.nodes[vn].subtree_end; x++) v.kind[x] = JK_MISSING;
+      v.kind[vn] = kind_of(c);
+      v.off[vn] = vs - s;
+      v.esc[vn] = 0;
+    }
+    if (c == '{') {
+      if (depth >= 8) return LS_FALLBACK;
+      stack = (stack << 8) | cur;
+      depth++;
+      cur = vn;
+      lm = vn != kNoNode ? P.nodes[vn].key_len_mask : 0ull;
+      p = vs + 1;
+      continue;
+    }
+    uint32_t ve;
+    if (c == '"') {
+      pop_special(sm, k, m);  // the opening quote, at vs
+      bool esc = false;
+      uint32_t r;
+      for (;;) {
+        r = pop_special(sm, k, m);
+        const uint32_t b = w[r];
+        if (b == '"') break;
+        if (b != '\\') return LS_FALLBACK;  // a control byte or the newline
+        esc = true;
+        const uint32_t x = w[r + 1];
+        if (x == '"' || x == '\\') {
+          pop_special(sm, k, m);  // the escaped byte is special itself
+        } else if (x == 'u') {
+          if (!hex4_at(w, r + 2)) return LS_FALLBACK;
+        } else if (!simple_escape(x)) {
+          return LS_FALLBACK;
+        }
+      }
+      ve = r + 1;
+      if (vn != kNoNode) v.esc[vn] = esc;
+    } else {
+      if (c == '[') return LS_FALLBACK;
+      ve = win_atom(w, vs, c);
+      if (!ve) return LS_FALLBACK;
+    }
+    if (vn != kNoNode) v.len[vn] = ve - vs;
+    // after a value: ',' and the next key, or '}' closing one or more objects
+    uint32_t t = w[ve];
+    while (t == '}') {
+      if (cur != kNoNode) v.len[cur] = ve + 1 - s - v.off[cur];
+      if (--depth == 0) return ve + 1 == e ? LS_OK : LS_FALLBACK;
+      cur = (uint32_t)(stack & 0xFFu);
+      stack >>= 8;
+      lm = cur != kNoNode ? P.nodes[cur].key_len_mask : 0ull;
+      t = w[++ve];
+    }
+    if (t != ',') return LS_FALLBACK;
+    p = ve + 1;
   }
 }
 
