@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/warpjq_kernels.h"
 #include "devutil.cuh"
 #include "fixsum.cuh"
 #include "plan.h"
@@ -36,7 +37,11 @@ namespace wjq {
 constexpr int kThreads = 32;                 // one warp per CTA; each warp owns its tile
 constexpr uint32_t kMaxLinesPerPass = 128;   // line-start list capacity per pass
 constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
-constexpr int kScanBlocksPerSM = 24;         // register budget of k_scan: 24 warps per SM
+// Register budgets of k_scan (warps per SM): the row and ungrouped variants
+// at 20 (shared memory allows ~20-23 tiles per SM, and 96 registers keep
+// them from spilling), the group-by variants at 16.
+constexpr int kScanBlocksPerSM = 20;
+constexpr int kScanBlocksPerSMGrouped = 16;
 
 constexpr int kGroupCache = 16;  // per-CTA group accumulators kept in shared memory
 
@@ -654,7 +659,7 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
 // kGroups: the group-by path is compiled in (grouped aggregates, mixed
 // batches); without it the kernel is lighter for every other query.
 template <bool kRows, bool kMulti = false, bool kGroups = kMulti>
-__global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
+__global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : kScanBlocksPerSM)
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
   const DevPlan &P = plan;
@@ -1004,7 +1009,43 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
           if (has_group && !same) kid = group_find_or_insert(sp, gk, gh);
           const uint32_t lkid = __shfl_sync(0xffffffffu, kid, leader);
           if (same) kid = lkid;
-          if (kid != 0xFFFFFFFFu) {
+          // Lanes holding the same key add up their contributions in the
+          // warp first; one lane per key then updates its accumulators
+          // (counts, the exact integer sum, min or max).  Fractional values
+          // go in per lane, exactly (fixsum.cuh).
+          const unsigned grp = __match_any_sync(0xffffffffu, kid);
+          const bool lead = kid != 0xFFFFFFFFu && lane == __ffs(grp) - 1;
+          const bool num_int = is_num && is_int;
+          const unsigned m_num = __ballot_sync(0xffffffffu, is_num) & grp;
+          const unsigned m_int = __ballot_sync(0xffffffffu, num_int) & grp;
+          const uint32_t ak = P.agg_kind;
+          unsigned long long s_lo = 0, s_hi = 0, ext = 0;
+          if ((ak == WARPJQ_AGG_SUM || ak == WARPJQ_AGG_AVG) && __any_sync(0xffffffffu, num_int)) {
+            // the key's integer values summed in three parts of at most 22
+            // bits (no part overflows 32 bits over 32 lanes), then as 128 bits
+            const unsigned long long u = num_int ? (unsigned long long)iv : 0ull;
+            const uint32_t p0 = __reduce_add_sync(grp, (uint32_t)(u & 0x1FFFFFu));
+            const uint32_t p1 = __reduce_add_sync(grp, (uint32_t)((u >> 21) & 0x1FFFFFu));
+            const uint32_t p2 = __reduce_add_sync(grp, (uint32_t)(u >> 42));
+            const uint32_t nneg = __popc(__ballot_sync(0xffffffffu, num_int && iv < 0) & grp);
+            const unsigned __int128 t = (unsigned __int128)p0 + ((unsigned __int128)p1 << 21) +
+                                        ((unsigned __int128)p2 << 42) - ((unsigned __int128)nneg << 64);
+            s_lo = (unsigned long long)t;
+            s_hi = (unsigned long long)(t >> 64);
+          }
+          if ((ak == WARPJQ_AGG_MIN || ak == WARPJQ_AGG_MAX) && __any_sync(0xffffffffu, is_num)) {
+            // 64-bit order keys: the high words first, then the low words of
+            // the lanes that hold the extreme high word
+            const unsigned long long ob = order_bits(fv);
+            const bool mn = ak == WARPJQ_AGG_MIN;
+            const uint32_t none = mn ? 0xFFFFFFFFu : 0u;
+            const uint32_t h = is_num ? (uint32_t)(ob >> 32) : none;
+            const uint32_t eh = mn ? __reduce_min_sync(grp, h) : __reduce_max_sync(grp, h);
+            const uint32_t l = (is_num && h == eh) ? (uint32_t)ob : none;
+            const uint32_t el = mn ? __reduce_min_sync(grp, l) : __reduce_max_sync(grp, l);
+            ext = ((unsigned long long)eh << 32) | el;
+          }
+          if (lead || (is_num && !is_int)) {
             // This CTA's cached entry for the key if it has (or can claim)
             // one, else the global record.
             GroupAcc *ap = &sp.g.acc[kid];
@@ -1016,25 +1057,26 @@ __global__ void __launch_bounds__(kThreads, kScanBlocksPerSM)
             }
             if (t == kid) ap = &gcache->acc[e];
             GroupAcc &a = *ap;
-            atomicAdd(&a.count, 1ull);
-            if (is_num) {
-              atomicAdd(&a.numeric, 1ull);
-              const unsigned long long ob = order_bits(fv);
-              atomicMin(&a.min_bits, ob);
-              atomicMax(&a.max_bits, ob);
-              if (is_int) {
-                const unsigned long long old = atomicAdd(&a.isum_lo, (unsigned long long)iv);
-                const unsigned long long carry = (old + (unsigned long long)iv) < old ? 1ull : 0ull;
-                const unsigned long long hi = (iv < 0 ? ~0ull : 0ull) + carry;
-                if (hi) atomicAdd(&a.isum_hi, hi);
-                atomicAdd(&a.n_int, 1ull);
-              } else {
-                fix_atomic_add(a.fix, &a.fbig, fv);
+            if (lead) {
+              atomicAdd(&a.count, (unsigned long long)__popc(grp));
+              if (m_num) atomicAdd(&a.numeric, (unsigned long long)__popc(m_num));
+              if (m_int) {
+                atomicAdd(&a.n_int, (unsigned long long)__popc(m_int));
+                if (s_lo || s_hi) {
+                  const unsigned long long old = atomicAdd(&a.isum_lo, s_lo);
+                  const unsigned long long carry = (old + s_lo) < old ? 1ull : 0ull;
+                  if (s_hi + carry) atomicAdd(&a.isum_hi, s_hi + carry);
+                }
               }
-            } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL && P.agg_slot >= 0) {
-              sp.g.keys[kid].saw_non_numeric = 1;
+              if (m_num && ak == WARPJQ_AGG_MIN) atomicMin(&a.min_bits, ext);
+              if (m_num && ak == WARPJQ_AGG_MAX) atomicMax(&a.max_bits, ext);
             }
+            if (is_num && !is_int && (ak == WARPJQ_AGG_SUM || ak == WARPJQ_AGG_AVG))
+              fix_atomic_add(a.fix, &a.fbig, fv);
           }
+          if (kid != 0xFFFFFFFFu && !is_num && aggv.kind != JK_MISSING && aggv.kind != JK_NULL &&
+              P.agg_slot >= 0)
+            sp.g.keys[kid].saw_non_numeric = 1;
         }
 
         if (kRows) {
