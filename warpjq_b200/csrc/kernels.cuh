@@ -38,9 +38,9 @@ constexpr int kThreads = 32;                 // one warp per CTA; each warp owns
 constexpr uint32_t kMaxLinesPerPass = 128;   // line-start list capacity per pass
 constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
 // Register budgets of k_scan (warps per SM): the row and ungrouped variants
-// at 20 (shared memory allows ~20-23 tiles per SM, and 96 registers keep
-// them from spilling), the group-by variants at 16.
-constexpr int kScanBlocksPerSM = 20;
+// at 24 (80 registers; more warps hide more latency than the few spills
+// cost), the group-by variants at 16 (128 registers).
+constexpr int kScanBlocksPerSM = 24;
 constexpr int kScanBlocksPerSMGrouped = 16;
 
 constexpr int kGroupCache = 16;  // per-CTA group accumulators kept in shared memory
@@ -1045,7 +1045,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
             const uint32_t el = mn ? __reduce_min_sync(grp, l) : __reduce_max_sync(grp, l);
             ext = ((unsigned long long)eh << 32) | el;
           }
-          if (lead || (is_num && !is_int)) {
+          if (kid != 0xFFFFFFFFu && (lead || (is_num && !is_int))) {  // no key id: the table is full
             // This CTA's cached entry for the key if it has (or can claim)
             // one, else the global record.
             GroupAcc *ap = &sp.g.acc[kid];
