@@ -480,11 +480,6 @@ __device__ __noinline__ double slow_decimal_to_double(const uint8_t *p, uint32_t
 // Parses a validated JSON number.  `is_int` is set when the text is an
 // integer literal (no fraction, no exponent) that fits in int64; `iv` then
 // holds its exact value.
-__device__ __noinline__ double parse_number_general(const uint8_t *p, uint32_t n, bool &is_int,
-                                                    long long &iv);
-
-// The short non-negative integers that dominate log fields (status codes,
-// sizes, timestamps up to 9 digits) inline; every other number out of line.
 __device__ __forceinline__ double parse_number(const uint8_t *p, uint32_t n, bool &is_int,
                                                long long &iv) {
   if (n <= 9) {  // exact in 32 bits
@@ -501,11 +496,6 @@ __device__ __forceinline__ double parse_number(const uint8_t *p, uint32_t n, boo
       return (double)v;
     }
   }
-  return parse_number_general(p, n, is_int, iv);
-}
-
-__device__ __noinline__ double parse_number_general(const uint8_t *p, uint32_t n, bool &is_int,
-                                                    long long &iv) {
   bool neg = p[0] == '-';
   uint32_t i = neg ? 1 : 0;
   unsigned long long mant = 0;

@@ -37,13 +37,36 @@ namespace wjq {
 constexpr int kThreads = 32;                 // one warp per CTA; each warp owns its tile
 constexpr uint32_t kMaxLinesPerPass = 128;   // line-start list capacity per pass
 constexpr int kReduceThreads = 128;          // block size of the per-tile reductions
-// Register budgets of k_scan (warps per SM): the row and ungrouped variants
-// at 24 (80 registers; more warps hide more latency than the few spills
-// cost), the group-by variants at 16 (128 registers).
+// Register budgets of k_scan (warps per SM), measured per variant on the
+// nginx workload: the ungrouped aggregate at 24 (80 registers; more warps
+// hide more latency than its few spills cost), the row variant at 20 (96
+// registers, which keep its record writing from spilling) and the group-by
+// variants at 16 (128 registers).
 constexpr int kScanBlocksPerSM = 24;
+constexpr int kScanBlocksPerSMRows = 20;
 constexpr int kScanBlocksPerSMGrouped = 16;
 
 constexpr int kGroupCache = 16;  // per-CTA group accumulators kept in shared memory
+
+// A CTA's line counts and ungrouped aggregate, in shared memory: each round
+// of up to 32 lines is reduced in the warp (ballots, warp reductions) and
+// lane 0 adds the round's totals here, so no lane keeps accumulators in
+// registers through the walk.  Flushed to the run's counters at the end of
+// the CTA (or of each tile, in a batch).
+struct CtaAcc {
+  unsigned long long lines, blank, invalid, type, sel;
+  unsigned long long count, numeric, n_int;
+  unsigned long long isum_lo, isum_hi;  // exact 128-bit sum of the integer values
+  unsigned long long min_bits, max_bits;
+  uint32_t saw;  // a selected line had a non-numeric, non-null value
+  uint32_t pad;
+  __device__ void clear() {
+    lines = blank = invalid = type = sel = count = numeric = n_int = isum_lo = isum_hi = 0;
+    min_bits = ~0ull;
+    max_bits = 0;
+    saw = 0;
+  }
+};
 
 // Readable bytes kept past a window's data: the end sentinel, the walker's
 // word reads after a line's newline, and the last chunk's 32-byte read.
@@ -65,6 +88,7 @@ __host__ __device__ inline size_t scan_smem_base(uint32_t T, uint32_t H) {
   size_t s = scan_win_bytes(T, H);
   s += 2 * (size_t)scan_chunk_words(T, H) * sizeof(uint32_t);
   s += kFixDigits * sizeof(long long);
+  s += sizeof(CtaAcc);
   s += sizeof(unsigned long long);  // the mbarrier of the tile copies
   s += (kMaxLinesPerPass + 2) * sizeof(uint16_t);
   return (s + 15) & ~(size_t)15;
@@ -480,23 +504,34 @@ __device__ void emit_row(const DevPlan &P, const uint8_t *line, const RowRec &r,
 // The scan kernel.
 // ---------------------------------------------------------------------------
 
-struct ThreadAgg {
-  uint32_t count, numeric, n_int;  // a lane's counts (flushed per CTA, or per tile in a batch)
-  unsigned long long isum_lo, isum_hi, min_bits, max_bits;
-  unsigned int saw;
-  __device__ void init() {
-    count = numeric = isum_lo = isum_hi = n_int = 0;
-    min_bits = ~0ull;
-    max_bits = 0;
-    saw = 0;
-  }
-  __device__ void add_int(long long v) {
-    unsigned long long lo = isum_lo + (unsigned long long)v;
-    unsigned long long carry = lo < isum_lo;
-    isum_lo = lo;
-    isum_hi += (v < 0 ? ~0ull : 0ull) + carry;
-  }
-};
+// The 128-bit sum over the lanes of `grp` of their signed 64-bit values
+// (0 where `on` is false): three parts of at most 22 bits, which cannot
+// overflow 32 bits over 32 lanes, recombined with the negatives' borrow.
+__device__ __forceinline__ void group_sum128(unsigned grp, bool on, long long v, unsigned long long &lo,
+                                             unsigned long long &hi) {
+  const unsigned long long u = on ? (unsigned long long)v : 0ull;
+  const uint32_t p0 = __reduce_add_sync(grp, (uint32_t)(u & 0x1FFFFFu));
+  const uint32_t p1 = __reduce_add_sync(grp, (uint32_t)((u >> 21) & 0x1FFFFFu));
+  const uint32_t p2 = __reduce_add_sync(grp, (uint32_t)(u >> 42));
+  const uint32_t nneg = __popc(__ballot_sync(0xffffffffu, on && v < 0) & grp);
+  const unsigned __int128 t = (unsigned __int128)p0 + ((unsigned __int128)p1 << 21) +
+                              ((unsigned __int128)p2 << 42) - ((unsigned __int128)nneg << 64);
+  lo = (unsigned long long)t;
+  hi = (unsigned long long)(t >> 64);
+}
+
+// The extreme (min or max) over the lanes of `grp` of 64-bit keys (lanes
+// with `on` false hold none): the high words first, then the low words of
+// the lanes holding the extreme high word.
+__device__ __forceinline__ unsigned long long group_extreme(unsigned grp, bool on, unsigned long long ob,
+                                                            bool mn) {
+  const uint32_t none = mn ? 0xFFFFFFFFu : 0u;
+  const uint32_t h = on ? (uint32_t)(ob >> 32) : none;
+  const uint32_t eh = mn ? __reduce_min_sync(grp, h) : __reduce_max_sync(grp, h);
+  const uint32_t l = (on && h == eh) ? (uint32_t)ob : none;
+  const uint32_t el = mn ? __reduce_min_sync(grp, l) : __reduce_max_sync(grp, l);
+  return ((unsigned long long)eh << 32) | el;
+}
 
 // One-CTA mbarrier (a tile's bulk copy completes on it) and the 1-D bulk
 // (TMA) copy from this GPU's own global memory into shared memory.  The
@@ -581,75 +616,46 @@ __device__ __forceinline__ void warp_scan2(uint32_t a, unsigned long long b, uin
   tb = __shfl_sync(0xffffffffu, ib, 31);
 }
 
-// Adds the warp's counts and (ungrouped) aggregate to `dst` and clears them;
-// `also` (a batch's totals, may be null) receives the line counts too.
-// The non-integer values' exact sum, gathered in the CTA's shared limbs
+// Adds the CTA's counts and (ungrouped) aggregate to `dst` and clears them;
+// `also` (a batch's totals, may be null) receives the line counts too.  The
+// non-integer values' exact sum, gathered in the CTA's shared limbs
 // `cta_fix`, goes into dst's limbs (and the shared limbs are cleared).
-__device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, const DevPlan &P,
-                                          bool rows, int lane, uint32_t &c_lines, uint32_t &c_blank,
-                                          uint32_t &c_invalid, uint32_t &c_type, uint32_t &c_sel,
-                                          ThreadAgg &agg, long long *cta_fix) {
-  const unsigned long long nl = warp_sum_u64(c_lines), nb = warp_sum_u64(c_blank),
-                           ni = warp_sum_u64(c_invalid), nt = warp_sum_u64(c_type),
-                           ns = warp_sum_u64(c_sel);
+__device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, const DevPlan &P, bool rows,
+                                          int lane, CtaAcc *acc, long long *cta_fix) {
+  __syncwarp();
   if (lane == 0) {
     for (RunCounters *c : {dst, also}) {
       if (!c) continue;
-      if (nl) atomicAdd(&c->n_lines, nl);
-      if (nb) atomicAdd(&c->n_blank, nb);
-      if (ni) atomicAdd(&c->n_invalid, ni);
-      if (nt) atomicAdd(&c->n_type_error, nt);
-      if (ns) atomicAdd(&c->n_selected, ns);
+      if (acc->lines) atomicAdd(&c->n_lines, acc->lines);
+      if (acc->blank) atomicAdd(&c->n_blank, acc->blank);
+      if (acc->invalid) atomicAdd(&c->n_invalid, acc->invalid);
+      if (acc->type) atomicAdd(&c->n_type_error, acc->type);
+      if (acc->sel) atomicAdd(&c->n_selected, acc->sel);
     }
-  }
-  c_lines = c_blank = c_invalid = c_type = c_sel = 0;
-  if (!rows && P.group_slot < 0 && P.output_kind == 3) {
-    const unsigned long long cnt = warp_sum_u64(agg.count), num = warp_sum_u64(agg.numeric),
-                             nint = warp_sum_u64(agg.n_int);
-    // 128-bit sums: reduce the low words with carry counting, per lane pair
-    unsigned long long lo = agg.isum_lo, hi = agg.isum_hi;
-    for (int d = 16; d > 0; d >>= 1) {
-      const unsigned long long olo = __shfl_down_sync(0xffffffffu, lo, d);
-      const unsigned long long ohi = __shfl_down_sync(0xffffffffu, hi, d);
-      if (lane + d < 32) {
-        const unsigned long long sum = lo + olo;
-        hi += ohi + (sum < lo);
-        lo = sum;
-      }
-    }
-    unsigned long long mn = agg.min_bits, mx = agg.max_bits;
-    for (int d = 16; d > 0; d >>= 1) {
-      mn = min(mn, __shfl_down_sync(0xffffffffu, mn, d));
-      mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
-    }
-    const unsigned int saw = __any_sync(0xffffffffu, agg.saw);
-    __syncwarp();
-    if (lane < kFixDigits) {
-      const long long v = cta_fix[lane];
-      cta_fix[lane] = 0;
-      if (v) atomicAdd((unsigned long long *)&dst->fix[lane], (unsigned long long)v);
-    }
-    __syncwarp();
-    if (lane == 0) {
-      if (cnt) atomicAdd(&dst->agg_count, cnt);
-      if (num) atomicAdd(&dst->agg_numeric, num);
-      if (nint) atomicAdd(&dst->agg_n_int, nint);
+    if (!rows && P.group_slot < 0 && P.output_kind == 3) {
+      if (acc->count) atomicAdd(&dst->agg_count, acc->count);
+      if (acc->numeric) atomicAdd(&dst->agg_numeric, acc->numeric);
+      if (acc->n_int) atomicAdd(&dst->agg_n_int, acc->n_int);
+      const unsigned long long lo = acc->isum_lo, hi = acc->isum_hi;
       if (lo || hi) {
         const unsigned long long old = atomicAdd(&dst->agg_isum_lo, lo);
         const unsigned long long carry = (old + lo) < old;
         if (hi + carry) atomicAdd(&dst->agg_isum_hi, hi + carry);
       }
-      if (num) {
-        atomicMin(&dst->agg_min_bits, mn);
-        atomicMax(&dst->agg_max_bits, mx);
+      if (acc->numeric) {
+        atomicMin(&dst->agg_min_bits, acc->min_bits);
+        atomicMax(&dst->agg_max_bits, acc->max_bits);
       }
-      if (saw) atomicOr(&dst->agg_saw_non_numeric, 1u);
     }
-  } else if (!rows) {
-    const unsigned int saw = __any_sync(0xffffffffu, agg.saw);
-    if (lane == 0 && saw) atomicOr(&dst->agg_saw_non_numeric, 1u);
+    if (!rows && acc->saw) atomicOr(&dst->agg_saw_non_numeric, 1u);
+    acc->clear();
   }
-  agg.init();
+  if (!rows && P.group_slot < 0 && P.output_kind == 3 && lane < kFixDigits) {
+    const long long v = cta_fix[lane];
+    cta_fix[lane] = 0;
+    if (v) atomicAdd((unsigned long long *)&dst->fix[lane], (unsigned long long)v);
+  }
+  __syncwarp();
 }
 
 // The plan is a kernel parameter (constant bank): fields at fixed offsets
@@ -659,7 +665,7 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
 // kGroups: the group-by path is compiled in (grouped aggregates, mixed
 // batches); without it the kernel is lighter for every other query.
 template <bool kRows, bool kMulti = false, bool kGroups = kMulti>
-__global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : kScanBlocksPerSM)
+__global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : (kRows ? kScanBlocksPerSMRows : kScanBlocksPerSM))
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
   const DevPlan &P = plan;
@@ -669,7 +675,8 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
   uint32_t *smask = (uint32_t *)(smem + scan_win_bytes(T, H));      // special bytes per chunk
   uint32_t *nlmask = smask + nwords;                                // newlines per chunk
   long long *cta_fix = (long long *)(nlmask + nwords);              // the CTA's exact FP sum
-  unsigned long long *s_bar = (unsigned long long *)(cta_fix + kFixDigits);  // tile copies' mbarrier
+  CtaAcc *acc = (CtaAcc *)(cta_fix + kFixDigits);                   // the CTA's counts and aggregate
+  unsigned long long *s_bar = (unsigned long long *)(acc + 1);       // tile copies' mbarrier
   uint16_t *lstart = (uint16_t *)(s_bar + 1);                       // kMaxLinesPerPass + 2
   GroupCache *gcache = (GroupCache *)(smem + scan_smem_base(T, H));  // grouped aggregates only
 
@@ -681,14 +688,12 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
   deep.words = sp.deep_words + (unsigned long long)blockIdx.x * (sp.deep_levels_per_cta / 32);
   deep.cap_levels = sp.deep_levels_per_cta;
 
-  ThreadAgg agg;
-  agg.init();
-  uint32_t c_lines = 0, c_blank = 0, c_invalid = 0, c_type = 0, c_sel = 0;  // a lane's line counts
   unsigned long long cta_recs = 0;  // records this CTA has appended (rows mode)
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
   if (lane < kFixDigits) cta_fix[lane] = 0;
+  if (lane == 0) acc->clear();
   const bool grouped = kGroups && !kRows && (kMulti ? sp.any_grouped != 0 : P.group_slot >= 0);
   if (grouped) {
     for (int k = lane; k < kGroupCache; k += 32) {
@@ -918,16 +923,11 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
             status = 101;  // selected
           }
         }
-        if (status == LS_BLANK) {
-          c_blank++;
-        } else if (status == LS_INVALID) {
-          c_invalid++;
+        if (status == LS_INVALID) {
           tile_first_invalid = min(tile_first_invalid, ordinal);
         } else if (status == LS_TYPE_ERROR) {
-          c_type++;
           tile_first_type = min(tile_first_type, ordinal);
         } else if (status == 101) {
-          c_sel++;
           if (kRows) {
             has_row = 1;
             row_len = row_length(P, lp, out_len, slots);
@@ -968,26 +968,53 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         long long iv = 0;
         double fv = 0.0;
         bool is_int = false, is_num = false;
+        bool saw = false;
         if (contrib && P.agg_slot >= 0) {
           if (aggv.kind == JK_NUM) {
             fv = parse_number(lp + aggv.off, aggv.len, is_int, iv);
             is_num = true;
           } else if (aggv.kind != JK_MISSING && aggv.kind != JK_NULL) {
-            agg.saw = 1;
+            saw = true;
           }
         }
-        if (contrib && !has_group) {
-          agg.count++;
-          if (is_num) {
-            agg.numeric++;
-            unsigned long long ob = order_bits(fv);
-            agg.min_bits = min(agg.min_bits, ob);
-            agg.max_bits = max(agg.max_bits, ob);
-            if (is_int) {
-              agg.add_int(iv);
-              agg.n_int++;
-            } else {
-              fix_atomic_add(cta_fix, &ctr_in->fbig, fv);  // exact, in the CTA's shared limbs
+        // The round's counts and ungrouped aggregate, reduced in the warp
+        // and added to the CTA's shared accumulator by lane 0.
+        {
+          const unsigned full = 0xffffffffu;
+          const unsigned m_blank = __ballot_sync(full, status == LS_BLANK);
+          const unsigned m_inv = __ballot_sync(full, status == LS_INVALID);
+          const unsigned m_type = __ballot_sync(full, status == LS_TYPE_ERROR);
+          const unsigned m_sel = __ballot_sync(full, status == 101);
+          const unsigned m_saw = __ballot_sync(full, saw);
+          const bool ung = contrib && !has_group;
+          const unsigned m_cnt = __ballot_sync(full, ung);
+          const unsigned m_num = __ballot_sync(full, ung && is_num);
+          const unsigned m_int = __ballot_sync(full, ung && is_num && is_int);
+          unsigned long long s_lo = 0, s_hi = 0, ext = 0;
+          const uint32_t ak = P.agg_kind;
+          if (m_int && (ak == WARPJQ_AGG_SUM || ak == WARPJQ_AGG_AVG))
+            group_sum128(full, ung && is_num && is_int, iv, s_lo, s_hi);
+          if (m_num && (ak == WARPJQ_AGG_MIN || ak == WARPJQ_AGG_MAX))
+            ext = group_extreme(full, ung && is_num, order_bits(fv), ak == WARPJQ_AGG_MIN);
+          if (ung && is_num && !is_int && (ak == WARPJQ_AGG_SUM || ak == WARPJQ_AGG_AVG))
+            fix_atomic_add(cta_fix, &ctr_in->fbig, fv);  // exact, in the CTA's shared limbs
+          if (lane == 0) {
+            acc->blank += __popc(m_blank);
+            acc->invalid += __popc(m_inv);
+            acc->type += __popc(m_type);
+            acc->sel += __popc(m_sel);
+            if (m_saw) acc->saw = 1;
+            if (m_cnt) {
+              acc->count += __popc(m_cnt);
+              acc->numeric += __popc(m_num);
+              acc->n_int += __popc(m_int);
+              if (s_lo || s_hi) {
+                const unsigned long long o = acc->isum_lo;
+                acc->isum_lo = o + s_lo;
+                acc->isum_hi += s_hi + (acc->isum_lo < o ? 1ull : 0ull);
+              }
+              if (m_num && ak == WARPJQ_AGG_MIN) acc->min_bits = min(acc->min_bits, ext);
+              if (m_num && ak == WARPJQ_AGG_MAX) acc->max_bits = max(acc->max_bits, ext);
             }
           }
         }
@@ -1020,31 +1047,10 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
           const unsigned m_int = __ballot_sync(0xffffffffu, num_int) & grp;
           const uint32_t ak = P.agg_kind;
           unsigned long long s_lo = 0, s_hi = 0, ext = 0;
-          if ((ak == WARPJQ_AGG_SUM || ak == WARPJQ_AGG_AVG) && __any_sync(0xffffffffu, num_int)) {
-            // the key's integer values summed in three parts of at most 22
-            // bits (no part overflows 32 bits over 32 lanes), then as 128 bits
-            const unsigned long long u = num_int ? (unsigned long long)iv : 0ull;
-            const uint32_t p0 = __reduce_add_sync(grp, (uint32_t)(u & 0x1FFFFFu));
-            const uint32_t p1 = __reduce_add_sync(grp, (uint32_t)((u >> 21) & 0x1FFFFFu));
-            const uint32_t p2 = __reduce_add_sync(grp, (uint32_t)(u >> 42));
-            const uint32_t nneg = __popc(__ballot_sync(0xffffffffu, num_int && iv < 0) & grp);
-            const unsigned __int128 t = (unsigned __int128)p0 + ((unsigned __int128)p1 << 21) +
-                                        ((unsigned __int128)p2 << 42) - ((unsigned __int128)nneg << 64);
-            s_lo = (unsigned long long)t;
-            s_hi = (unsigned long long)(t >> 64);
-          }
-          if ((ak == WARPJQ_AGG_MIN || ak == WARPJQ_AGG_MAX) && __any_sync(0xffffffffu, is_num)) {
-            // 64-bit order keys: the high words first, then the low words of
-            // the lanes that hold the extreme high word
-            const unsigned long long ob = order_bits(fv);
-            const bool mn = ak == WARPJQ_AGG_MIN;
-            const uint32_t none = mn ? 0xFFFFFFFFu : 0u;
-            const uint32_t h = is_num ? (uint32_t)(ob >> 32) : none;
-            const uint32_t eh = mn ? __reduce_min_sync(grp, h) : __reduce_max_sync(grp, h);
-            const uint32_t l = (is_num && h == eh) ? (uint32_t)ob : none;
-            const uint32_t el = mn ? __reduce_min_sync(grp, l) : __reduce_max_sync(grp, l);
-            ext = ((unsigned long long)eh << 32) | el;
-          }
+          if ((ak == WARPJQ_AGG_SUM || ak == WARPJQ_AGG_AVG) && __any_sync(0xffffffffu, num_int))
+            group_sum128(grp, num_int, iv, s_lo, s_hi);
+          if ((ak == WARPJQ_AGG_MIN || ak == WARPJQ_AGG_MAX) && __any_sync(0xffffffffu, is_num))
+            ext = group_extreme(grp, is_num, order_bits(fv), ak == WARPJQ_AGG_MIN);
           if (kid != 0xFFFFFFFFu && (lead || (is_num && !is_int))) {  // no key id: the table is full
             // This CTA's cached entry for the key if it has (or can claim)
             // one, else the global record.
@@ -1109,7 +1115,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
       }
       __syncwarp();
     }
-    if (lane == 0) c_lines += n_lines_tile;
+    if (lane == 0) acc->lines += n_lines_tile;
 
     // Per-tile bookkeeping.
     tile_first_invalid = __reduce_min_sync(0xffffffffu, tile_first_invalid);
@@ -1139,7 +1145,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
     }
     // A batch input's counts and aggregate go to its own record, tile by tile.
     if (sp.tile_input)
-      flush_counts(ctr_in, sp.ctr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, cta_fix);
+      flush_counts(ctr_in, sp.ctr, P, kRows, lane, acc, cta_fix);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
@@ -1171,7 +1177,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
   }
 
   // Flush this CTA's counters (a batch's were flushed per tile).
-  flush_counts(sp.ctr, nullptr, P, kRows, lane, c_lines, c_blank, c_invalid, c_type, c_sel, agg, cta_fix);
+  flush_counts(sp.ctr, nullptr, P, kRows, lane, acc, cta_fix);
 }
 
 // The index of the first invalid / type-error line: lines of the tiles
