@@ -3,7 +3,9 @@ cudaMalloc (an engine that owns all device memory through its own pool, or a
 caller that cannot afford cudaMalloc's device synchronisation).  It keeps all
 its scratch in one fixed device array, so this test checks that it gives the
 same answers as the allocating entry point (warpjq_launch_device /
-warpjq_collect_device) on two calls in a row.
+warpjq_collect_device) on two calls in a row, that what it returns prints
+as the oracle's output for the same bytes, and where its fixed nesting
+stack ends.
 
 The file name sorts last so a run that stops at the first failure has
 already run every other test; it also passes when run alone."""
@@ -13,6 +15,8 @@ import ctypes
 import pytest
 
 import warpjq_b200 as wjq
+from oracle import pyoracle as orc
+from tests.test_gpu_parity import close_enough
 
 pytestmark = pytest.mark.gpu
 
@@ -133,10 +137,52 @@ def test_noalloc_matches_the_allocating_entry_point():
             for f in ("n_lines", "n_blank", "n_invalid", "n_type_error", "first_invalid", "count",
                       "numeric", "isum_lo", "isum_hi", "n_int", "saw_non_numeric"):
                 assert getattr(got, f) == getattr(want, f), (ctx, f, getattr(got, f), getattr(want, f))
-            if want.numeric:
-                assert got.min == want.min and got.max == want.max, ctx
-            assert got.fsum == pytest.approx(want.fsum, rel=1e-12, abs=0.0), ctx
-            assert got.sum == pytest.approx(want.sum, rel=1e-12, abs=0.0), ctx
+            # both sum exactly and round once: the same bits, not just close
+            for f in ("min", "max", "fsum", "sum"):
+                assert getattr(got, f) == getattr(want, f), (ctx, f, getattr(got, f), getattr(want, f))
+            # and, on its own, what the oracle prints for the same bytes
+            printed = q.render_device(as_device_result(got), data)
+            oracle = orc.run(query, data)
+            assert oracle.rc == 0 and close_enough(printed, oracle.out), (ctx, printed, oracle.out)
+            assert got.n_lines == oracle.stats["lines_in"] and got.n_invalid == oracle.stats["malformed"], ctx
+        q.close()
+
+
+def as_device_result(r: NoAllocResult) -> "wjq.DeviceResult":
+    """The no-allocation result in the allocating path's result struct, so
+    the host library's formatter prints it."""
+    d = wjq.DeviceResult()
+    for f in ("n_lines", "n_blank", "n_invalid", "n_type_error", "n_selected", "first_invalid", "count",
+              "numeric", "isum_lo", "isum_hi", "n_int", "fsum", "min", "max", "sum", "saw_non_numeric"):
+        setattr(d, f, getattr(r, f))
+    return d
+
+
+def test_noalloc_nesting_limit():
+    """Lines nest in the fixed scratch up to 16,448 levels (64 in registers,
+    16,384 in the array): such a line is counted like any other; one level
+    more and the call reports status 1 instead of a wrong count."""
+    import torch
+    k, _ = wjq.libraries()
+    fn = k.warpjq_aggregate_noalloc
+    fn.argtypes = [ctypes.POINTER(Program), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                   ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    fn.restype = ctypes.c_int
+    prog, keep = lower(keys=[], agg_kind=0)
+    err = ctypes.create_string_buffer(512)
+    res = torch.zeros(ctypes.sizeof(NoAllocResult), dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    for depth, status in ((16448, 0), (16449, 1)):
+        data = b'{"a":1}\n' + b"[" * depth + b"]" * depth + b'\n{"b":2}\n'
+        dev = torch.empty(len(data) + 16, dtype=torch.uint8, device="cuda")
+        dev[: len(data)].copy_(torch.frombuffer(bytearray(data), dtype=torch.uint8))
+        assert fn(ctypes.byref(prog), dev.data_ptr(), len(data), stream.cuda_stream, res.data_ptr(), err,
+                  len(err)) == 0, err.value
+        torch.cuda.synchronize()
+        got = NoAllocResult.from_buffer_copy(bytes(res.cpu().numpy()))
+        assert got.status == status, depth
+        if status == 0:
+            assert got.count == 3 and got.n_lines == 3 and got.n_invalid == 0
 
 
 def test_noalloc_rejects_what_it_cannot_run():

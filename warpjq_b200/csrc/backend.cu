@@ -785,8 +785,8 @@ static warpjq_status fetch_groups(warpjq_ctx *ctx, Slot &s, const RunCounters &h
     g.n_int = a.n_int;
     // exact sums, rounded once (fixsum.cuh)
     g.fsum = fix_to_double(a.fix, 0, 0) + a.fbig;
-    g.min = a.numeric ? from_order_bits(a.min_bits) : 1.0 / 0.0;
-    g.max = a.numeric ? from_order_bits(a.max_bits) : -1.0 / 0.0;
+    g.min = a.numeric ? min_of_bits(a.min_bits) : __builtin_huge_val();
+    g.max = a.numeric ? max_of_bits(a.max_bits) : -__builtin_huge_val();
     g.sum = fix_to_double(a.fix, a.isum_lo, a.isum_hi) + a.fbig;
     out.push_back(g);
     if (inputs) inputs->push_back(keys[k].input);
@@ -820,8 +820,8 @@ warpjq_status warpjq_wait(warpjq_ctx *ctx, uint32_t slot, warpjq_chunk_result *o
       out->agg.count = h.agg_count;
       out->agg.numeric = h.agg_numeric;
       out->agg.sum = h.sum_total;
-      out->agg.min = h.agg_numeric ? from_order_bits(h.agg_min_bits) : 1.0 / 0.0;
-      out->agg.max = h.agg_numeric ? from_order_bits(h.agg_max_bits) : -1.0 / 0.0;
+      out->agg.min = h.agg_numeric ? min_of_bits(h.agg_min_bits) : __builtin_huge_val();
+      out->agg.max = h.agg_numeric ? max_of_bits(h.agg_max_bits) : -__builtin_huge_val();
       out->agg.saw_non_numeric = h.agg_saw_non_numeric;
     } else {
       std::vector<warpjq_group_ext> gs;
@@ -999,8 +999,8 @@ warpjq_status warpjq_collect_device(warpjq_ctx *ctx, warpjq_device_result *out, 
   out->isum_hi = h.agg_isum_hi;
   out->n_int = h.agg_n_int;
   out->fsum = h.fsum_total;
-  out->min = h.agg_numeric ? from_order_bits(h.agg_min_bits) : 1.0 / 0.0;
-  out->max = h.agg_numeric ? from_order_bits(h.agg_max_bits) : -1.0 / 0.0;
+  out->min = h.agg_numeric ? min_of_bits(h.agg_min_bits) : __builtin_huge_val();
+  out->max = h.agg_numeric ? max_of_bits(h.agg_max_bits) : -__builtin_huge_val();
   out->sum = h.sum_total;
   out->saw_non_numeric = h.agg_saw_non_numeric;
   if (P.output_kind == WARPJQ_OUT_AGG && P.group_slot >= 0) {
@@ -1159,8 +1159,8 @@ warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
     it.isum_hi = c.agg_isum_hi;
     it.n_int = c.agg_n_int;
     it.fsum = c.fsum_total;
-    it.min = c.agg_numeric ? from_order_bits(c.agg_min_bits) : 1.0 / 0.0;
-    it.max = c.agg_numeric ? from_order_bits(c.agg_max_bits) : -1.0 / 0.0;
+    it.min = c.agg_numeric ? min_of_bits(c.agg_min_bits) : __builtin_huge_val();
+    it.max = c.agg_numeric ? max_of_bits(c.agg_max_bits) : -__builtin_huge_val();
     it.sum = c.sum_total;
     it.saw_non_numeric = c.agg_saw_non_numeric;
     it.group_begin = first[i];

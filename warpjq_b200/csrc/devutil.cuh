@@ -124,6 +124,17 @@ __host__ __device__ inline double from_order_bits(unsigned long long o) {
   return d;
 }
 
+// The minimum / maximum recorded in order keys, or +inf / -inf when none
+// was: the keys start at ~0 and 0, which no number encodes, and stay there
+// when no value arrived or the aggregate does not track them (only min and
+// max queries do).
+__host__ __device__ inline double min_of_bits(unsigned long long o) {
+  return o == ~0ull ? __builtin_huge_val() : from_order_bits(o);
+}
+__host__ __device__ inline double max_of_bits(unsigned long long o) {
+  return o == 0ull ? -__builtin_huge_val() : from_order_bits(o);
+}
+
 // ---------------------------------------------------------------------------
 // JSON string decoding (json.rs:594-654): yields the decoded bytes of a
 // validated string body one at a time.  \u escapes become UTF-8; a lone

@@ -148,8 +148,8 @@ __global__ void k_noalloc_result(const RunCounters *ctr, warpjq_noalloc_result *
   r.isum_hi = c.agg_isum_hi;
   r.n_int = c.agg_n_int;
   r.fsum = c.fsum_total;  // exact sums rounded once (fixsum.cuh)
-  r.min = c.agg_numeric ? from_order_bits(c.agg_min_bits) : __longlong_as_double(0x7FF0000000000000ll);
-  r.max = c.agg_numeric ? from_order_bits(c.agg_max_bits) : -__longlong_as_double(0x7FF0000000000000ll);
+  r.min = c.agg_numeric ? min_of_bits(c.agg_min_bits) : __builtin_huge_val();
+  r.max = c.agg_numeric ? max_of_bits(c.agg_max_bits) : -__builtin_huge_val();
   r.sum = c.sum_total;
   r.saw_non_numeric = c.agg_saw_non_numeric;
   r.status = (c.overflow || c.error) ? 1u : 0u;
