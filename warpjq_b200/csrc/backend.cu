@@ -176,7 +176,8 @@ struct warpjq_ctx {
   uint32_t tile_bytes = 6144;
   uint32_t halo_bytes = 2048;
   uint32_t group_keys0 = 1u << 16;  // distinct keys a fresh group table has room for
-  unsigned grid = 0;        // persistent CTAs for the scan kernel
+  unsigned grid = 0;        // CTAs per-CTA buffers are sized for (the largest variant's grid)
+  unsigned grid_rows = 0, grid_agg = 0, grid_group = 0, grid_mixed = 0;  // persistent CTAs per variant
   size_t scan_smem = 0;
   std::vector<Slot> slots;
   // device-resident runs
@@ -231,16 +232,24 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
      "cudaFuncSetAttribute(scan grouped)");
   CK(cudaFuncSetAttribute(k_scan<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan mixed)");
-  int a = 0, b = 0;
+  // Each variant runs as many CTAs per SM as its own registers and shared
+  // memory allow; buffers sized per CTA take the largest of them.
+  int a = 0, b = 0, g = 0, m = 0;
+  const size_t grouped_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes, true);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_scan<true>, kThreads, c->scan_smem),
      "occupancy");
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scan<false>, kThreads, c->scan_smem),
      "occupancy");
-  int g = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, k_scan<false, false, true>, kThreads, c->scan_smem),
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, k_scan<false, false, true>, kThreads, grouped_smem),
      "occupancy");
-  per_sm = std::max(1, std::min(a, std::min(b, g)));
-  c->grid = (unsigned)(c->num_sms * per_sm);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_scan<false, true>, kThreads, grouped_smem),
+     "occupancy");
+  c->grid_rows = (unsigned)(c->num_sms * std::max(1, a));
+  c->grid_agg = (unsigned)(c->num_sms * std::max(1, b));
+  c->grid_group = (unsigned)(c->num_sms * std::max(1, g));
+  c->grid_mixed = (unsigned)(c->num_sms * std::max(1, m));
+  per_sm = std::max(std::max(a, b), std::max(g, m));
+  c->grid = (unsigned)(c->num_sms * std::max(1, per_sm));
   return WARPJQ_OK;
 }
 
@@ -379,7 +388,11 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       sp.in_tile0 = rb.b_in_tile0.p;
       sp.in_ctr = rb.b_in_ctr.p;
     }
-    unsigned grid = (unsigned)std::min<unsigned long long>(c->grid, n_tiles);
+    const unsigned vgrid = (b && b->mixed) ? c->grid_mixed
+                           : P.needs_rows ? c->grid_rows
+                           : groups      ? c->grid_group
+                                         : c->grid_agg;
+    unsigned grid = (unsigned)std::min<unsigned long long>(vgrid, n_tiles);
     if (!s.scan_t0 && !capturing) {
       CK(cudaEventCreate(&s.scan_t0), "event");
       CK(cudaEventCreate(&s.scan_t1), "event");
