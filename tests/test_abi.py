@@ -34,7 +34,8 @@ def test_libraries_load():
 def test_every_declared_symbol_is_exported():
     kern = exported(wjq.KERNELS_SO)
     host = exported(wjq.HOST_SO)
-    for hdr, lib in (("warpjq_kernels.h", kern), ("warpjq_ext.h", kern), ("warpjq_host.h", host)):
+    for hdr, lib in (("warpjq_kernels.h", kern), ("warpjq_ext.h", kern), ("warpjq_host.h", host),
+                     ("warpjq_serve.h", host)):
         missing = [f for f in declared_functions(hdr) if f not in lib]
         assert not missing, (hdr, missing)
     assert set(wjq.ABI_SYMBOLS) <= kern and set(wjq.EXT_SYMBOLS) <= kern

@@ -47,7 +47,8 @@ HOST_SYMBOLS = [
     "warpjq_gen_nginx", "warpjq_gen_nginx_block", "warpjq_query_open_host", "warpjq_query_is_grouped",
     "warpjq_gen_nested", "warpjq_gen_nested_block", "warpjq_query_run_file", "warpjq_query_run_csv",
     "warpjq_gen_nginx_csv", "warpjq_gen_nginx_csv_block", "warpjq_gen_nginx_csv_as_ndjson",
-    "warpjq_query_render_batch",
+    "warpjq_query_render_batch", "warpjq_serve_open", "warpjq_serve_warm", "warpjq_serve_enqueue",
+    "warpjq_serve_poll", "warpjq_serve_pending", "warpjq_serve_close",
 ]
 
 
@@ -414,9 +415,9 @@ class Query:
             raise RuntimeError(err.value.decode(errors="replace"))
 
     def batch_launch_mixed(self, queries, d_ptr: int, offsets, lengths, stream: int = 0):
-        """Enqueues one mixed batch on this (aggregate) query's context:
-        input i is d_ptr[offsets[i], + lengths[i]) and runs queries[i] (all
-        aggregate queries; each tile takes its input's plan).  Collect with
+        """Enqueues one mixed batch on this query's context: input i is
+        d_ptr[offsets[i], + lengths[i]) and runs queries[i] (aggregate or row
+        queries; each tile takes its input's plan).  Collect with
         batch_collect() and render with batch_outputs_mixed()."""
         k, _ = _load()
         n = len(offsets)

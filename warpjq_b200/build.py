@@ -4,7 +4,7 @@
   warpjq_b200/_lib/libwarpjq_kernels.a   -- the same, as the static library the
                                             reference's Rust crate links
   warpjq_b200/_lib/libwarpjq_host.so     -- the C++ host driver (query front-end,
-                                            pipeline, formatting)
+                                            pipeline, formatting, serving loop)
 
 Run: python -m warpjq_b200.build   (nvcc cross-compiles; no GPU needed)
 """
@@ -26,8 +26,10 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 KERNEL_SRCS = [os.path.join(CSRC, "backend.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "csv.cu")]
 KERNEL_DEPS = [os.path.join(CSRC, f) for f in ("kernels.cuh", "walker.cuh", "devutil.cuh", "fixsum.cuh", "plan.h",
                                                "plan_build.h", "csv_rows.cuh")]
-HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc")]
-HEADERS = [os.path.join(ROOT, "include", f) for f in ("warpjq_kernels.h", "warpjq_ext.h", "warpjq_host.h")]
+HOST_SRCS = [os.path.join(CSRC, "host", f) for f in ("query.cc", "engine.cc", "gen.cc", "serve.cc")]
+HEADERS = [os.path.join(ROOT, "include", f)
+           for f in ("warpjq_kernels.h", "warpjq_ext.h", "warpjq_host.h", "warpjq_serve.h")]
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 EXPORTS = os.path.join(CSRC, "exports.map")  # only the C ABI is exported
 
 
@@ -67,8 +69,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> None:
     hdeps = HOST_SRCS + [os.path.join(CSRC, "host", "query.h")] + HEADERS + [so, EXPORTS]
     if force or _stale(host, hdeps):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wl,--version-script=" + EXPORTS, "-o", host,
-              *HOST_SRCS,
-              "-L" + LIB, "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+              *HOST_SRCS, "-I" + os.path.join(CUDA_HOME, "include"),
+              "-L" + LIB, "-lwarpjq_kernels", "-Wl,-rpath,$ORIGIN",
+              # the serving loop's streams, events and copies: the CUDA runtime, linked in statically
+              os.path.join(CUDA_HOME, "lib64", "libcudart_static.a"), "-ldl", "-lrt", "-lpthread"])
 
 
 if __name__ == "__main__":

@@ -190,8 +190,10 @@ struct warpjq_ctx {
   struct Batch {
     bool active = false;
     bool tables_on_device = false;  // enqueue without uploading the tables (graph capture)
-    // a mixed batch: input i runs plans[in_plan[i]] (aggregate plans only)
-    bool mixed = false, any_grouped = false;
+    // a mixed batch: input i runs plans[in_plan[i]]; any_rows when one of
+    // them prints rows (records then take the largest plan's stride)
+    bool mixed = false, any_grouped = false, any_rows = false;
+    uint32_t rec_stride = 0;
     std::vector<DevPlan> plans;
     std::vector<uint32_t> in_plan;
     uint64_t epoch = 0;             // bumped whenever a plain batch replaces the device tables
@@ -256,16 +258,15 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
 // Sizes the buffers of `s` for an input of n bytes (first use, or growth).
 warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
                           unsigned long long n_tiles, cudaStream_t st, bool cap, char *err, size_t err_len,
-                          bool grouped) {
+                          bool grouped, bool rows, uint32_t rec_stride) {
   RunBufs &rb = s.rb;
-  const DevPlan &P = c->plan;
   if (n_tiles == 0) n_tiles = 1;
   CK(rb.ctr.ensure(1, st, cap), "alloc counters");
   CK(rb.tiles.ensure(n_tiles, st, cap), "alloc tiles");
   CK(rb.block_lines.ensure(2 * kReduceBlocks, st, cap), "alloc reduce");
   if (!rb.deep_levels) rb.deep_levels = 1u << 16;
   CK(rb.deep.ensure((size_t)c->grid * (rb.deep_levels / 32), st, cap), "alloc deep stack");
-  if (P.needs_rows) {
+  if (rows) {
     CK(rb.row_tiles.ensure(n_tiles, st, cap), "alloc row tiles");
     CK(rb.row_bsum.ensure(3 * ((n_tiles + 31) / 32), st, cap), "alloc row prefixes");
     // Records accumulate over all of a CTA's tiles: room for a row per KiB
@@ -273,7 +274,7 @@ warpjq_status ensure_bufs(warpjq_ctx *c, Slot &s, unsigned long long n,
     // input's size too (a larger input than the last does not overflow
     // for that reason alone).
     rb.rec_cap_per_cta = std::max(rb.rec_cap_per_cta, n / 1024 / std::max(1u, c->grid) + 1024);
-    CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * P.rec_stride, st, cap), "alloc records");
+    CK(rb.recs.ensure((size_t)c->grid * rb.rec_cap_per_cta * rec_stride, st, cap), "alloc records");
     rb.out_cap = std::max(rb.out_cap, n + n / 4 + (1u << 20));
     CK(rb.out.ensure(rb.out_cap, st, cap), "alloc output");
     rb.rows_cap = std::max(rb.rows_cap, n / 32 + 4096);
@@ -299,6 +300,17 @@ bool run_grouped(const warpjq_ctx *c, const warpjq_ctx::Batch *b) {
   return c->plan.output_kind == WARPJQ_OUT_AGG && c->plan.group_slot >= 0;
 }
 
+// Whether a run prints rows (the context's plan does, or one of a mixed
+// batch's plans does), and the bytes of its row records.
+bool run_rows(const warpjq_ctx *c, const warpjq_ctx::Batch *b) {
+  if (b && b->mixed) return b->any_rows;
+  return c->plan.needs_rows != 0;
+}
+uint32_t run_rec_stride(const warpjq_ctx *c, const warpjq_ctx::Batch *b) {
+  if (b && b->mixed) return b->rec_stride;
+  return c->plan.rec_stride;
+}
+
 GroupTable group_view(RunBufs &rb, bool on) {
   GroupTable g{};
   if (!on) return g;
@@ -320,7 +332,9 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(st, &cap), "capture status");
   const bool capturing = cap != cudaStreamCaptureStatusNone;
-  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, st, capturing, err, err_len, run_grouped(c, b));
+  const bool rows = run_rows(c, b);
+  warpjq_status rc = ensure_bufs(c, s, n, n_tiles, st, capturing, err, err_len, run_grouped(c, b), rows,
+                                 run_rec_stride(c, b));
   if (rc != WARPJQ_OK) return rc;
   RunBufs &rb = s.rb;
   const DevPlan &P = c->plan;
@@ -376,10 +390,12 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.g = g;
     sp.deep_words = rb.deep.p;
     sp.deep_levels_per_cta = rb.deep_levels;
+    sp.rec_stride = run_rec_stride(c, b);
     if (b && b->mixed) {
       sp.plans = rb.b_plans.p;
       sp.in_plan = rb.b_in_plan.p;
       sp.any_grouped = b->any_grouped ? 1u : 0u;
+      sp.any_rows = b->any_rows ? 1u : 0u;
     }
     if (b) {
       sp.tile_input = rb.b_tile_input.p;
@@ -411,7 +427,7 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     s.kernels++;
     CK(cudaGetLastError(), "launch scan");
     if (s.timed) CK(cudaEventRecord(s.scan_t1, st), "event record");
-    if (P.needs_rows) {
+    if (rows) {
       const uint32_t tpb = rows_tiles_per_block(n_tiles);
       const unsigned nb = (unsigned)((n_tiles + tpb - 1) / tpb);
       k_rows_block_sums<<<nb, kEmitThreads, 0, st>>>(rb.row_tiles.p, rb.tiles.p, n_tiles, tpb,
@@ -421,6 +437,12 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       EmitParams ep{};
       ep.data = d_data;
       ep.plan = c->d_plan;
+      ep.rec_stride = sp.rec_stride;
+      if (b && b->mixed) {
+        ep.plans = rb.b_plans.p;
+        ep.in_plan = rb.b_in_plan.p;
+        ep.tile_input = rb.b_tile_input.p;
+      }
       ep.row_tiles = rb.row_tiles.p;
       ep.tiles = rb.tiles.p;
       ep.n_tiles = n_tiles;
@@ -636,7 +658,8 @@ warpjq_status warpjq_ctx_create(const warpjq_program *prog, uint64_t max_chunk_b
     CK(cudaHostAlloc((void **)&s.h_ctr, sizeof(RunCounters), cudaHostAllocDefault), "pinned ctr");
     if (max_chunk_bytes) {
       rc = ensure_bufs(c.get(), s, max_chunk_bytes, (max_chunk_bytes + c->tile_bytes - 1) / c->tile_bytes,
-                       s.stream, false, err, err_len, run_grouped(c.get(), nullptr));
+                       s.stream, false, err, err_len, run_grouped(c.get(), nullptr), run_rows(c.get(), nullptr),
+                       run_rec_stride(c.get(), nullptr));
       if (rc != WARPJQ_OK) return rc;
       CK(cudaStreamSynchronize(s.stream), "stream sync");
     }
@@ -1066,7 +1089,8 @@ static warpjq_status batch_prepare(warpjq_ctx *ctx, const uint8_t *d_data, const
   }
   b.tile0[n_inputs] = tiles;
   b.n_tiles = tiles;
-  b.mixed = b.any_grouped = false;
+  b.mixed = b.any_grouped = b.any_rows = false;
+  b.rec_stride = 0;
   b.plans.clear();
   b.in_plan.clear();
   return WARPJQ_OK;
@@ -1087,16 +1111,12 @@ warpjq_status warpjq_batch_launch_mixed(warpjq_ctx *ctx, warpjq_ctx *const *inpu
                                         const uint64_t *offsets, const uint64_t *lengths, uint32_t n_inputs,
                                         void *stream, char *err, size_t err_len) {
   if (!ctx || (n_inputs && !input_ctx)) return WARPJQ_ERR_INVALID_ARG;
-  if (ctx->plan.output_kind != WARPJQ_OUT_AGG) {
-    set_err(err, err_len, "a mixed batch runs on an aggregate query's context");
-    return WARPJQ_ERR_INVALID_ARG;
-  }
   std::vector<const warpjq_ctx *> distinct;
   std::vector<uint32_t> in_plan(n_inputs);
   for (uint32_t i = 0; i < n_inputs; i++) {
     const warpjq_ctx *q = input_ctx[i];
-    if (!q || q->plan.output_kind != WARPJQ_OUT_AGG) {
-      set_err(err, err_len, "input %u of a mixed batch does not have an aggregate query", i);
+    if (!q) {
+      set_err(err, err_len, "input %u of a mixed batch has no query context", i);
       return WARPJQ_ERR_INVALID_ARG;
     }
     uint32_t k = 0;
@@ -1108,9 +1128,12 @@ warpjq_status warpjq_batch_launch_mixed(warpjq_ctx *ctx, warpjq_ctx *const *inpu
   if (rc != WARPJQ_OK) return rc;
   warpjq_ctx::Batch &b = ctx->batch;
   b.mixed = true;
+  b.rec_stride = kRowRecBytes;
   for (const warpjq_ctx *q : distinct) {
     b.plans.push_back(q->plan);
-    b.any_grouped = b.any_grouped || q->plan.group_slot >= 0;
+    b.any_grouped = b.any_grouped || (q->plan.output_kind == WARPJQ_OUT_AGG && q->plan.group_slot >= 0);
+    b.any_rows = b.any_rows || q->plan.needs_rows;
+    b.rec_stride = std::max(b.rec_stride, q->plan.rec_stride);
   }
   if (b.plans.empty()) b.plans.push_back(ctx->plan);
   b.in_plan = std::move(in_plan);
@@ -1159,7 +1182,8 @@ warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
     it.n_blank = c.n_blank;
     it.n_invalid = c.n_invalid;
     it.n_type_error = c.n_type_error;
-    it.n_selected = P.output_kind == WARPJQ_OUT_AGG ? 0 : c.n_selected;
+    const DevPlan &Pi = b.mixed ? b.plans[b.in_plan[i]] : P;
+    it.n_selected = Pi.output_kind == WARPJQ_OUT_AGG ? 0 : c.n_selected;
     it.first_invalid = c.first_invalid;
     it.first_type_error = c.first_type_error;
     it.row_begin = rows;
@@ -1185,10 +1209,18 @@ warpjq_status warpjq_batch_collect(warpjq_ctx *ctx, warpjq_batch_item *items,
     all->n_blank = h.n_blank;
     all->n_invalid = h.n_invalid;
     all->n_type_error = h.n_type_error;
-    all->n_selected = h.n_selected;
+    // rows of the batch: every selected line, except a mixed batch's
+    // aggregate inputs' (their selected lines print no row)
+    unsigned long long n_rows = h.n_selected;
+    if (b.mixed) {
+      n_rows = 0;
+      for (uint32_t i = 0; i < n; i++)
+        if (b.plans[b.in_plan[i]].output_kind != WARPJQ_OUT_AGG) n_rows += b.h_ctr[i].n_selected;
+    }
+    all->n_selected = n_rows;
     all->first_invalid = ~0ull;
     all->first_type_error = ~0ull;
-    if (P.needs_rows) {
+    if (run_rows(ctx, &b)) {
       all->d_out_bytes = s.rb.out.p;
       all->out_len = h.out_len;
       all->d_out_line_idx = (const uint64_t *)s.rb.line_idx.p;

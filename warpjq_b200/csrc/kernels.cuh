@@ -210,12 +210,20 @@ struct ScanParams {
   const DevPlan *plans;
   const uint32_t *in_plan;
   uint32_t any_grouped;
+  uint32_t any_rows;    // a mixed batch: one of the plans prints rows
+  uint32_t rec_stride;  // bytes per row record (a mixed batch: the largest of its plans')
 };
 
 // Rows emission.
 struct EmitParams {
   const uint8_t *data;
   const DevPlan *plan;
+  // A mixed batch: tile t's rows are rendered by plans[in_plan[tile_input[t]]]
+  // (null otherwise).
+  const DevPlan *plans;
+  const uint32_t *in_plan;
+  const uint32_t *tile_input;
+  uint32_t rec_stride;
   const RowTile *row_tiles;
   const TileDesc *tiles;
   unsigned long long n_tiles;
@@ -681,8 +689,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
   GroupCache *gcache = (GroupCache *)(smem + scan_smem_base(T, H));  // grouped aggregates only
 
   const int lane = threadIdx.x;
-  const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
-  const uint32_t rec_stride = P.rec_stride;
+  const uint32_t rec_stride = sp.rec_stride;
   uint8_t *my_recs = sp.rec_scratch + (unsigned long long)blockIdx.x * sp.rec_cap_per_cta * rec_stride;
   DeepStack deep;
   deep.words = sp.deep_words + (unsigned long long)blockIdx.x * (sp.deep_levels_per_cta / 32);
@@ -728,6 +735,9 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
     }
     // The tile's plan (a mixed batch: its input's own).
     const DevPlan &P = kMulti ? sp.plans[sp.in_plan[input]] : plan;
+    // Whether the tile's query prints rows (a mixed batch holds both kinds).
+    const bool rowsT = kMulti ? P.needs_rows != 0 : kRows;
+    const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
     const unsigned long long te = min(ts + T, data_end);
     const uint32_t tlen = (uint32_t)(te - ts);
     const uint32_t wlen = (uint32_t)min((unsigned long long)T + H, data_end - ts);
@@ -928,7 +938,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         } else if (status == LS_TYPE_ERROR) {
           tile_first_type = min(tile_first_type, ordinal);
         } else if (status == 101) {
-          if (kRows) {
+          if (rowsT) {
             has_row = 1;
             row_len = row_length(P, lp, out_len, slots);
           } else {
@@ -964,7 +974,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         }
 
         // Aggregate contribution of this line.
-        bool contrib = !kRows && status == 101;
+        bool contrib = !rowsT && status == 101;
         long long iv = 0;
         double fv = 0.0;
         bool is_int = false, is_num = false;
@@ -1018,7 +1028,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
             }
           }
         }
-        if (kGroups && !kRows && P.group_slot >= 0) {
+        if (kGroups && !rowsT && P.group_slot >= 0) {
           // Lanes whose keys hash alike compare their key bytes with the
           // lowest such lane; only lanes that differ from it look up the
           // table themselves.
@@ -1085,7 +1095,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
             sp.g.keys[kid].saw_non_numeric = 1;
         }
 
-        if (kRows) {
+        if (rowsT) {
           uint32_t er, tr;
           unsigned long long eb, tb;
           warp_scan2(has_row, (unsigned long long)row_len, er, eb, tr, tb);
@@ -1133,7 +1143,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         if (sp.tile_input) atomicMin(&ctr_in->first_type_tile, tile);
       }
     }
-    if (kRows) {
+    if (rowsT || (kMulti && sp.any_rows)) {  // an aggregate tile of a batch with rows has none
       if (lane == 0) {
         RowTile rt;
         rt.rec_begin = (unsigned long long)blockIdx.x * sp.rec_cap_per_cta + tile_rec0;
@@ -1145,7 +1155,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
     }
     // A batch input's counts and aggregate go to its own record, tile by tile.
     if (sp.tile_input)
-      flush_counts(ctr_in, sp.ctr, P, kRows, lane, acc, cta_fix);
+      flush_counts(ctr_in, sp.ctr, P, rowsT, lane, acc, cta_fix);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
@@ -1386,9 +1396,8 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
   __shared__ unsigned long long s_rec[kEmitThreads];
   __shared__ uint32_t s_rows[kEmitThreads];
   if (ep.ctr->overflow & 3u) return;  // the run is repeated with bigger buffers
-  const DevPlan &P = *ep.plan;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t rec_stride = P.rec_stride;
+  const uint32_t rec_stride = ep.rec_stride;
   unsigned long long carry[3];
   for (int k = 0; k < 3; k++) carry[k] = ep.block_prefix[blockIdx.x * 3 + k];
   const uint32_t tpb = ep.tiles_per_block;
@@ -1414,6 +1423,8 @@ __global__ void __launch_bounds__(kEmitThreads) k_rows_emit(EmitParams ep) {
     const int n_here = (int)min((uint32_t)kEmitThreads, tpb - sub);
     for (int i = warp; i < n_here; i += kEmitThreads / 32) {
       const uint32_t rows = s_rows[i];
+      if (!rows) continue;
+      const DevPlan &P = ep.plans ? ep.plans[ep.in_plan[ep.tile_input[t0 + sub + i]]] : *ep.plan;
       const unsigned long long row0 = s_pre[0][i], byte0 = s_pre[1][i], line0 = s_pre[2][i];
       for (uint32_t r = 0; r < rows; r++) {
         const RowRec *rr = (const RowRec *)(ep.recs + (s_rec[i] + r) * rec_stride);

@@ -618,6 +618,13 @@ __device__ __forceinline__ uint32_t pop_special(const uint32_t *sm, uint32_t &k,
 // values; for any other line (whitespace, arrays, escaped keys, deeper
 // nesting, anything malformed) it returns LS_FALLBACK and records nothing
 // that walk_masked does not overwrite.  Same window contract as walk_masked.
+//
+// Checks whose outcome does not steer the walk (that a key's quotes are
+// quotes where they were expected, the ':' after it, an escape's letter)
+// are folded into `bad` and decided once, when the line's object closes, so
+// the shared-memory loads behind them do not stall each step.  Every pop is
+// bounded by the line's newline (a special byte), so a walk over a line of
+// another shape still ends at e.
 __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, const uint32_t *sm,
                                             uint32_t s, uint32_t e, NodeVals &v) {
   using namespace detail;
@@ -637,16 +644,18 @@ __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, 
   uint32_t k = (s + 1) >> 5;
   uint32_t m = sm[k] & (0xFFFFFFFFu << ((s + 1) & 31u));
   uint32_t p = s + 1;  // where the next key's opening quote must be
+  uint32_t bad = 0;    // deferred checks: nonzero when the line is not of this shape
   for (;;) {
     const uint32_t q0 = pop_special(sm, k, m);
-    if (q0 != p || w[q0] != '"') return LS_FALLBACK;
+    if (q0 >= e) return LS_FALLBACK;
     const uint32_t q1 = pop_special(sm, k, m);
-    if (w[q1] != '"') return LS_FALLBACK;
+    if (q1 >= e) return LS_FALLBACK;
+    bad |= (q0 ^ p) | ((uint32_t)w[q0] ^ '"') | ((uint32_t)w[q1] ^ '"');
     uint32_t vn = kNoNode;
     const uint32_t kl = q1 - q0 - 1;
     if ((lm >> (kl < 63u ? kl : 63u)) & 1ull) vn = match_key_win(P, (uint8_t)cur, w, q0 + 1, kl, false);
     const uint32_t la = load4(w, q1 + 1);
-    if ((la & 0xFFu) != ':') return LS_FALLBACK;
+    bad |= (la & 0xFFu) ^ ':';
     const uint32_t c = (la >> 8) & 0xFFu;
     const uint32_t vs = q1 + 2;
     if (vn != kNoNode) {
@@ -666,7 +675,9 @@ __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, 
     }
     uint32_t ve;
     if (c == '"') {
-      pop_special(sm, k, m);  // the opening quote, at vs
+      const uint32_t r0 = pop_special(sm, k, m);  // the opening quote, at vs
+      if (r0 >= e) return LS_FALLBACK;
+      bad |= r0 ^ vs;
       bool esc = false;
       uint32_t r;
       for (;;) {
@@ -677,11 +688,11 @@ __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, 
         esc = true;
         const uint32_t x = w[r + 1];
         if (x == '"' || x == '\\') {
-          pop_special(sm, k, m);  // the escaped byte is special itself
+          pop_special(sm, k, m);  // the escaped byte is special itself (r + 1 < e)
         } else if (x == 'u') {
-          if (!hex4_at(w, r + 2)) return LS_FALLBACK;
-        } else if (!simple_escape(x)) {
-          return LS_FALLBACK;
+          bad |= hex4_at(w, r + 2) ? 0u : 1u;
+        } else {
+          bad |= simple_escape(x) ? 0u : 1u;  // a special x stops the next pop
         }
       }
       ve = r + 1;
@@ -696,7 +707,7 @@ __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, 
     uint32_t t = w[ve];
     while (t == '}') {
       if (cur != kNoNode) v.len[cur] = ve + 1 - s - v.off[cur];
-      if (--depth == 0) return ve + 1 == e ? LS_OK : LS_FALLBACK;
+      if (--depth == 0) return (ve + 1 == e && !bad) ? LS_OK : LS_FALLBACK;
       cur = (uint32_t)(stack & 0xFFu);
       stack >>= 8;
       lm = cur != kNoNode ? P.nodes[cur].key_len_mask : 0ull;

@@ -349,3 +349,136 @@ def _device_tensor(ptr: int, n: int):
     import torch
     from .shard import _DeviceBytes
     return torch.as_tensor(_DeviceBytes(ptr, n), device="cuda")
+
+
+# ---------------------------------------------------------------------------
+# The native server (include/warpjq_serve.h): the same continuous batching,
+# with the loop, admission, placement and rendering in a C++ thread.
+# ---------------------------------------------------------------------------
+
+import ctypes as _ct
+
+
+class _ServeConfig(_ct.Structure):
+    _fields_ = [("n_slots", _ct.c_uint32), ("max_batch", _ct.c_uint32), ("budget_bytes", _ct.c_uint64),
+                ("format", _ct.c_uint32), ("mixed_min", _ct.c_uint32), ("chunk_bytes", _ct.c_uint64)]
+
+
+class _ServeResult(_ct.Structure):
+    _fields_ = [("id", _ct.c_uint64), ("query", _ct.c_uint32), ("rc", _ct.c_int32), ("out", _ct.c_void_p),
+                ("out_len", _ct.c_uint64), ("n_lines", _ct.c_uint64), ("n_invalid", _ct.c_uint64),
+                ("queue_ms", _ct.c_double), ("latency_ms", _ct.c_double), ("err", _ct.c_char * 160)]
+
+
+SERVE_DEVICE = 1
+SERVE_CSV = 2
+
+
+@dataclass
+class NativeResult:
+    id: int
+    query: int
+    rc: int
+    out: bytes
+    n_lines: int
+    n_invalid: int
+    queue_ms: float
+    latency_ms: float
+    error: str
+
+
+class NativeServer:
+    """Binding of the native serving loop (warpjq_serve_*).  submit() queues
+    a request and returns its id (the input must stay alive and unchanged
+    until its result is polled: the server keeps a reference to it here);
+    poll() returns finished requests; drain() waits for all of them."""
+
+    def __init__(self, queries, n_slots: int = 3, budget_bytes: int = 120 << 30, fmt_out: str = "ndjson",
+                 max_batch: int = 0, mixed_min: int = MIXED_MIN, chunk_bytes: int = 1 << 20):
+        from . import FORMATS, _load
+        _, h = _load()
+        self._h = h
+        vp, u32, u64, cp = _ct.c_void_p, _ct.c_uint32, _ct.c_uint64, _ct.c_char_p
+        h.warpjq_serve_open.argtypes = [_ct.POINTER(cp), u32, _ct.POINTER(_ServeConfig), _ct.POINTER(vp), cp,
+                                        _ct.c_size_t]
+        h.warpjq_serve_open.restype = _ct.c_int
+        h.warpjq_serve_warm.argtypes = [vp, u64, cp, _ct.c_size_t]
+        h.warpjq_serve_warm.restype = _ct.c_int
+        h.warpjq_serve_enqueue.argtypes = [vp, u32, vp, u64, u32, _ct.POINTER(u64), cp, _ct.c_size_t]
+        h.warpjq_serve_enqueue.restype = _ct.c_int
+        h.warpjq_serve_poll.argtypes = [vp, _ct.POINTER(_ServeResult), u32, _ct.c_int]
+        h.warpjq_serve_poll.restype = u32
+        h.warpjq_serve_pending.argtypes = [vp]
+        h.warpjq_serve_pending.restype = u64
+        h.warpjq_serve_close.argtypes = [vp]
+        h.warpjq_serve_close.restype = None
+        self.queries = list(dict.fromkeys(queries))
+        self._index = {q: i for i, q in enumerate(self.queries)}
+        arr = (cp * len(self.queries))(*[q.encode() for q in self.queries])
+        cfg = _ServeConfig(n_slots, max_batch, budget_bytes, FORMATS[fmt_out], mixed_min, chunk_bytes)
+        self._s = vp()
+        err = _ct.create_string_buffer(1024)
+        rc = h.warpjq_serve_open(arr, len(self.queries), _ct.byref(cfg), _ct.byref(self._s), err, len(err))
+        if rc:
+            raise RuntimeError(err.value.decode(errors="replace"))
+        self._keep = {}  # request id -> the input object (kept alive until polled)
+        self._buf = (_ServeResult * 256)()
+
+    def warm(self, reserve_bytes: int = 64 << 20):
+        err = _ct.create_string_buffer(1024)
+        if self._h.warpjq_serve_warm(self._s, reserve_bytes, err, len(err)):
+            raise RuntimeError(err.value.decode(errors="replace"))
+
+    def submit(self, query: str, data, fmt: str = "ndjson") -> int:
+        """Queues `query` over `data`: bytes / a numpy uint8 array (host) or
+        a CUDA uint8 tensor (device, used in place when 16-byte aligned)."""
+        flags = SERVE_CSV if fmt == "csv" else 0
+        if hasattr(data, "is_cuda") and data.is_cuda:
+            flags |= SERVE_DEVICE
+            ptr, n = data.data_ptr(), int(data.numel())
+        elif isinstance(data, (bytes, bytearray)):
+            data = np.frombuffer(data, dtype=np.uint8)
+            ptr, n = data.ctypes.data, data.size
+        else:
+            data = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+            ptr, n = data.ctypes.data, data.size
+        rid = _ct.c_uint64()
+        err = _ct.create_string_buffer(512)
+        if self._h.warpjq_serve_enqueue(self._s, self._index[query], ptr, n, flags, _ct.byref(rid), err, len(err)):
+            raise RuntimeError(err.value.decode(errors="replace"))
+        self._keep[rid.value] = data
+        return rid.value
+
+    def poll(self, timeout_ms: int = 0) -> list:
+        n = self._h.warpjq_serve_poll(self._s, self._buf, len(self._buf), timeout_ms)
+        out = []
+        for i in range(n):
+            r = self._buf[i]
+            body = _ct.string_at(r.out, r.out_len) if r.out else b""
+            if r.out:
+                self._h.warpjq_host_free(_ct.c_void_p(r.out))
+            self._keep.pop(r.id, None)
+            out.append(NativeResult(r.id, r.query, r.rc, body, r.n_lines, r.n_invalid, r.queue_ms, r.latency_ms,
+                                    r.err.decode(errors="replace")))
+        return out
+
+    def pending(self) -> int:
+        return int(self._h.warpjq_serve_pending(self._s))
+
+    def drain(self) -> list:
+        out = []
+        while self.pending():
+            out += self.poll(timeout_ms=-1)
+        return out
+
+    def close(self):
+        if self._s:
+            self._h.warpjq_serve_close(self._s)
+            self._s = _ct.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
