@@ -204,19 +204,20 @@ def device_output(Q, r, host_data) -> bytes:
     return _d2h(r.d_out_bytes, r.out_len) if r.out_len else b""
 
 
-def batch_workload(hnp, n, n_inputs=4096, lo=4096, hi=4 << 20, seed=7):
-    """Device-resident batch inputs: newline-aligned slices of the bench
-    input with log-uniform sizes, packed at 16-byte aligned offsets, and a
-    query index per input drawn uniformly from BATCH_QUERIES."""
+def batch_workload(dsrc, hnp, n, n_inputs=4096, lo=4096, hi=64 << 20, seed=7):
+    """Device-resident batch inputs (the batching configuration): 4096
+    newline-aligned slices of the bench input with log-uniform sizes of
+    4 KB - 64 MB, packed on the device at 16-byte aligned offsets, and a
+    query index per input drawn uniformly from BATCH_QUERIES.  `dsrc` is the
+    bench input on the device, `hnp` its host copy (for the cut points)."""
     import math
     import random
-    import numpy as np
     import torch
     rng = random.Random(seed)
     spans, pos = [], 0
     for _ in range(n_inputs):
         sz = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
-        if pos + sz >= n:
+        if pos + sz + 4096 >= n:
             pos = 0
         end = pos + sz
         k = bytes(hnp[end - 1:min(n, end + 4096)]).find(b"\n")
@@ -229,12 +230,9 @@ def batch_workload(hnp, n, n_inputs=4096, lo=4096, hi=4 << 20, seed=7):
         total = (total + 15) & ~15
         offs.append(total)
         total += b - a
-    packed = torch.empty(total + 16, dtype=torch.uint8).pin_memory()
-    pn = packed.numpy()
-    for (a, b), o in zip(spans, offs):
-        pn[o:o + (b - a)] = hnp[a:b]
     dev = torch.empty(total + 16, dtype=torch.uint8, device="cuda")
-    dev.copy_(packed)
+    for (a, b), o in zip(spans, offs):
+        dev[o:o + (b - a)].copy_(dsrc[a:b])
     torch.cuda.synchronize()
     return dev, offs, [b - a for a, b in spans], qidx
 
@@ -284,22 +282,15 @@ def measure_batch(wjq, dev, offs, lens, qidx):
         for k in range(len(groups)):
             graph_q[k].batch_collect()
 
-    # mixed: the aggregate queries' inputs in one launch, each input with
-    # its own plan; the two row queries as batches of their own
-    agg_k = [k for k, q in enumerate(batch_q) if q.is_aggregate]
-    row_k = [k for k in range(len(BATCH_QUERIES)) if k not in agg_k]
-    mixed_in = [i for i in range(len(offs)) if qidx[i] in agg_k]
-    driver = wjq.Query(BATCH_QUERIES[agg_k[0]], chunk_bytes=1 << 20)
-    tune.apply(driver, tuned[BATCH_QUERIES[agg_k[0]]])
+    # mixed: every input in one launch sequence, each with its own plan
+    # (aggregate and row queries alike)
+    driver = wjq.Query(BATCH_QUERIES[0], chunk_bytes=1 << 20)
+    tune.apply(driver, tuned[BATCH_QUERIES[0]])
+    every = list(range(len(offs)))
 
     def mixed():
-        driver.batch_launch_mixed([batch_q[qidx[i]] for i in mixed_in], ptr, [offs[i] for i in mixed_in],
-                                  [lens[i] for i in mixed_in], stream)
-        for k in row_k:
-            batch_q[k].batch_launch(ptr, [offs[i] for i in groups[k]], [lens[i] for i in groups[k]], stream)
+        driver.batch_launch_mixed([batch_q[qidx[i]] for i in every], ptr, offs, lens, stream)
         driver.batch_collect()
-        for k in row_k:
-            batch_q[k].batch_collect()
 
     out = {}
     for name, fn in (("plain", plain), ("batched", batched), ("graph", replay), ("mixed", mixed)):
@@ -311,8 +302,8 @@ def measure_batch(wjq, dev, offs, lens, qidx):
         out[name] = time.perf_counter() - t0
     graph.close()
     return {"inputs": len(offs), "bytes": total,
-            "sizes": "log-uniform 4 KiB - 4 MiB (rescaled from 4 KB - 64 MB, whose ~28 GB does not "
-                     "fit the bench's time budget)",
+            "sizes": "log-uniform 4 KB - 64 MB (the configuration's sizes; 4096 of them total "
+                     "about 28 GB, not the configuration's approximate 8 GB)",
             "queries": len(BATCH_QUERIES), "residency": "device",
             "plain_gbs": round(total / out["plain"] / 1e9, 3),
             "batched_gbs": round(total / out["batched"] / 1e9, 3),
@@ -320,12 +311,13 @@ def measure_batch(wjq, dev, offs, lens, qidx):
             "plain_s": round(out["plain"], 4), "batched_s": round(out["batched"], 4),
             "graph_s": round(out["graph"], 4),
             "mixed_gbs": round(total / out["mixed"] / 1e9, 3),
-            "mixed": "the 6 aggregate queries' inputs in one launch, each with its own plan, "
-                     "plus one batch per row query",
+            "mixed": "all 4096 inputs in one launch sequence, each with its own plan (8 queries: "
+                     "aggregates, projection and passthrough)",
             "graph": "one CUDA graph: the 8 queries' batches captured on forked streams, one launch",
             "speedup": round(out["plain"] / out["batched"], 2),
             "graph_speedup": round(out["plain"] / out["graph"], 2),
-            "tuned": {q: {"tile": c["tile"], "halo": c["halo"], "group_keys": c["group_keys"],
+            "tuned": {q: {"lines_per_warp": c["lines_per_warp"], "tile": c["tile"], "halo": c["halo"],
+                          "group_keys": c["group_keys"],
                           "gbs": c["gbs"], "autotile": c["autotile"], "autotile_gbs": c["autotile_gbs"]}
                       for q, c in tuned.items()}}
 
@@ -337,91 +329,148 @@ SERVE_QUERIES = BATCH_QUERIES + [
 ]
 
 
-def serve_csv_inputs(wjq, n_inputs=512, lo=4096, hi=4 << 20, seed=13):
-    """Device-resident CSV requests: a header row and a run of rows of the
-    nginx records as CSV, log-uniform sizes; a list of device tensors."""
+def serve_pool(wjq, dsrc, hnp, n, n_req, seed=11, lo=1 << 10, hi=256 << 20, csv_share=0.2, host_share=0.3):
+    """The serving configuration's requests: sizes log-uniform 1 KB - 256 MB,
+    one of SERVE_QUERIES each, 20% CSV (32 distinct CSV inputs of such sizes,
+    a header row and a run of the nginx records' rows, reused), the NDJSON
+    ones newline-aligned slices of the bench input starting on a 16-byte
+    aligned line start, 30% of them read from page-locked host memory and
+    the rest from device memory in place.  Returns (requests, keep) with
+    requests as (query, data, fmt, nbytes)."""
     import math
     import random
+    import numpy as np
     import torch
     rng = random.Random(seed)
-    buf, used, _ = wjq.gen_nginx_csv(256 << 20, seed=seed)
-    raw = bytes(buf[:used])
-    head_end = raw.index(b"\n") + 1
-    head = raw[:head_end]
-    parts, pos = [], head_end
-    for _ in range(n_inputs):
-        sz = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
-        if pos + sz >= used:
-            pos = head_end
-        end = raw.index(b"\n", pos + sz - 1) + 1 if raw.find(b"\n", pos + sz - 1) >= 0 else used
-        parts.append(head + raw[pos:end])
-        pos = end
-    return [torch.frombuffer(bytearray(p), dtype=torch.uint8).cuda() for p in parts]
-
-
-def measure_serving(wjq, dev, offs, lens, csv_inputs, rate=2000.0, n_req=4096, seed=11):
-    """Open-loop Poisson arrivals at `rate` req/s, 16 queries, 20% of the
-    requests CSV, all inputs device-resident.  "batched": the continuous-
-    batching server (warpjq_b200/serve.py: 3 slots, every arrived request
-    that fits the 120 GB budget joins the next free slot, slots overlap on
-    the device); "one_at_a_time": the same server with one slot taking one
-    request at a time.  Latency = completion - arrival (wall clock)."""
-    import random
-    import torch
-    from warpjq_b200.serve import Server
-    rng = random.Random(seed)
+    size = lambda: int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+    buf, used, _ = wjq.gen_nginx_csv(1 << 30, seed=seed)
+    raw = np.asarray(buf[:used])
+    head_end = int(bytes(raw[:4096]).index(b"\n")) + 1
+    csv_pool = []
+    for k in range(32):
+        sz = min(size(), used - head_end - 8192)
+        a = rng.randrange(head_end, used - sz - 4096)
+        a += bytes(raw[a:a + 8192]).index(b"\n") + 1
+        e = a + sz
+        e += bytes(raw[e:e + 8192]).index(b"\n") + 1
+        h = torch.empty(head_end + e - a, dtype=torch.uint8).pin_memory()
+        hn = h.numpy()
+        hn[:head_end] = raw[:head_end]
+        hn[head_end:] = raw[a:e]
+        csv_pool.append(h if k % 3 == 0 else h.cuda())
     reqs = []
     for _ in range(n_req):
         q = SERVE_QUERIES[rng.randrange(len(SERVE_QUERIES))]
-        if rng.random() < 0.2:
-            t = csv_inputs[rng.randrange(len(csv_inputs))]
-            reqs.append((q, t, "csv"))
-        else:
-            i = rng.randrange(len(offs))
-            reqs.append((q, dev[offs[i]:offs[i] + lens[i]], "ndjson"))
+        if rng.random() < csv_share:
+            t = csv_pool[rng.randrange(len(csv_pool))]
+            reqs.append((q, t, "csv", int(t.numel())))
+            continue
+        sz = size()
+        a = rng.randrange(0, n - sz - (1 << 20))
+        while True:  # a line start on a 16-byte boundary
+            j = bytes(hnp[a:a + 8192]).find(b"\n")
+            a += j + 1
+            if a % 16 == 0:
+                break
+        e = a + sz
+        e += bytes(hnp[e - 1:e + 8192]).find(b"\n")
+        src = hnp[a:e] if rng.random() < host_share else dsrc[a:e]
+        reqs.append((q, src, "ndjson", e - a))
+    return reqs, csv_pool
+
+
+def measure_serving(wjq, reqs, rate, n_slots=3, max_batch=0, seed=5):
+    """Open-loop Poisson arrivals at `rate` req/s through the native serving
+    loop (include/warpjq_serve.h): continuous batching over `n_slots` slots
+    with a 120 GB device-memory budget (with n_slots=1, max_batch=1: one
+    request at a time).  Latency = completion - arrival, wall clock; every
+    output rendered on the host."""
+    import random
+    import torch
+    from warpjq_b200.serve import NativeServer
+    rng = random.Random(seed)
+    n_req = len(reqs)
     gaps = [rng.expovariate(rate) for _ in range(n_req)]
-    total = sum(int(t.numel()) for _, t, _ in reqs)
+    total = sum(r[3] for r in reqs)
+    srv = NativeServer(SERVE_QUERIES, n_slots=n_slots, budget_bytes=120 << 30, max_batch=max_batch)
+    srv.warm(256 << 20)
+    for q, x, f, _ in reqs[:32]:  # warm: every path once
+        srv.submit(q, x, f)
+    srv.drain()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter() + 0.01
+    arrive, t = [], t0
+    for g in gaps:
+        t += g
+        arrive.append(t)
+    nxt, done = 0, []
+    while nxt < n_req:
+        now = time.perf_counter()
+        while nxt < n_req and arrive[nxt] <= now:
+            q, x, f, _ = reqs[nxt]
+            srv.submit(q, x, f)
+            nxt += 1
+        done += srv.poll()
+        if nxt < n_req:
+            time.sleep(max(0.0, min(arrive[nxt] - time.perf_counter(), 0.0005)))
+    done += srv.drain()
+    span = time.perf_counter() - t0
+    srv.close()
+    bad = [r for r in done if r.rc]
+    assert not bad, bad[0].error
+    lat = sorted(r.latency_ms for r in done)
+    pick = lambda f: round(lat[min(n_req - 1, int(f * n_req))], 3)
+    return {"p50_ms": pick(0.50), "p99_ms": pick(0.99), "p999_ms": pick(0.999),
+            "sustained_gbs": round(total / span / 1e9, 3), "span_s": round(span, 3)}
 
-    def run(slots, max_batch):
-        srv = Server(SERVE_QUERIES, n_slots=slots, budget_bytes=120 << 30, max_batch=max_batch)
-        srv.warm(256 << 20)
-        for q, t, f in reqs[:64]:  # warm: the CSV path and the render path
-            srv.submit(q, t, f)
-        srv.drain()
-        srv.done.clear()
-        torch.cuda.synchronize()
-        # the earlier legs leave a large heap: keep the collector's full
-        # passes over it out of the timed loop
-        import gc
-        gc.collect()
-        gc.freeze()
-        t0 = time.perf_counter() + 0.01
-        arrive, t = [], t0
-        for g in gaps:
-            t += g
-            arrive.append(t)
-        nxt, hs = 0, []
-        while nxt < n_req or srv.pending():
-            now = time.perf_counter()
-            while nxt < n_req and arrive[nxt] <= now:
-                q, x, f = reqs[nxt]
-                hs.append(srv.submit(q, x, f, t_arrive=arrive[nxt]))
-                nxt += 1
-            srv.poll()
-        span = time.perf_counter() - t0
-        gc.unfreeze()
-        srv.close()
-        assert all(not h.error for h in hs)
-        lat = sorted(h.latency for h in hs)
-        pick = lambda f: round(lat[min(n_req - 1, int(f * n_req))] * 1e3, 3)
-        return {"p50_ms": pick(0.50), "p99_ms": pick(0.99), "p999_ms": pick(0.999),
-                "sustained_gbs": round(total / span / 1e9, 3)}
 
-    return {"offered_req_per_s": rate, "requests": n_req, "queries": len(SERVE_QUERIES), "csv_share": 0.2,
-            "residency": "device",
-            "sizes": "log-uniform 4 KiB - 4 MiB (rescaled from 1 KB - 256 MB)",
-            "offered_gbs": round(total / sum(gaps) / 1e9, 3),
-            "batched": run(3, 0), "one_at_a_time": run(1, 1)}
+def measure_serving_baselines(reqs, k=8):
+    """The comparators of the serving configuration on the first k requests,
+    run back to back: the plain one-process-per-query GPU path (a fresh
+    process per request: interpreter, library load, CUDA context and query
+    set-up, then warpjq_run_bytes over the request's bytes from a file in
+    /dev/shm), and the CPU backend (the oracle, all host threads)."""
+    import tempfile
+    import numpy as np
+    from oracle import pyoracle as orc
+    from oracle import csv_map
+    sample = reqs[:k]
+    total = sum(r[3] for r in sample)
+    datas = []
+    for q, x, f, _ in sample:
+        b = bytes(x.cpu().numpy()) if hasattr(x, "is_cuda") else bytes(np.asarray(x))
+        datas.append(b)
+    lat_p = []
+    t0 = time.perf_counter()
+    for (q, _, f, _), b in zip(sample, datas):
+        with tempfile.NamedTemporaryFile(dir="/dev/shm" if os.path.isdir("/dev/shm") else None,
+                                         delete=False) as tf:
+            tf.write(b)
+            path = tf.name
+        code = ("import sys; sys.path.insert(0, %r); import warpjq_b200 as w; "
+                "d = open(%r, 'rb').read(); " % (ROOT, path) +
+                ("r = w.Query(%r).run_csv(d)" % q if f == "csv" else "r = w.run_bytes(%r, d)" % q) +
+                "; sys.exit(r.rc)")
+        a = time.perf_counter()
+        rc = subprocess.run([sys.executable, "-c", code]).returncode
+        lat_p.append((time.perf_counter() - a) * 1e3)
+        os.unlink(path)
+        assert rc == 0
+    span_p = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    lat_c = []
+    for (q, _, f, _), b in zip(sample, datas):
+        a = time.perf_counter()
+        r = orc.run(q, csv_map.csv_to_ndjson(b) if f == "csv" else b)
+        lat_c.append((time.perf_counter() - a) * 1e3)
+        assert r.rc == 0
+    span_c = time.perf_counter() - t0
+    return {"requests": k, "bytes": total,
+            "process_per_query": {"gbs": round(total / span_p / 1e9, 3),
+                                  "mean_ms": round(sum(lat_p) / k, 1)},
+            "cpu_backend": {"gbs": round(total / span_c / 1e9, 3), "mean_ms": round(sum(lat_c) / k, 1),
+                            "cores": os.cpu_count(),
+                            "note": "CSV requests are mapped to NDJSON on the host first (timed)"}}
 
 
 NESTED_QUERIES = [
@@ -775,15 +824,28 @@ def main():
 
     batch = serve = nested = e2e_file = csv_leg = None
     if rank == 0 and world == 1 and not args.no_batch:
-        bdev, boffs, blens, bq = batch_workload(hnp, n)
+        bdev, boffs, blens, bq = batch_workload(dev, hnp, n)
         batch = measure_batch(wjq, bdev, boffs, blens, bq)
-        # the configuration's top rate, and ten times it (the rescaled inputs
-        # are ~35x smaller than the configuration's, so its offered bytes
-        # per second need the higher rate)
-        csv_in = serve_csv_inputs(wjq)
-        serve = [measure_serving(wjq, bdev, boffs, blens, csv_in, rate=r) for r in (2000.0, 20000.0)]
-        del csv_in
         del bdev
+        torch.cuda.empty_cache()
+        # the serving configuration: 1 KB - 256 MB requests, 20% CSV, some
+        # from host memory, at three arrival rates; the one-at-a-time server
+        # and the per-process / CPU comparators beside it
+        sreqs, keep = serve_pool(wjq, dev, hnp, n, 2000)
+        serve = {"queries": len(SERVE_QUERIES), "csv_share": 0.2, "host_share_of_ndjson": 0.3,
+                 "sizes": "log-uniform 1 KB - 256 MB", "budget_bytes": 120 << 30, "rates": []}
+        for rate, k in ((50.0, 100), (500.0, 1000), (2000.0, 2000)):
+            sub = sreqs[:k]
+            span = k / rate
+            entry = {"offered_req_per_s": rate, "requests": k,
+                     "offered_gbs": round(sum(r[3] for r in sub) / span / 1e9, 3),
+                     "batched": measure_serving(wjq, sub, rate)}
+            if rate <= 500.0:
+                entry["one_at_a_time"] = measure_serving(wjq, sub, rate, n_slots=1, max_batch=1)
+            serve["rates"].append(entry)
+        serve["baselines"] = measure_serving_baselines(sreqs)
+        del sreqs, keep
+        torch.cuda.empty_cache()
         nested = measure_nested(wjq)
         csv_leg = measure_csv(wjq)
         e2e_file = measure_file(wjq, hnp, n)

@@ -64,9 +64,11 @@ typedef struct {
 int warpjq_serve_open(const char *const *queries, uint32_t n_queries, const warpjq_serve_config *cfg,
                       warpjq_server **out, char *err, size_t err_len);
 
-/* Runs every slot's every query once over `reserve_bytes` of blank lines and
- * converts a small CSV input, so buffers reach their working sizes and every
- * kernel is loaded before requests arrive.  Call before the first request. */
+/* Runs every slot's every query once over `reserve_bytes` of blank lines,
+ * converts a CSV input of a quarter of that size and reserves each slot's
+ * input arena and row buffers for inputs that large, so buffers reach their
+ * working sizes and every kernel is loaded before requests arrive.  Call
+ * before the first request. */
 int warpjq_serve_warm(warpjq_server *s, uint64_t reserve_bytes, char *err, size_t err_len);
 
 /* Queues one request: query `query` over `len` bytes at `data` (host memory

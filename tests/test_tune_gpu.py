@@ -1,5 +1,6 @@
-"""The autotuner on the device: it measures the tile sweep (and, for
-group_by, the table capacity), never picks something slower than the
+"""The autotuner on the device: it measures the lines-per-warp sweep (tiles
+of that many mean lines; and, for group_by, the table capacity), never
+picks something slower than the
 analytic choice on its sample, reuses its cache, and a context set from the
 choice still prints the oracle's bytes."""
 
@@ -24,6 +25,7 @@ def test_tune_sweeps_caches_and_keeps_results_exact(tmp_path):
         assert not c["from_cache"]
         assert c["gbs"] >= c["autotile_gbs"]
         assert len(c["swept"]) >= 5
+        assert c["lines_per_warp"] > 0 and abs(c["lines_per_warp"] * 210.5 - c["tile"]) < 0.25 * c["tile"]
         again = tune.tune(q, dev.data_ptr(), n, sample, cache_path=path)
         assert again["from_cache"] and again["tile"] == c["tile"]
         Q = wjq.Query(q)

@@ -161,6 +161,11 @@ struct Slot {
   size_t h_groups_cap = 0;
   bool launched = false;
   uint32_t kernels = 0;
+  // page-locked staging of a batch's tables (copied from here without a
+  // host wait for the stream), and the event after its last copies
+  uint8_t *h_btab = nullptr;
+  size_t h_btab_cap = 0;
+  cudaEvent_t btab_done = nullptr;
   cudaEvent_t scan_t0 = nullptr, scan_t1 = nullptr;  // around the scan kernel
   bool timed = false;  // the last run recorded scan_t0/scan_t1 (not a graph replay)
   unsigned long long last_first_invalid = ~0ull;
@@ -346,28 +351,46 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     CK(rb.b_in_tile0.ensure(n_inputs + 1, st, capturing), "alloc batch tables");
     CK(rb.b_in_ctr.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch tables");
     CK(rb.b_tile_input.ensure(std::max<unsigned long long>(n_tiles, 1), st, capturing), "alloc batch tables");
+    // The tables are packed into page-locked staging and copied from there:
+    // a copy from pageable memory would make the host wait for the stream's
+    // earlier work (the previous batches of a serving slot).
+    const size_t n8 = n_inputs * 8ull, t8 = (n_inputs + 1) * 8ull, tt = n_tiles * 4ull;
+    const size_t p_in = n_inputs * 4ull, p_pl = b->mixed ? b->plans.size() * sizeof(DevPlan) : 0;
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t o_end = up16(n8), o_t0 = o_end + up16(n8), o_ti = o_t0 + up16(t8), o_ip = o_ti + up16(tt),
+                 o_pl = o_ip + up16(p_in), need = o_pl + p_pl;
+    if (!s.btab_done) CK(cudaEventCreateWithFlags(&s.btab_done, cudaEventDisableTiming), "event");
+    CK(cudaEventSynchronize(s.btab_done), "batch staging wait");  // the last batch's copies are done
+    if (need > s.h_btab_cap) {
+      if (s.h_btab) cudaFreeHost(s.h_btab);
+      s.h_btab = nullptr;
+      s.h_btab_cap = 0;
+      const size_t cap = std::max<size_t>(need + need / 2, 1u << 16);
+      CK(cudaMallocHost((void **)&s.h_btab, cap), "alloc batch staging");
+      s.h_btab_cap = cap;
+    }
+    uint8_t *hb = s.h_btab;
+    if (n8) {
+      std::memcpy(hb, b->start.data(), n8);
+      std::memcpy(hb + o_end, b->end.data(), n8);
+    }
+    std::memcpy(hb + o_t0, b->tile0.data(), t8);
+    if (tt) std::memcpy(hb + o_ti, b->tile_input.data(), tt);
     if (b->mixed) {
       CK(rb.b_plans.ensure(b->plans.size(), st, capturing), "alloc batch plans");
       CK(rb.b_in_plan.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch plans");
-      CK(cudaMemcpyAsync(rb.b_plans.p, b->plans.data(), b->plans.size() * sizeof(DevPlan), cudaMemcpyHostToDevice,
-                         st),
-         "H2D batch plans");
-      if (n_inputs)
-        CK(cudaMemcpyAsync(rb.b_in_plan.p, b->in_plan.data(), n_inputs * 4ull, cudaMemcpyHostToDevice, st),
-           "H2D batch plans");
+      if (p_in) std::memcpy(hb + o_ip, b->in_plan.data(), p_in);
+      std::memcpy(hb + o_pl, b->plans.data(), p_pl);
+      CK(cudaMemcpyAsync(rb.b_plans.p, hb + o_pl, p_pl, cudaMemcpyHostToDevice, st), "H2D batch plans");
+      if (p_in) CK(cudaMemcpyAsync(rb.b_in_plan.p, hb + o_ip, p_in, cudaMemcpyHostToDevice, st), "H2D batch plans");
     }
-    // pageable sources: staged by the driver before the calls return
-    CK(cudaMemcpyAsync(rb.b_in_start.p, b->start.data(), n_inputs * 8ull, cudaMemcpyHostToDevice, st),
-       "H2D batch tables");
-    CK(cudaMemcpyAsync(rb.b_in_end.p, b->end.data(), n_inputs * 8ull, cudaMemcpyHostToDevice, st),
-       "H2D batch tables");
-    CK(cudaMemcpyAsync(rb.b_in_tile0.p, b->tile0.data(), (n_inputs + 1) * 8ull,
-                       cudaMemcpyHostToDevice, st),
-       "H2D batch tables");
-    if (n_tiles)
-      CK(cudaMemcpyAsync(rb.b_tile_input.p, b->tile_input.data(), n_tiles * 4ull,
-                         cudaMemcpyHostToDevice, st),
-         "H2D batch tables");
+    if (n8) {
+      CK(cudaMemcpyAsync(rb.b_in_start.p, hb, n8, cudaMemcpyHostToDevice, st), "H2D batch tables");
+      CK(cudaMemcpyAsync(rb.b_in_end.p, hb + o_end, n8, cudaMemcpyHostToDevice, st), "H2D batch tables");
+    }
+    CK(cudaMemcpyAsync(rb.b_in_tile0.p, hb + o_t0, t8, cudaMemcpyHostToDevice, st), "H2D batch tables");
+    if (tt) CK(cudaMemcpyAsync(rb.b_tile_input.p, hb + o_ti, tt, cudaMemcpyHostToDevice, st), "H2D batch tables");
+    CK(cudaEventRecord(s.btab_done, st), "event record");
   }
   if (b && n_inputs) k_batch_reset<<<(n_inputs + 255) / 256, 256, 0, st>>>(rb.b_in_ctr.p, n_inputs);
   GroupTable g = group_view(rb, groups);
@@ -683,6 +706,8 @@ static void free_slot(Slot &s) {
   if (s.h_groups) cudaFreeHost(s.h_groups);
   if (s.scan_t0) cudaEventDestroy(s.scan_t0);
   if (s.scan_t1) cudaEventDestroy(s.scan_t1);
+  if (s.h_btab) cudaFreeHost(s.h_btab);
+  if (s.btab_done) cudaEventDestroy(s.btab_done);
   s = Slot();
 }
 

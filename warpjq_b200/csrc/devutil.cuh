@@ -83,12 +83,18 @@ __host__ __device__ __forceinline__ uint32_t flags_newline(uint32_t x) {
   return ~(sn | x) & 0x80808080u;
 }
 
-// Moves the four flags of word k (0..7) of a chunk to bits 4k..4k+3.  The
-// multiply by 1 + 2^7 + 2^14 + 2^21 lands byte j's flag (bit 8j + 7) on bit
-// 28 + j; no two partial products share a bit, so nothing carries.
-__host__ __device__ __forceinline__ uint32_t flags_to_bits(uint32_t f, int k) {
-  const uint32_t prod = f * 0x00204081u;
-  return k == 7 ? (prod & 0xF0000000u) : ((prod >> (28 - 4 * k)) & (0xFu << (4 * k)));
+// Shifts the nibbles gathered so far up by four and moves the four flags of
+// `f` (bit 7 of each byte) in below them, byte j's flag on bit j.  The
+// multiply by 1 + 2^7 + 2^14 + 2^21 lands byte j's flag on bit 28 + j (no
+// two partial products share a bit, so nothing carries); one funnel shift
+// brings those four bits in.  Pushing a chunk's words from the last to the
+// first leaves word k's flags on bits 4k..4k+3.
+__host__ __device__ __forceinline__ uint32_t flags_push(uint32_t acc, uint32_t f) {
+#ifdef __CUDA_ARCH__
+  return __funnelshift_l(f * 0x00204081u, acc, 4);
+#else
+  return (acc << 4) | ((f * 0x00204081u) >> 28);
+#endif
 }
 
 // Classifies one 32-byte chunk given as eight little-endian words: returns
@@ -100,9 +106,9 @@ __host__ __device__ __forceinline__ uint32_t flags_to_bits(uint32_t f, int k) {
 __host__ __device__ __forceinline__ uint32_t classify_chunk(const uint32_t w[8], uint32_t *special) {
   uint32_t s = 0, nl = 0;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    s |= flags_to_bits(flags_special(w[k]), k);
-    nl |= flags_to_bits(flags_newline(w[k]), k);
+  for (int k = 7; k >= 0; k--) {
+    s = flags_push(s, flags_special(w[k]));
+    nl = flags_push(nl, flags_newline(w[k]));
   }
   *special = s;
   return nl;

@@ -516,8 +516,12 @@ int warpjq_serve_warm(warpjq_server *S, uint64_t reserve_bytes, char *err, size_
     return 1;
   }
   cudaMemcpy(d, h.data(), reserve_bytes, cudaMemcpyHostToDevice);
+  // CSV of about a quarter of the reserve: the converter's buffers grow to
+  // what inputs that large need
   std::string rows = "a,b\n";
-  for (int i = 0; i < 4096; i++) rows += "\"x\",1\n";
+  const uint64_t csv_target = std::max<uint64_t>(reserve_bytes / 4, 1u << 16);
+  rows.reserve(csv_target + 16);
+  while (rows.size() < csv_target) rows += "\"x\",1\n";
   uint8_t *dc = nullptr;
   cudaMalloc((void **)&dc, rows.size() + 16);
   cudaMemcpy(dc, rows.data(), rows.size(), cudaMemcpyHostToDevice);
@@ -547,7 +551,11 @@ int warpjq_serve_warm(warpjq_server *S, uint64_t reserve_bytes, char *err, size_
         put_err(err, err_len, std::string("CUDA error: ") + e);
         rc = 1;
       }
-      s.arena.reserve(4ull << 20, 0, s.st);
+      // room for host inputs and converted CSV of the reserve's size, and
+      // page-locked room for a quarter of it in rows
+      s.arena.reserve(reserve_bytes + reserve_bytes / 2, 0, s.st);
+      s.rows.reserve(reserve_bytes / 4);
+      s.row_off.reserve(reserve_bytes / 32);
       cudaStreamSynchronize(s.st);
     }
   }

@@ -3,14 +3,15 @@ on a sample of its input, and caches the choice.
 
 Swept, each timed with CUDA events around the device-resident run (best of
 `reps` after a warm-up):
-  - tile bytes (the bytes one warp stages and walks per tile; with one line
-    per lane, the tile sets how many 32-line rounds a warp runs per tile),
-    with the halo from warpjq_autotile's longest-line rule;
+  - lines per warp: how many lines a warp takes from the work queue at a
+    time (walked 32 at a time, one per lane).  The unit of work is a tile of
+    bytes, so a lines-per-warp candidate L is the tile L x the sample's mean
+    line length (rounded to 256 bytes, within the tiling limits); the tile
+    bytes follow from it, with the halo from warpjq_autotile's longest-line
+    rule, and warpjq_autotile's own tile is a candidate too;
   - for group_by queries, the group table's starting capacity (a table
     sized for the input's cardinality avoids an overflow rerun; a small one
     is cleared and cached faster).
-Lines per round are fixed at 32 by the design (one line per lane), so they
-are not swept.
 
 The cache is a JSON file keyed by device name, the device library's build,
 query and the sample's mean line length (rounded to a power of two), so
@@ -28,7 +29,7 @@ import os
 
 from . import Query, device_name
 
-TILES = (2048, 3072, 4096, 5120, 6144, 6400, 7168, 8192, 10240, 12288, 16384)
+LINES_PER_WARP = (8, 16, 24, 32, 48, 64, 96, 128, 192, 256)
 GROUP_KEYS = (1 << 12, 1 << 14, 1 << 16, 1 << 18, 1 << 20)
 
 
@@ -100,7 +101,14 @@ def tune(query: str, d_ptr: int, n: int, sample: bytes, reps: int = 3, cache_pat
         return dict(cache[key], from_cache=True)
     Q = Query(query)
     t0, h = Q.autotile(sample[: 1 << 20])
-    tiles = sorted(set(t for t in TILES if t + h <= 65535 - 64) | {t0})
+    head = sample[: 1 << 20]
+    mean = len(head) / max(1, head.count(b"\n"))
+    per = {}
+    for L in LINES_PER_WARP:
+        t = max(1024, int(L * mean) // 256 * 256)
+        if t + h <= 65535 - 64:
+            per.setdefault(t, L)
+    tiles = sorted(set(per) | {t0})
     timings = {}
     for t in tiles:
         Q.set_tiling(t, h)
@@ -115,7 +123,8 @@ def tune(query: str, d_ptr: int, n: int, sample: bytes, reps: int = 3, cache_pat
             if ms < best_ms:
                 best_keys, best_ms = k, ms
     Q.close()
-    res = {"tile": best_t, "halo": h, "group_keys": best_keys, "gbs": round(n / (best_ms / 1e3) / 1e9, 2),
+    res = {"lines_per_warp": round(best_t / mean, 1), "tile": best_t, "halo": h, "group_keys": best_keys,
+           "gbs": round(n / (best_ms / 1e3) / 1e9, 2),
            "autotile": t0, "autotile_gbs": round(n / (timings[t0] / 1e3) / 1e9, 2),
            "swept": {str(t): round(n / (ms / 1e3) / 1e9, 2) for t, ms in timings.items()}}
     if use_cache:
