@@ -309,6 +309,9 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
     for (auto &r : take) failed.push_back(fail_result(r, "out of device memory for the request's input"));
     take.clear();
   }
+  // CSV requests first: their conversion waits on the host for its own
+  // counts, which should not also wait behind this slot's input copies
+  std::stable_partition(take.begin(), take.end(), [](const Req &r) { return (r.flags & WARPJQ_SERVE_CSV) != 0; });
   uint64_t pos = 0;
   for (auto &r : take) {
     const bool dev = r.flags & WARPJQ_SERVE_DEVICE;

@@ -152,29 +152,13 @@ struct GroupKeyDesc {
 };
 static_assert(sizeof(GroupKeyDesc) == 24, "group key descriptor");
 
-// A CTA's recently seen group keys (direct-mapped by hash): a key of at most
-// kKeyCacheBytes bytes without escapes is found here, by its hash and its
-// bytes, without probing the global table.
-constexpr int kKeyCache = 32;
-constexpr uint32_t kKeyCacheBytes = 24;
-struct KeyCacheEntry {
-  uint32_t hash;  // 0: empty (a key's hash is never 0)
-  uint32_t kid;
-  uint32_t input;
-  uint8_t len, kind, pad[2];
-  uint8_t bytes[kKeyCacheBytes];
-};
-static_assert(sizeof(KeyCacheEntry) == 40, "key cache entry");
-
 // A CTA's private accumulators for up to kGroupCache keys (direct-mapped by
 // key id), merged into the global records when the CTA finishes.  Hot keys
 // then cost shared-memory atomics instead of contended global ones.
 struct GroupCache {
   uint32_t tag[kGroupCache];  // key id held by the entry, or 0xFFFFFFFF
   GroupAcc acc[kGroupCache];
-  KeyCacheEntry keys[kKeyCache];
 };
-
 
 __host__ __device__ inline size_t scan_smem_bytes(uint32_t T, uint32_t H, bool groups) {
   return scan_smem_base(T, H) + (groups ? sizeof(GroupCache) : 0);
@@ -325,16 +309,6 @@ __device__ uint32_t group_find_or_insert(const ScanParams &sp, const KeyRef &k, 
   }
   atomicOr(&sp.ctr->overflow, 4u);
   return 0xFFFFFFFFu;
-}
-
-// The key id of `k` (hash h) from the CTA's key cache, or 0xFFFFFFFF.
-__device__ __forceinline__ uint32_t key_cache_find(const GroupCache *gc, const KeyRef &k, uint32_t h) {
-  if (k.esc || k.len > kKeyCacheBytes) return 0xFFFFFFFFu;
-  const KeyCacheEntry &e = gc->keys[h & (kKeyCache - 1)];
-  if (e.hash != h || e.len != k.len || e.kind != k.kind || e.input != k.input) return 0xFFFFFFFFu;
-  for (uint32_t t = 0; t < k.len; t++)
-    if (e.bytes[t] != k.p[t]) return 0xFFFFFFFFu;
-  return e.kid;
 }
 
 // ---------------------------------------------------------------------------
@@ -733,7 +707,6 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
       gcache->tag[k] = 0xFFFFFFFFu;
       group_acc_init(gcache->acc[k]);
     }
-    for (int k = lane; k < kKeyCache; k += 32) gcache->keys[k].hash = 0;
   }
   const uint32_t bar = (uint32_t)__cvta_generic_to_shared(s_bar);
   if (lane == 0) mbar_init(bar);
@@ -1070,29 +1043,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
           const bool same = has_group && lane != leader && gk.kind == lkind && input == linput &&
                             key_bytes_equal(gk, (const uint8_t *)lp, llen, (uint8_t)lesc);
           uint32_t kid = 0xFFFFFFFFu;
-          bool fill = false;  // found in the global table: enter it into the key cache
-          if (has_group && !same) {
-            kid = key_cache_find(gcache, gk, gh);
-            if (kid == 0xFFFFFFFFu) {
-              kid = group_find_or_insert(sp, gk, gh);
-              fill = kid != 0xFFFFFFFFu && !gk.esc && gk.len <= kKeyCacheBytes;
-            }
-          }
-          {
-            // one writer per cache entry (lanes whose keys share an entry
-            // would otherwise interleave their fields)
-            const uint32_t ci = fill ? (gh & (kKeyCache - 1)) : 0xFFFFFFFFu;
-            const unsigned same_ci = __match_any_sync(0xffffffffu, ci);
-            if (fill && lane == __ffs(same_ci) - 1) {
-              KeyCacheEntry &e = gcache->keys[ci];
-              e.hash = gh;
-              e.kid = kid;
-              e.input = gk.input;
-              e.len = (uint8_t)gk.len;
-              e.kind = gk.kind;
-              for (uint32_t t = 0; t < gk.len; t++) e.bytes[t] = gk.p[t];
-            }
-          }
+          if (has_group && !same) kid = group_find_or_insert(sp, gk, gh);
           const uint32_t lkid = __shfl_sync(0xffffffffu, kid, leader);
           if (same) kid = lkid;
           // Lanes holding the same key add up their contributions in the
