@@ -615,9 +615,12 @@ __device__ __forceinline__ uint32_t pop_special(const uint32_t *sm, uint32_t &k,
 // to special byte: a key is its two quotes, a string value its quotes and
 // escapes, and only the bytes right after them are read ('"' ':' value, ','
 // or '}').  Lines of that shape get exactly walk_masked's verdict and node
-// values; for any other line (whitespace, arrays, escaped keys, deeper
-// nesting, anything malformed) it returns LS_FALLBACK and records nothing
-// that walk_masked does not overwrite.  Same window contract as walk_masked.
+// values; a line it finds malformed where every check so far has passed (a
+// raw control byte or the line's end inside a string, a value that is no
+// number or literal) is LS_INVALID without the general walk; for any other
+// line (whitespace, arrays, escaped keys, deeper nesting, anything else
+// malformed) it returns LS_FALLBACK and records nothing that walk_masked
+// does not overwrite.  Same window contract as walk_masked.
 //
 // Checks whose outcome does not steer the walk (that a key's quotes are
 // quotes where they were expected, the ':' after it, an escape's letter)
@@ -684,7 +687,9 @@ __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, 
         r = pop_special(sm, k, m);
         const uint32_t b = w[r];
         if (b == '"') break;
-        if (b != '\\') return LS_FALLBACK;  // a control byte or the newline
+        // a raw control byte or the newline inside a string: with every
+        // earlier check passed, the line is malformed whatever its shape
+        if (b != '\\') return bad ? LS_FALLBACK : LS_INVALID;
         esc = true;
         const uint32_t x = w[r + 1];
         if (x == '"' || x == '\\') {
@@ -700,7 +705,10 @@ __device__ __forceinline__ int walk_objects(const DevPlan &P, const uint8_t *w, 
     } else {
       if (c == '[') return LS_FALLBACK;
       ve = win_atom(w, vs, c);
-      if (!ve) return LS_FALLBACK;
+      // no number or literal at the value's place (a bare word, a bad
+      // number, a cut literal): malformed, unless an earlier check failed
+      // or the value is only preceded by whitespace
+      if (!ve) return (bad || c == ' ' || c == '\t' || c == '\r') ? LS_FALLBACK : LS_INVALID;
     }
     if (vn != kNoNode) v.len[vn] = ve - vs;
     // after a value: ',' and the next key, or '}' closing one or more objects
