@@ -395,7 +395,7 @@ def measure_serving(wjq, reqs, rate, n_slots=4, max_batch=0, seed=5):
     # one batch per query in a slot (mixed batches carry every path and run
     # slower than the specialised kernels here)
     srv = NativeServer(SERVE_QUERIES, n_slots=n_slots, budget_bytes=120 << 30, max_batch=max_batch, mixed_min=0)
-    srv.warm(256 << 20)
+    srv.warm(1 << 30)
     for q, x, f, _ in reqs[:32]:  # warm: every path once
         srv.submit(q, x, f)
     srv.drain()

@@ -40,6 +40,8 @@ typedef struct {
                           * (one launch sequence, each input with its own plan) from this
                           * many on (0: never) */
   uint64_t chunk_bytes;  /* the contexts' chunk size (0: 1 MiB; only sizes host-run buffers) */
+  uint64_t slot_bytes;   /* input bytes one slot takes at a time (0: 1 GiB; a larger request
+                          * goes alone), so waiting work spreads over the slots */
 } warpjq_serve_config;
 
 /* Request flags. */

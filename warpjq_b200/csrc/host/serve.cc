@@ -432,10 +432,13 @@ void loop_main(warpjq_server *S) {
       {
         std::lock_guard<std::mutex> lk(S->mu);
         uint64_t total = 0;
+        uint64_t bytes = 0;
         while (!S->waiting.empty()) {
           const Req &r = S->waiting.front();
           if (S->in_flight_bytes + total + r.fp > S->cfg.budget_bytes) break;
           if (S->cfg.max_batch && take.size() >= S->cfg.max_batch) break;
+          if (!take.empty() && bytes + r.len > S->cfg.slot_bytes) break;
+          bytes += r.len;
           total += r.fp;
           take.push_back(r);
           S->waiting.pop_front();
@@ -478,6 +481,7 @@ int warpjq_serve_open(const char *const *queries, uint32_t n_queries, const warp
   if (!S->cfg.n_slots) S->cfg.n_slots = 3;
   if (!S->cfg.budget_bytes) S->cfg.budget_bytes = 120ull << 30;
   if (!S->cfg.chunk_bytes) S->cfg.chunk_bytes = 1ull << 20;
+  if (!S->cfg.slot_bytes) S->cfg.slot_bytes = 1ull << 30;
   cudaGetDevice(&S->device);
   for (uint32_t i = 0; i < n_queries; i++) S->queries.push_back(queries[i]);
   S->slots.resize(S->cfg.n_slots);

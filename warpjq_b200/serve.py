@@ -361,7 +361,8 @@ import ctypes as _ct
 
 class _ServeConfig(_ct.Structure):
     _fields_ = [("n_slots", _ct.c_uint32), ("max_batch", _ct.c_uint32), ("budget_bytes", _ct.c_uint64),
-                ("format", _ct.c_uint32), ("mixed_min", _ct.c_uint32), ("chunk_bytes", _ct.c_uint64)]
+                ("format", _ct.c_uint32), ("mixed_min", _ct.c_uint32), ("chunk_bytes", _ct.c_uint64),
+                ("slot_bytes", _ct.c_uint64)]
 
 
 class _ServeResult(_ct.Structure):
@@ -394,7 +395,8 @@ class NativeServer:
     poll() returns finished requests; drain() waits for all of them."""
 
     def __init__(self, queries, n_slots: int = 3, budget_bytes: int = 120 << 30, fmt_out: str = "ndjson",
-                 max_batch: int = 0, mixed_min: int = MIXED_MIN, chunk_bytes: int = 1 << 20):
+                 max_batch: int = 0, mixed_min: int = MIXED_MIN, chunk_bytes: int = 1 << 20,
+                 slot_bytes: int = 1 << 30):
         from . import FORMATS, _load
         _, h = _load()
         self._h = h
@@ -415,7 +417,7 @@ class NativeServer:
         self.queries = list(dict.fromkeys(queries))
         self._index = {q: i for i, q in enumerate(self.queries)}
         arr = (cp * len(self.queries))(*[q.encode() for q in self.queries])
-        cfg = _ServeConfig(n_slots, max_batch, budget_bytes, FORMATS[fmt_out], mixed_min, chunk_bytes)
+        cfg = _ServeConfig(n_slots, max_batch, budget_bytes, FORMATS[fmt_out], mixed_min, chunk_bytes, slot_bytes)
         self._s = vp()
         err = _ct.create_string_buffer(1024)
         rc = h.warpjq_serve_open(arr, len(self.queries), _ct.byref(cfg), _ct.byref(self._s), err, len(err))
