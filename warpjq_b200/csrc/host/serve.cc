@@ -4,9 +4,10 @@
 // (crates/warpjq-cli/src/run.rs:16-96) and pays the device context's set-up
 // each time.  Here a server owns, per slot, a CUDA stream, one query (and so
 // one device context and compiled plan) per served query, a driver context
-// for mixed batches, a CSV converter, a device arena for inputs that are not
-// usable in place, and page-locked buffers for row output; all of it lives
-// as long as the server.  One loop thread does everything that touches the
+// for mixed batches, a device arena for inputs that are not usable in place,
+// and page-locked buffers for row output; all of it lives as long as the
+// server.  CSV requests are converted to NDJSON on the device by a thread of
+// their own before they join the queue.  One loop thread does everything that touches the
 // device: it completes slots whose event has fired, then gives each free
 // slot the longest prefix of the waiting requests that fits the memory
 // budget beside what is in flight, so requests that arrive while others run
@@ -59,6 +60,7 @@ struct Req {
   Clock::time_point t_arrive, t_admit;
   uint64_t addr = 0;  // device address of the request's NDJSON in the slot
   uint64_t nd = 0;    // its length
+  uint8_t *owned = nullptr;  // CSV converted ahead of admission: its NDJSON (freed at completion)
 };
 
 // A device buffer that grows stream-ordered (the slot's stream), keeping
@@ -134,6 +136,15 @@ struct warpjq_server {
   uint64_t next_id = 1;
   bool stop = false;
   std::thread loop;
+  // CSV requests are converted by a thread of their own, on its own stream,
+  // before they join the waiting queue, so the loop never waits on the
+  // converter's host synchronisations
+  std::deque<Req> to_convert;
+  uint64_t converting = 0;  // taken by the converter, not yet queued
+  std::condition_variable cv_conv;
+  warpjq_csv *conv = nullptr;
+  cudaStream_t conv_st = nullptr;
+  std::thread converter;
 };
 
 namespace {
@@ -278,6 +289,8 @@ void complete_slot(warpjq_server *S, Slot &s) {
   for (size_t qi = 0; qi < s.by_q.size(); qi++)
     if (!s.by_q[qi].empty()) complete_batch(S, s, warpjq_query_ctx(s.qs[qi]), s.qs[qi], s.by_q[qi], false, out);
   S->in_flight_bytes -= s.fp;
+  for (auto &r : s.reqs)
+    if (r.owned) cudaFreeAsync(r.owned, s.st);  // after every use on this stream
   {
     std::lock_guard<std::mutex> lk(S->mu);
     for (auto &x : out) S->done.push_back(x);
@@ -302,40 +315,18 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
   for (auto &r : take) {
     r.t_admit = now;
     const bool dev = r.flags & WARPJQ_SERVE_DEVICE;
-    if (r.flags & WARPJQ_SERVE_CSV) room += 2 * r.len + 32;
-    else if (!dev || (uintptr_t)r.data % 16) room += r.len + 16;
+    if (!r.owned && (!dev || (uintptr_t)r.data % 16)) room += r.len + 16;
   }
   if (!s.arena.reserve(room, 0, s.st)) {
     for (auto &r : take) failed.push_back(fail_result(r, "out of device memory for the request's input"));
     take.clear();
   }
-  // CSV requests first: their conversion waits on the host for its own
-  // counts, which should not also wait behind this slot's input copies
-  std::stable_partition(take.begin(), take.end(), [](const Req &r) { return (r.flags & WARPJQ_SERVE_CSV) != 0; });
   uint64_t pos = 0;
   for (auto &r : take) {
     const bool dev = r.flags & WARPJQ_SERVE_DEVICE;
     std::string why;
-    if (r.flags & WARPJQ_SERVE_CSV) {
-      const uint8_t *d = nullptr;
-      uint64_t nd = 0, consumed = 0, recs = 0;
-      char e[512] = {0};
-      warpjq_csv_reset(s.conv);
-      const uint32_t fl = WARPJQ_CSV_FINAL | (dev ? 0u : WARPJQ_CSV_HOST_INPUT);
-      if (warpjq_csv_convert(s.conv, r.data, r.len, fl, s.st, &d, &nd, &consumed, &recs, e, sizeof e) !=
-          WARPJQ_OK) {
-        why = std::string("CSV conversion failed: ") + e;
-      } else {
-        pos = (pos + 15) & ~15ull;
-        if (!s.arena.reserve(pos + nd + 16, pos, s.st)) {
-          why = "out of device memory for the converted CSV";
-        } else {
-          if (nd) cudaMemcpyAsync(s.arena.p + pos, d, nd, cudaMemcpyDeviceToDevice, s.st);
-          r.addr = (uint64_t)(uintptr_t)(s.arena.p + pos);
-          r.nd = nd;
-          pos += nd;
-        }
-      }
+    if (r.owned) {
+      // CSV, converted by the converter thread: addr and nd are set
     } else if (dev && (uintptr_t)r.data % 16 == 0) {
       r.addr = (uint64_t)(uintptr_t)r.data;
       r.nd = r.len;
@@ -349,8 +340,12 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
       r.nd = r.len;
       pos += r.len;
     }
-    if (!why.empty()) failed.push_back(fail_result(r, why));
-    else s.reqs.push_back(r);
+    if (!why.empty()) {
+      failed.push_back(fail_result(r, why));
+      if (r.owned) cudaFreeAsync(r.owned, s.st);
+    } else {
+      s.reqs.push_back(r);
+    }
   }
   // batches: a slot's requests of several queries as one mixed batch (each
   // input with its own plan) from mixed_min requests on, else one batch per query
@@ -409,12 +404,63 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
     for (size_t i : v) s.fp += s.reqs[i].fp;
   S->in_flight_bytes += s.fp;
   s.busy = launched > 0;
+  if (!s.busy)
+    for (auto &r : s.reqs)
+      if (r.owned) cudaFreeAsync(r.owned, s.st);
   {
     std::lock_guard<std::mutex> lk(S->mu);
     for (auto &x : failed) S->done.push_back(x);
     S->on_device -= take.size() - launched;
   }
   if (!failed.empty()) S->cv_done.notify_all();
+}
+
+// The converter thread: CSV requests in arrival order, each converted on the
+// device into a buffer of its own and then queued for admission as NDJSON
+// (a request that fails to convert completes with its error).
+void converter_main(warpjq_server *S) {
+  cudaSetDevice(S->device);
+  for (;;) {
+    Req r;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_conv.wait(lk, [&] { return S->stop || !S->to_convert.empty(); });
+      if (S->stop) break;
+      r = S->to_convert.front();
+      S->to_convert.pop_front();
+      S->converting++;
+    }
+    std::string why;
+    const uint8_t *d = nullptr;
+    uint64_t nd = 0, consumed = 0, recs = 0;
+    char e[512] = {0};
+    warpjq_csv_reset(S->conv);
+    const uint32_t fl = WARPJQ_CSV_FINAL | ((r.flags & WARPJQ_SERVE_DEVICE) ? 0u : WARPJQ_CSV_HOST_INPUT);
+    if (warpjq_csv_convert(S->conv, r.data, r.len, fl, S->conv_st, &d, &nd, &consumed, &recs, e, sizeof e) !=
+        WARPJQ_OK) {
+      why = std::string("CSV conversion failed: ") + e;
+    } else if (cudaMallocAsync((void **)&r.owned, nd + 16, S->conv_st) != cudaSuccess) {
+      r.owned = nullptr;
+      why = "out of device memory for the converted CSV";
+    } else {
+      if (nd) cudaMemcpyAsync(r.owned, d, nd, cudaMemcpyDeviceToDevice, S->conv_st);
+      if (cudaStreamSynchronize(S->conv_st) != cudaSuccess) why = "CUDA error converting CSV";
+      r.addr = (uint64_t)(uintptr_t)r.owned;
+      r.nd = nd;
+    }
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->converting--;
+      if (why.empty()) {
+        S->waiting.push_back(r);
+      } else {
+        if (r.owned) cudaFreeAsync(r.owned, S->conv_st);
+        S->done.push_back(fail_result(r, why));
+      }
+    }
+    S->cv_loop.notify_one();
+    S->cv_done.notify_all();
+  }
 }
 
 void loop_main(warpjq_server *S) {
@@ -506,7 +552,11 @@ int warpjq_serve_open(const char *const *queries, uint32_t n_queries, const warp
       return fail(1, e);
     if (warpjq_csv_create(&s.conv) != WARPJQ_OK) return fail(1, "CUDA error: creating a CSV converter");
   }
+  if (warpjq_csv_create(&S->conv) != WARPJQ_OK ||
+      cudaStreamCreateWithFlags(&S->conv_st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(1, "CUDA error: creating the CSV converter");
   S->loop = std::thread(loop_main, S);
+  S->converter = std::thread(converter_main, S);
   *out = S;
   return 0;
 }
@@ -549,15 +599,7 @@ int warpjq_serve_warm(warpjq_server *S, uint64_t reserve_bytes, char *err, size_
           rc = 1;
         }
       }
-      const uint8_t *o = nullptr;
-      uint64_t nd, consumed, recs;
-      char e[512] = {0};
-      warpjq_csv_reset(s.conv);
-      if (warpjq_csv_convert(s.conv, dc, rows.size(), WARPJQ_CSV_FINAL, s.st, &o, &nd, &consumed, &recs, e,
-                             sizeof e) != WARPJQ_OK) {
-        put_err(err, err_len, std::string("CUDA error: ") + e);
-        rc = 1;
-      }
+
       // room for host inputs and converted CSV of the reserve's size, and
       // page-locked room for a quarter of it in rows
       s.arena.reserve(reserve_bytes + reserve_bytes / 2, 0, s.st);
@@ -565,6 +607,19 @@ int warpjq_serve_warm(warpjq_server *S, uint64_t reserve_bytes, char *err, size_
       s.row_off.reserve(reserve_bytes / 32);
       cudaStreamSynchronize(s.st);
     }
+  }
+  {
+    // the converter thread's converter (idle: no request has arrived yet)
+    const uint8_t *o = nullptr;
+    uint64_t nd, consumed, recs;
+    char e[512] = {0};
+    warpjq_csv_reset(S->conv);
+    if (warpjq_csv_convert(S->conv, dc, rows.size(), WARPJQ_CSV_FINAL, S->conv_st, &o, &nd, &consumed, &recs, e,
+                           sizeof e) != WARPJQ_OK) {
+      put_err(err, err_len, std::string("CUDA error: ") + e);
+      rc = 1;
+    }
+    cudaStreamSynchronize(S->conv_st);
   }
   cudaFree(d);
   cudaFree(dc);
@@ -599,15 +654,20 @@ int warpjq_serve_enqueue(warpjq_server *S, uint32_t query, const uint8_t *data, 
       S->cv_done.notify_all();
       return 0;
     }
-    S->waiting.push_back(r);
+    if (flags & WARPJQ_SERVE_CSV) S->to_convert.push_back(r);
+    else S->waiting.push_back(r);
   }
-  S->cv_loop.notify_one();
+  if (flags & WARPJQ_SERVE_CSV) S->cv_conv.notify_one();
+  else S->cv_loop.notify_one();
   return 0;
 }
 
 uint32_t warpjq_serve_poll(warpjq_server *S, warpjq_serve_result *done, uint32_t max_done, int timeout_ms) {
   std::unique_lock<std::mutex> lk(S->mu);
-  auto ready = [&] { return !S->done.empty() || (S->waiting.empty() && S->on_device == 0); };
+  auto ready = [&] {
+    return !S->done.empty() ||
+           (S->waiting.empty() && S->on_device == 0 && S->to_convert.empty() && S->converting == 0);
+  };
   if (timeout_ms < 0) S->cv_done.wait(lk, ready);
   else if (timeout_ms > 0) S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
   uint32_t n = 0;
@@ -620,7 +680,7 @@ uint32_t warpjq_serve_poll(warpjq_server *S, warpjq_serve_result *done, uint32_t
 
 uint64_t warpjq_serve_pending(warpjq_server *S) {
   std::lock_guard<std::mutex> lk(S->mu);
-  return S->waiting.size() + S->on_device + S->done.size();
+  return S->to_convert.size() + S->converting + S->waiting.size() + S->on_device + S->done.size();
 }
 
 void warpjq_serve_close(warpjq_server *S) {
@@ -628,10 +688,20 @@ void warpjq_serve_close(warpjq_server *S) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
     S->stop = true;
+    for (auto &r : S->waiting)
+      if (r.owned) cudaFreeAsync(r.owned, S->conv_st);
     S->waiting.clear();
+    S->to_convert.clear();
   }
   S->cv_loop.notify_all();
+  S->cv_conv.notify_all();
   if (S->loop.joinable()) S->loop.join();
+  if (S->converter.joinable()) S->converter.join();
+  if (S->conv) warpjq_csv_destroy(S->conv);
+  if (S->conv_st) {
+    cudaStreamSynchronize(S->conv_st);
+    cudaStreamDestroy(S->conv_st);
+  }
   for (auto &x : S->done) free(x.out);
   for (auto &s : S->slots) {
     if (s.st) cudaStreamSynchronize(s.st);
