@@ -5,7 +5,8 @@
  * context's set-up every time.  A server keeps, for a fixed list of
  * queries, every device context, compiled plan, stream, CSV converter and
  * staging buffer alive, and runs requests (one query over one input each)
- * with continuous batching: a native loop thread admits waiting requests
+ * with continuous batching (CSV requests first converted on the device by
+ * a converter thread): a native loop thread admits waiting requests
  * into a free slot while earlier slots are still on the device, as long as
  * their device-memory footprints fit the budget beside what is in flight
  * (in arrival order, no overtaking), runs each slot's requests as one

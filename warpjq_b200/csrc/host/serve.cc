@@ -6,13 +6,13 @@
 // one device context and compiled plan) per served query, a driver context
 // for mixed batches, a device arena for inputs that are not usable in place,
 // and page-locked buffers for row output; all of it lives as long as the
-// server.  CSV requests are converted to NDJSON on the device by a thread of
-// their own before they join the queue.  One loop thread does everything that touches the
-// device: it completes slots whose event has fired, then gives each free
-// slot the longest prefix of the waiting requests that fits the memory
-// budget beside what is in flight, so requests that arrive while others run
-// are admitted as slots and memory free up and the slots' work overlaps on
-// the device.
+// server.  CSV requests are converted to NDJSON on the device by a converter
+// thread (its own converter and stream) before they join the queue.  One
+// loop thread runs the slots: it completes slots whose event has fired, then
+// gives each free slot the longest prefix of the waiting requests that fits
+// the memory budget beside what is in flight, so requests that arrive while
+// others run are admitted as slots and memory free up and the slots' work
+// overlaps on the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
