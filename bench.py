@@ -833,10 +833,10 @@ def main():
         # the serving configuration: 1 KB - 256 MB requests, 20% CSV, some
         # from host memory, at three arrival rates; the one-at-a-time server
         # and the per-process / CPU comparators beside it
-        sreqs, keep = serve_pool(wjq, dev, hnp, n, 2000)
+        sreqs, keep = serve_pool(wjq, dev, hnp, n, 4000)
         serve = {"queries": len(SERVE_QUERIES), "csv_share": 0.2, "host_share_of_ndjson": 0.3,
                  "sizes": "log-uniform 1 KB - 256 MB", "budget_bytes": 120 << 30, "rates": []}
-        for rate, k in ((50.0, 100), (500.0, 1000), (2000.0, 2000)):
+        for rate, k in ((50.0, 100), (500.0, 1000), (2000.0, 4000)):
             sub = sreqs[:k]
             span = k / rate
             entry = {"offered_req_per_s": rate, "requests": k,
