@@ -379,7 +379,7 @@ def serve_pool(wjq, dsrc, hnp, n, n_req, seed=11, lo=1 << 10, hi=256 << 20, csv_
     return reqs, csv_pool
 
 
-def measure_serving(wjq, reqs, rate, n_slots=4, max_batch=0, seed=5):
+def measure_serving(wjq, reqs, rate, n_slots=4, max_batch=0, seed=5, mixed_min=0):
     """Open-loop Poisson arrivals at `rate` req/s through the native serving
     loop (include/warpjq_serve.h): continuous batching over `n_slots` slots
     with a 120 GB device-memory budget (with n_slots=1, max_batch=1: one
@@ -394,7 +394,8 @@ def measure_serving(wjq, reqs, rate, n_slots=4, max_batch=0, seed=5):
     total = sum(r[3] for r in reqs)
     # one batch per query in a slot (mixed batches carry every path and run
     # slower than the specialised kernels here)
-    srv = NativeServer(SERVE_QUERIES, n_slots=n_slots, budget_bytes=120 << 30, max_batch=max_batch, mixed_min=0)
+    srv = NativeServer(SERVE_QUERIES, n_slots=n_slots, budget_bytes=120 << 30, max_batch=max_batch,
+                       mixed_min=mixed_min)
     srv.warm(1 << 30)
     for q, x, f, _ in reqs[:32]:  # warm: every path once
         srv.submit(q, x, f)
