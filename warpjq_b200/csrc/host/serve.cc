@@ -142,9 +142,10 @@ struct warpjq_server {
   std::deque<Req> to_convert;
   uint64_t converting = 0;  // taken by the converter, not yet queued
   std::condition_variable cv_conv;
-  warpjq_csv *conv = nullptr;
-  cudaStream_t conv_st = nullptr;
-  std::thread converter;
+  static constexpr int kConverters = 2;  // conversions overlap: each waits on its own kernels
+  warpjq_csv *conv[kConverters] = {nullptr, nullptr};
+  cudaStream_t conv_st[kConverters] = {nullptr, nullptr};
+  std::thread converter[kConverters];
 };
 
 namespace {
@@ -418,7 +419,9 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
 // The converter thread: CSV requests in arrival order, each converted on the
 // device into a buffer of its own and then queued for admission as NDJSON
 // (a request that fails to convert completes with its error).
-void converter_main(warpjq_server *S) {
+void converter_main(warpjq_server *S, int ci) {
+  warpjq_csv *conv = S->conv[ci];
+  cudaStream_t cst = S->conv_st[ci];
   cudaSetDevice(S->device);
   for (;;) {
     Req r;
@@ -434,17 +437,17 @@ void converter_main(warpjq_server *S) {
     const uint8_t *d = nullptr;
     uint64_t nd = 0, consumed = 0, recs = 0;
     char e[512] = {0};
-    warpjq_csv_reset(S->conv);
+    warpjq_csv_reset(conv);
     const uint32_t fl = WARPJQ_CSV_FINAL | ((r.flags & WARPJQ_SERVE_DEVICE) ? 0u : WARPJQ_CSV_HOST_INPUT);
-    if (warpjq_csv_convert(S->conv, r.data, r.len, fl, S->conv_st, &d, &nd, &consumed, &recs, e, sizeof e) !=
+    if (warpjq_csv_convert(conv, r.data, r.len, fl, cst, &d, &nd, &consumed, &recs, e, sizeof e) !=
         WARPJQ_OK) {
       why = std::string("CSV conversion failed: ") + e;
-    } else if (cudaMallocAsync((void **)&r.owned, nd + 16, S->conv_st) != cudaSuccess) {
+    } else if (cudaMallocAsync((void **)&r.owned, nd + 16, cst) != cudaSuccess) {
       r.owned = nullptr;
       why = "out of device memory for the converted CSV";
     } else {
-      if (nd) cudaMemcpyAsync(r.owned, d, nd, cudaMemcpyDeviceToDevice, S->conv_st);
-      if (cudaStreamSynchronize(S->conv_st) != cudaSuccess) why = "CUDA error converting CSV";
+      if (nd) cudaMemcpyAsync(r.owned, d, nd, cudaMemcpyDeviceToDevice, cst);
+      if (cudaStreamSynchronize(cst) != cudaSuccess) why = "CUDA error converting CSV";
       r.addr = (uint64_t)(uintptr_t)r.owned;
       r.nd = nd;
     }
@@ -454,7 +457,7 @@ void converter_main(warpjq_server *S) {
       if (why.empty()) {
         S->waiting.push_back(r);
       } else {
-        if (r.owned) cudaFreeAsync(r.owned, S->conv_st);
+        if (r.owned) cudaFreeAsync(r.owned, cst);
         S->done.push_back(fail_result(r, why));
       }
     }
@@ -552,11 +555,17 @@ int warpjq_serve_open(const char *const *queries, uint32_t n_queries, const warp
       return fail(1, e);
     if (warpjq_csv_create(&s.conv) != WARPJQ_OK) return fail(1, "CUDA error: creating a CSV converter");
   }
-  if (warpjq_csv_create(&S->conv) != WARPJQ_OK ||
-      cudaStreamCreateWithFlags(&S->conv_st, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(1, "CUDA error: creating the CSV converter");
+  // the converter's stream at the highest priority: its kernels are short
+  // and the converter thread waits on each of them, so they go ahead of the
+  // slots' queued scans
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  for (int c = 0; c < warpjq_server::kConverters; c++)
+    if (warpjq_csv_create(&S->conv[c]) != WARPJQ_OK ||
+        cudaStreamCreateWithPriority(&S->conv_st[c], cudaStreamNonBlocking, prio_hi) != cudaSuccess)
+      return fail(1, "CUDA error: creating a CSV converter");
   S->loop = std::thread(loop_main, S);
-  S->converter = std::thread(converter_main, S);
+  for (int c = 0; c < warpjq_server::kConverters; c++) S->converter[c] = std::thread(converter_main, S, c);
   *out = S;
   return 0;
 }
@@ -613,13 +622,15 @@ int warpjq_serve_warm(warpjq_server *S, uint64_t reserve_bytes, char *err, size_
     const uint8_t *o = nullptr;
     uint64_t nd, consumed, recs;
     char e[512] = {0};
-    warpjq_csv_reset(S->conv);
-    if (warpjq_csv_convert(S->conv, dc, rows.size(), WARPJQ_CSV_FINAL, S->conv_st, &o, &nd, &consumed, &recs, e,
-                           sizeof e) != WARPJQ_OK) {
-      put_err(err, err_len, std::string("CUDA error: ") + e);
-      rc = 1;
+    for (int c = 0; c < warpjq_server::kConverters; c++) {
+      warpjq_csv_reset(S->conv[c]);
+      if (warpjq_csv_convert(S->conv[c], dc, rows.size(), WARPJQ_CSV_FINAL, S->conv_st[c], &o, &nd, &consumed,
+                             &recs, e, sizeof e) != WARPJQ_OK) {
+        put_err(err, err_len, std::string("CUDA error: ") + e);
+        rc = 1;
+      }
+      cudaStreamSynchronize(S->conv_st[c]);
     }
-    cudaStreamSynchronize(S->conv_st);
   }
   cudaFree(d);
   cudaFree(dc);
@@ -689,18 +700,21 @@ void warpjq_serve_close(warpjq_server *S) {
     std::lock_guard<std::mutex> lk(S->mu);
     S->stop = true;
     for (auto &r : S->waiting)
-      if (r.owned) cudaFreeAsync(r.owned, S->conv_st);
+      if (r.owned) cudaFreeAsync(r.owned, S->conv_st[0]);
     S->waiting.clear();
     S->to_convert.clear();
   }
   S->cv_loop.notify_all();
   S->cv_conv.notify_all();
   if (S->loop.joinable()) S->loop.join();
-  if (S->converter.joinable()) S->converter.join();
-  if (S->conv) warpjq_csv_destroy(S->conv);
-  if (S->conv_st) {
-    cudaStreamSynchronize(S->conv_st);
-    cudaStreamDestroy(S->conv_st);
+  for (auto &t : S->converter)
+    if (t.joinable()) t.join();
+  for (int c = 0; c < warpjq_server::kConverters; c++) {
+    if (S->conv[c]) warpjq_csv_destroy(S->conv[c]);
+    if (S->conv_st[c]) {
+      cudaStreamSynchronize(S->conv_st[c]);
+      cudaStreamDestroy(S->conv_st[c]);
+    }
   }
   for (auto &x : S->done) free(x.out);
   for (auto &s : S->slots) {
