@@ -379,7 +379,7 @@ def serve_pool(wjq, dsrc, hnp, n, n_req, seed=11, lo=1 << 10, hi=256 << 20, csv_
     return reqs, csv_pool
 
 
-def measure_serving(wjq, reqs, rate, n_slots=4, max_batch=0, seed=5, mixed_min=0):
+def measure_serving(wjq, reqs, rate, n_slots=8, max_batch=0, seed=5, mixed_min=0):
     """Open-loop Poisson arrivals at `rate` req/s through the native serving
     loop (include/warpjq_serve.h): continuous batching over `n_slots` slots
     with a 120 GB device-memory budget (with n_slots=1, max_batch=1: one
