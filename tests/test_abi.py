@@ -65,3 +65,12 @@ def test_no_device_is_reported_cleanly_without_a_gpu():
     if torch.cuda.is_available():
         pytest.skip("a GPU is present")
     assert wjq.probe() != ""
+
+
+def test_serving_open_fails_cleanly_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from warpjq_b200.serve import NativeServer
+    with pytest.raises(RuntimeError):
+        NativeServer(["count"], n_slots=2)

@@ -709,6 +709,10 @@ void warpjq_serve_close(warpjq_server *S) {
   if (S->loop.joinable()) S->loop.join();
   for (auto &t : S->converter)
     if (t.joinable()) t.join();
+  // a conversion that finished while the threads stopped queued its request
+  for (auto &r : S->waiting)
+    if (r.owned) cudaFreeAsync(r.owned, S->conv_st[0]);
+  S->waiting.clear();
   for (int c = 0; c < warpjq_server::kConverters; c++) {
     if (S->conv[c]) warpjq_csv_destroy(S->conv[c]);
     if (S->conv_st[c]) {
