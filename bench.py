@@ -482,7 +482,7 @@ NESTED_QUERIES = [
 ]
 
 
-def measure_nested(wjq, n_bytes=2_000_000_000, reps=3, check=True):
+def measure_nested(wjq, n_bytes=4_000_000_000, reps=3, check=True):
     """Device-resident GB/s of the nested workload's two queries (best of
     `reps` after a warm-up run; CUDA events around all kernels of a run)."""
     import torch
@@ -493,7 +493,7 @@ def measure_nested(wjq, n_bytes=2_000_000_000, reps=3, check=True):
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     out = {"bytes": n, "lines": lines, "residency": "device",
-           "sizes": "2 GB (rescaled from 4 GB for the bench's time budget), 1M Zipf(0.9) user ids",
+           "sizes": f"{n_bytes / 1e9:g} GB, 1M Zipf(0.9) user ids",
            "per_query_gbs": {}}
     outs = []
     for q in NESTED_QUERIES:
