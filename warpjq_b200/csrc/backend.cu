@@ -81,9 +81,17 @@ struct RunBufs {
   DevBuf<uint32_t> b_tile_input;
   DevBuf<unsigned long long> b_in_start, b_in_end, b_in_tile0;
   DevBuf<RunCounters> b_in_ctr;
-  // mixed batches: the inputs' distinct plans and each input's plan index
+  // mixed batches: the inputs' distinct plans, each input's plan index, the
+  // inputs in plan order with their running tile counts, the tiles of each
+  // plan's inputs (one list after another, built on the device), each
+  // plan's launch's ticket counter and the row launches' per-CTA record
+  // counts
   DevBuf<DevPlan> b_plans;
   DevBuf<uint32_t> b_in_plan;
+  DevBuf<uint32_t> b_list_inputs;
+  DevBuf<unsigned long long> b_list_tile0;
+  DevBuf<uint32_t> b_plan_tiles;
+  DevBuf<unsigned long long> b_tickets, b_rec_cursor;
   DevBuf<uint8_t> recs;
   DevBuf<uint8_t> out;
   DevBuf<unsigned long long> row_off, line_idx;
@@ -108,6 +116,11 @@ struct RunBufs {
     b_in_ctr.release();
     b_plans.release();
     b_in_plan.release();
+    b_list_inputs.release();
+    b_list_tile0.release();
+    b_plan_tiles.release();
+    b_tickets.release();
+    b_rec_cursor.release();
     recs.release(); out.release(); row_off.release(); line_idx.release();
     block_lines.release(); deep.release(); g_slots.release();
     g_keys.release(); g_acc.release();
@@ -201,12 +214,16 @@ struct warpjq_ctx {
     uint32_t rec_stride = 0;
     std::vector<DevPlan> plans;
     std::vector<uint32_t> in_plan;
+    // the inputs in plan order, their running tile counts (list_tile0, one
+    // more entry than inputs), and plan k's share of those tiles
+    // [plan_tile0[k], plan_tile0[k + 1])
+    std::vector<uint32_t> list_inputs;
+    std::vector<unsigned long long> list_tile0, plan_tile0;
     uint64_t epoch = 0;             // bumped whenever a plain batch replaces the device tables
     const uint8_t *d_data = nullptr;
     cudaStream_t stream = nullptr;
     unsigned long long n_tiles = 0, total = 0;
     std::vector<unsigned long long> start, end, tile0;
-    std::vector<uint32_t> tile_input;
     std::vector<RunCounters> h_ctr;
     std::vector<warpjq_group_ext> groups;
     std::vector<uint32_t> group_input;
@@ -354,11 +371,13 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     // The tables are packed into page-locked staging and copied from there:
     // a copy from pageable memory would make the host wait for the stream's
     // earlier work (the previous batches of a serving slot).
-    const size_t n8 = n_inputs * 8ull, t8 = (n_inputs + 1) * 8ull, tt = n_tiles * 4ull;
-    const size_t p_in = n_inputs * 4ull, p_pl = b->mixed ? b->plans.size() * sizeof(DevPlan) : 0;
+    // (Per-tile tables are built on the device from these, below.)
+    const size_t n8 = n_inputs * 8ull, t8 = (n_inputs + 1) * 8ull, n4 = n_inputs * 4ull;
+    const size_t p_pl = b->mixed ? b->plans.size() * sizeof(DevPlan) : 0, p_m4 = b->mixed ? n4 : 0,
+                 p_m8 = b->mixed ? t8 : 0;
     auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
-    const size_t o_end = up16(n8), o_t0 = o_end + up16(n8), o_ti = o_t0 + up16(t8), o_ip = o_ti + up16(tt),
-                 o_pl = o_ip + up16(p_in), need = o_pl + p_pl;
+    const size_t o_end = up16(n8), o_t0 = o_end + up16(n8), o_ip = o_t0 + up16(t8), o_pl = o_ip + up16(p_m4),
+                 o_li = o_pl + up16(p_pl), o_lt = o_li + up16(p_m4), need = o_lt + p_m8;
     if (!s.btab_done) CK(cudaEventCreateWithFlags(&s.btab_done, cudaEventDisableTiming), "event");
     CK(cudaEventSynchronize(s.btab_done), "batch staging wait");  // the last batch's copies are done
     if (need > s.h_btab_cap) {
@@ -375,26 +394,47 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       std::memcpy(hb + o_end, b->end.data(), n8);
     }
     std::memcpy(hb + o_t0, b->tile0.data(), t8);
-    if (tt) std::memcpy(hb + o_ti, b->tile_input.data(), tt);
     if (b->mixed) {
       CK(rb.b_plans.ensure(b->plans.size(), st, capturing), "alloc batch plans");
       CK(rb.b_in_plan.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch plans");
-      if (p_in) std::memcpy(hb + o_ip, b->in_plan.data(), p_in);
+      CK(rb.b_list_inputs.ensure(std::max<uint32_t>(n_inputs, 1), st, capturing), "alloc batch plans");
+      CK(rb.b_list_tile0.ensure(n_inputs + 1, st, capturing), "alloc batch plans");
+      CK(rb.b_plan_tiles.ensure(std::max<unsigned long long>(n_tiles, 1), st, capturing), "alloc batch plans");
       std::memcpy(hb + o_pl, b->plans.data(), p_pl);
+      if (n4) {
+        std::memcpy(hb + o_ip, b->in_plan.data(), n4);
+        std::memcpy(hb + o_li, b->list_inputs.data(), n4);
+      }
+      std::memcpy(hb + o_lt, b->list_tile0.data(), t8);
       CK(cudaMemcpyAsync(rb.b_plans.p, hb + o_pl, p_pl, cudaMemcpyHostToDevice, st), "H2D batch plans");
-      if (p_in) CK(cudaMemcpyAsync(rb.b_in_plan.p, hb + o_ip, p_in, cudaMemcpyHostToDevice, st), "H2D batch plans");
+      if (n4) {
+        CK(cudaMemcpyAsync(rb.b_in_plan.p, hb + o_ip, n4, cudaMemcpyHostToDevice, st), "H2D batch plans");
+        CK(cudaMemcpyAsync(rb.b_list_inputs.p, hb + o_li, n4, cudaMemcpyHostToDevice, st), "H2D batch plans");
+      }
+      CK(cudaMemcpyAsync(rb.b_list_tile0.p, hb + o_lt, t8, cudaMemcpyHostToDevice, st), "H2D batch plans");
     }
     if (n8) {
       CK(cudaMemcpyAsync(rb.b_in_start.p, hb, n8, cudaMemcpyHostToDevice, st), "H2D batch tables");
       CK(cudaMemcpyAsync(rb.b_in_end.p, hb + o_end, n8, cudaMemcpyHostToDevice, st), "H2D batch tables");
     }
     CK(cudaMemcpyAsync(rb.b_in_tile0.p, hb + o_t0, t8, cudaMemcpyHostToDevice, st), "H2D batch tables");
-    if (tt) CK(cudaMemcpyAsync(rb.b_tile_input.p, hb + o_ti, tt, cudaMemcpyHostToDevice, st), "H2D batch tables");
     CK(cudaEventRecord(s.btab_done, st), "event record");
   }
-  if (b && n_inputs) k_batch_reset<<<(n_inputs + 255) / 256, 256, 0, st>>>(rb.b_in_ctr.p, n_inputs);
-  GroupTable g = group_view(rb, groups);
   s.kernels = 0;
+  if (b && n_inputs) {
+    k_batch_reset<<<(n_inputs + 255) / 256, 256, 0, st>>>(rb.b_in_ctr.p, n_inputs);
+    s.kernels++;
+    if (n_tiles) {
+      const unsigned nb = (unsigned)std::min<unsigned long long>((n_tiles + 255) / 256, 8ull * c->num_sms);
+      k_batch_expand<<<nb, 256, 0, st>>>(n_tiles, n_inputs, rb.b_in_tile0.p, rb.b_tile_input.p,
+                                         b->mixed ? rb.b_list_inputs.p : nullptr,
+                                         b->mixed ? rb.b_list_tile0.p : nullptr,
+                                         b->mixed ? rb.b_plan_tiles.p : nullptr);
+      s.kernels++;
+      CK(cudaGetLastError(), "launch batch tables");
+    }
+  }
+  GroupTable g = group_view(rb, groups);
   k_reset_run<<<256, 256, 0, st>>>(rb.ctr.p, g, groups ? rb.g_cap : 0, groups ? rb.g_key_cap : 0);
   s.kernels++;
   CK(cudaGetLastError(), "launch reset");
@@ -415,10 +455,13 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.deep_levels_per_cta = rb.deep_levels;
     sp.rec_stride = run_rec_stride(c, b);
     if (b && b->mixed) {
-      sp.plans = rb.b_plans.p;
-      sp.in_plan = rb.b_in_plan.p;
       sp.any_grouped = b->any_grouped ? 1u : 0u;
       sp.any_rows = b->any_rows ? 1u : 0u;
+      CK(rb.b_tickets.ensure(b->plans.size(), st, capturing), "alloc batch tickets");
+      CK(rb.b_rec_cursor.ensure(c->grid, st, capturing), "alloc batch tickets");
+      CK(cudaMemsetAsync(rb.b_tickets.p, 0, b->plans.size() * sizeof(unsigned long long), st), "reset tickets");
+      if (b->any_rows)
+        CK(cudaMemsetAsync(rb.b_rec_cursor.p, 0, c->grid * sizeof(unsigned long long), st), "reset tickets");
     }
     if (b) {
       sp.tile_input = rb.b_tile_input.p;
@@ -438,10 +481,35 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     }
     s.timed = !capturing;  // a captured sequence is not timed
     if (s.timed) CK(cudaEventRecord(s.scan_t0, st), "event record");
-    if (b && b->mixed)  // the inputs' plans may group where the context's does not
-      k_scan<false, true><<<grid, kThreads, scan_smem_bytes(c->tile_bytes, c->halo_bytes, b->any_grouped), st>>>(
-          sp, c->plan);
-    else if (P.needs_rows)
+    if (b && b->mixed) {
+      // One launch per distinct plan over its inputs' tiles, each the
+      // variant specialised for that plan (the plan a kernel parameter, as
+      // in a plain run).  The launches share the run's counters, per-tile
+      // tables and group table; row launches append to the CTAs' record
+      // arenas one after another.
+      for (size_t k = 0; k < b->plans.size(); k++) {
+        const unsigned long long n_k = b->plan_tile0[k + 1] - b->plan_tile0[k];
+        if (!n_k) continue;
+        const DevPlan &Pk = b->plans[k];
+        const bool gk = Pk.output_kind == WARPJQ_OUT_AGG && Pk.group_slot >= 0;
+        ScanParams spk = sp;
+        spk.tile_list = rb.b_plan_tiles.p + b->plan_tile0[k];
+        spk.n_list = n_k;
+        spk.ticket = rb.b_tickets.p + k;
+        spk.rec_cursor = Pk.needs_rows ? rb.b_rec_cursor.p : nullptr;
+        const unsigned vg = Pk.needs_rows ? c->grid_rows : gk ? c->grid_group : c->grid_agg;
+        const unsigned gr = (unsigned)std::min<unsigned long long>(vg, n_k);
+        const size_t smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes, gk);
+        if (Pk.needs_rows)
+          k_scan<true><<<gr, kThreads, smem, st>>>(spk, Pk);
+        else if (gk)
+          k_scan<false, false, true><<<gr, kThreads, smem, st>>>(spk, Pk);
+        else
+          k_scan<false><<<gr, kThreads, smem, st>>>(spk, Pk);
+        s.kernels++;
+      }
+      s.kernels--;  // counted once more below
+    } else if (P.needs_rows)
       k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
     else if (groups)
       k_scan<false, false, true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
@@ -583,6 +651,10 @@ uint64_t bufs_signature(const warpjq_ctx *c) {
   mix((uintptr_t)rb.b_tile_input.p); mix(rb.b_tile_input.n);
   mix((uintptr_t)rb.b_in_start.p); mix((uintptr_t)rb.b_in_end.p);
   mix((uintptr_t)rb.b_in_tile0.p); mix((uintptr_t)rb.b_in_ctr.p);
+  mix((uintptr_t)rb.b_plans.p); mix((uintptr_t)rb.b_in_plan.p); mix((uintptr_t)rb.b_plan_tiles.p);
+  mix((uintptr_t)rb.b_list_inputs.p); mix((uintptr_t)rb.b_list_tile0.p);
+  mix(rb.b_plan_tiles.n); mix((uintptr_t)rb.b_tickets.p); mix(rb.b_tickets.n);
+  mix((uintptr_t)rb.b_rec_cursor.p); mix(rb.b_rec_cursor.n);
   mix((uintptr_t)rb.recs.p); mix(rb.recs.n);
   mix((uintptr_t)rb.out.p); mix(rb.out.n);
   mix((uintptr_t)rb.row_off.p); mix((uintptr_t)rb.line_idx.p);
@@ -1095,7 +1167,6 @@ static warpjq_status batch_prepare(warpjq_ctx *ctx, const uint8_t *d_data, const
   b.start.resize(n_inputs);
   b.end.resize(n_inputs);
   b.tile0.resize(n_inputs + 1);
-  b.tile_input.clear();
   b.total = 0;
   const unsigned long long T = ctx->tile_bytes;
   unsigned long long tiles = 0;
@@ -1107,9 +1178,7 @@ static warpjq_status batch_prepare(warpjq_ctx *ctx, const uint8_t *d_data, const
     b.start[i] = offsets[i];
     b.end[i] = offsets[i] + lengths[i];
     b.tile0[i] = tiles;
-    const unsigned long long nt = (lengths[i] + T - 1) / T;
-    b.tile_input.insert(b.tile_input.end(), nt, i);
-    tiles += nt;
+    tiles += (lengths[i] + T - 1) / T;
     b.total += lengths[i];
   }
   b.tile0[n_inputs] = tiles;
@@ -1162,6 +1231,25 @@ warpjq_status warpjq_batch_launch_mixed(warpjq_ctx *ctx, warpjq_ctx *const *inpu
   }
   if (b.plans.empty()) b.plans.push_back(ctx->plan);
   b.in_plan = std::move(in_plan);
+  // The inputs plan by plan (in input order within a plan) and their
+  // running tile counts; the device lists each plan's tiles from these.
+  const size_t n_plans = b.plans.size();
+  std::vector<uint32_t> first(n_plans + 1, 0);
+  for (uint32_t i = 0; i < n_inputs; i++) first[b.in_plan[i] + 1]++;
+  for (size_t k = 0; k < n_plans; k++) first[k + 1] += first[k];
+  b.list_inputs.resize(n_inputs);
+  for (uint32_t i = 0; i < n_inputs; i++) b.list_inputs[first[b.in_plan[i]]++] = i;
+  b.list_tile0.resize(n_inputs + 1);
+  b.plan_tile0.assign(n_plans + 1, 0);
+  unsigned long long run = 0;
+  for (uint32_t j = 0; j < n_inputs; j++) {
+    const uint32_t i = b.list_inputs[j];
+    b.list_tile0[j] = run;
+    run += b.tile0[i + 1] - b.tile0[i];
+    b.plan_tile0[b.in_plan[i] + 1] = run;
+  }
+  b.list_tile0[n_inputs] = run;
+  for (size_t k = 0; k < n_plans; k++) b.plan_tile0[k + 1] = std::max(b.plan_tile0[k + 1], b.plan_tile0[k]);
   rc = enqueue_run(ctx, ctx->dev, d_data, b.total, b.stream, err, err_len, &b);
   if (rc == WARPJQ_OK) b.active = true;
   return rc;

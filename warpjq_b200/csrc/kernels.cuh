@@ -212,6 +212,15 @@ struct ScanParams {
   uint32_t any_grouped;
   uint32_t any_rows;    // a mixed batch: one of the plans prints rows
   uint32_t rec_stride;  // bytes per row record (a mixed batch: the largest of its plans')
+  // A mixed batch runs as one launch per distinct plan: this launch takes
+  // its tiles from tile_list[0, n_list) (null: every tile) by tickets from
+  // *ticket (null: ctr->next_tile), and a CTA's records follow those its
+  // earlier launches of the batch appended (rec_cursor, one count per CTA,
+  // read at the start and written back at the end; null: none).
+  const uint32_t *tile_list;
+  unsigned long long n_list;
+  unsigned long long *ticket;
+  unsigned long long *rec_cursor;
 };
 
 // Rows emission.
@@ -695,7 +704,8 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
   deep.words = sp.deep_words + (unsigned long long)blockIdx.x * (sp.deep_levels_per_cta / 32);
   deep.cap_levels = sp.deep_levels_per_cta;
 
-  unsigned long long cta_recs = 0;  // records this CTA has appended (rows mode)
+  // records this CTA has appended (rows mode)
+  unsigned long long cta_recs = (kRows && sp.rec_cursor) ? sp.rec_cursor[blockIdx.x] : 0;
   NodeVals nv;
   SlotVal slots[kMaxSlots];
 
@@ -715,12 +725,15 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
 
   // Tickets are taken one tile ahead, so the atomic's latency overlaps a
   // tile's work.
+  unsigned long long *const ticket_ctr = sp.ticket ? sp.ticket : &sp.ctr->next_tile;
   unsigned long long next_ticket = 0;
-  if (lane == 0) next_ticket = atomicAdd(&sp.ctr->next_tile, 1ull);
+  if (lane == 0) next_ticket = atomicAdd(ticket_ctr, 1ull);
+  const unsigned long long n_work = sp.tile_list ? sp.n_list : sp.n_tiles;
   for (;;) {
-    const unsigned long long tile = __shfl_sync(0xffffffffu, next_ticket, 0);
-    if (tile >= sp.n_tiles) break;
-    if (lane == 0) next_ticket = atomicAdd(&sp.ctr->next_tile, 1ull);
+    const unsigned long long ticket = __shfl_sync(0xffffffffu, next_ticket, 0);
+    if (ticket >= n_work) break;
+    const unsigned long long tile = sp.tile_list ? sp.tile_list[ticket] : ticket;
+    if (lane == 0) next_ticket = atomicAdd(ticket_ctr, 1ull);
     // The tile's input: the whole data, or one input of a batch (a window
     // never reaches past its input's end).
     uint32_t input = 0;
@@ -804,9 +817,9 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
 
     // The next tile's window is fetched into L2 now (its ticket has
     // arrived), so its bulk copy reads from L2 rather than waiting on HBM.
-    if (lane == 0) {
-      const unsigned long long nt = next_ticket;
-      if (nt < sp.n_tiles) {
+    if (lane == 0 && next_ticket < n_work) {
+      const unsigned long long nt = sp.tile_list ? sp.tile_list[next_ticket] : next_ticket;
+      {
         unsigned long long ns = nt * T, ne = sp.n;
         if (sp.tile_input) {
           const uint32_t ni = sp.tile_input[nt];
@@ -1143,7 +1156,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         if (sp.tile_input) atomicMin(&ctr_in->first_type_tile, tile);
       }
     }
-    if (rowsT || (kMulti && sp.any_rows)) {  // an aggregate tile of a batch with rows has none
+    if (rowsT || sp.any_rows) {  // an aggregate tile of a batch with rows has none
       if (lane == 0) {
         RowTile rt;
         rt.rec_begin = (unsigned long long)blockIdx.x * sp.rec_cap_per_cta + tile_rec0;
@@ -1186,6 +1199,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
     }
   }
 
+  if (kRows && sp.rec_cursor && lane == 0) sp.rec_cursor[blockIdx.x] = cta_recs;
   // Flush this CTA's counters (a batch's were flushed per tile).
   flush_counts(sp.ctr, nullptr, P, kRows, lane, acc, cta_fix);
 }
@@ -1263,6 +1277,39 @@ __global__ void k_batch_reset(RunCounters *in_ctr, uint32_t n_inputs) {
     z.first_invalid = ~0ull;
     z.first_type_error = ~0ull;
     in_ctr[i] = z;
+  }
+}
+
+// The largest i in [0, n) with a[i] <= t (a[0] <= t, a ascending).
+__device__ __forceinline__ uint32_t last_at_or_below(const unsigned long long *a, uint32_t n,
+                                                     unsigned long long t) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (a[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// A batch's per-tile tables, built on the device from its per-input ones
+// (host work stays proportional to the inputs, not the tiles): tile t
+// belongs to the input i with in_tile0[i] <= t < in_tile0[i + 1] (an empty
+// input owns none, so the last input starting at or below t is its owner).
+// A mixed batch also lists, plan after plan, the tiles of each plan's
+// inputs: position p of list_tiles is tile p - list_tile0[j] of input
+// list_inputs[j] (list_tile0 running over the inputs in list order).
+__global__ void k_batch_expand(unsigned long long n_tiles, uint32_t n_inputs, const unsigned long long *in_tile0,
+                               uint32_t *tile_input, const uint32_t *list_inputs,
+                               const unsigned long long *list_tile0, uint32_t *list_tiles) {
+  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles;
+       t += (unsigned long long)gridDim.x * blockDim.x) {
+    tile_input[t] = last_at_or_below(in_tile0, n_inputs, t);
+    if (list_tiles) {
+      const uint32_t j = last_at_or_below(list_tile0, n_inputs, t);
+      const uint32_t i = list_inputs[j];
+      list_tiles[t] = (uint32_t)(in_tile0[i] + (t - list_tile0[j]));
+    }
   }
 }
 
