@@ -195,7 +195,7 @@ struct warpjq_ctx {
   uint32_t halo_bytes = 2048;
   uint32_t group_keys0 = 1u << 16;  // distinct keys a fresh group table has room for
   unsigned grid = 0;        // CTAs per-CTA buffers are sized for (the largest variant's grid)
-  unsigned grid_rows = 0, grid_agg = 0, grid_group = 0, grid_mixed = 0;  // persistent CTAs per variant
+  unsigned grid_rows = 0, grid_agg = 0, grid_group = 0;  // persistent CTAs per variant
   size_t scan_smem = 0;
   std::vector<Slot> slots;
   // device-resident runs
@@ -252,27 +252,22 @@ warpjq_status configure_grid(warpjq_ctx *c, char *err, size_t err_len) {
      "cudaFuncSetAttribute(scan rows)");
   CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
      "cudaFuncSetAttribute(scan agg)");
-  CK(cudaFuncSetAttribute(k_scan<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
-     "cudaFuncSetAttribute(scan grouped)");
   CK(cudaFuncSetAttribute(k_scan<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max),
-     "cudaFuncSetAttribute(scan mixed)");
+     "cudaFuncSetAttribute(scan grouped)");
   // Each variant runs as many CTAs per SM as its own registers and shared
   // memory allow; buffers sized per CTA take the largest of them.
-  int a = 0, b = 0, g = 0, m = 0;
+  int a = 0, b = 0, g = 0;
   const size_t grouped_smem = scan_smem_bytes(c->tile_bytes, c->halo_bytes, true);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_scan<true>, kThreads, c->scan_smem),
      "occupancy");
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scan<false>, kThreads, c->scan_smem),
      "occupancy");
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, k_scan<false, false, true>, kThreads, grouped_smem),
-     "occupancy");
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_scan<false, true>, kThreads, grouped_smem),
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, k_scan<false, true>, kThreads, grouped_smem),
      "occupancy");
   c->grid_rows = (unsigned)(c->num_sms * std::max(1, a));
   c->grid_agg = (unsigned)(c->num_sms * std::max(1, b));
   c->grid_group = (unsigned)(c->num_sms * std::max(1, g));
-  c->grid_mixed = (unsigned)(c->num_sms * std::max(1, m));
-  per_sm = std::max(std::max(a, b), std::max(g, m));
+  per_sm = std::max(std::max(a, b), g);
   c->grid = (unsigned)(c->num_sms * std::max(1, per_sm));
   return WARPJQ_OK;
 }
@@ -455,7 +450,6 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
     sp.deep_levels_per_cta = rb.deep_levels;
     sp.rec_stride = run_rec_stride(c, b);
     if (b && b->mixed) {
-      sp.any_grouped = b->any_grouped ? 1u : 0u;
       sp.any_rows = b->any_rows ? 1u : 0u;
       CK(rb.b_tickets.ensure(b->plans.size(), st, capturing), "alloc batch tickets");
       CK(rb.b_rec_cursor.ensure(c->grid, st, capturing), "alloc batch tickets");
@@ -470,11 +464,6 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
       sp.in_tile0 = rb.b_in_tile0.p;
       sp.in_ctr = rb.b_in_ctr.p;
     }
-    const unsigned vgrid = (b && b->mixed) ? c->grid_mixed
-                           : P.needs_rows ? c->grid_rows
-                           : groups      ? c->grid_group
-                                         : c->grid_agg;
-    unsigned grid = (unsigned)std::min<unsigned long long>(vgrid, n_tiles);
     if (!s.scan_t0 && !capturing) {
       CK(cudaEventCreate(&s.scan_t0), "event");
       CK(cudaEventCreate(&s.scan_t1), "event");
@@ -503,20 +492,24 @@ warpjq_status enqueue_run(warpjq_ctx *c, Slot &s, const uint8_t *d_data, unsigne
         if (Pk.needs_rows)
           k_scan<true><<<gr, kThreads, smem, st>>>(spk, Pk);
         else if (gk)
-          k_scan<false, false, true><<<gr, kThreads, smem, st>>>(spk, Pk);
+          k_scan<false, true><<<gr, kThreads, smem, st>>>(spk, Pk);
         else
           k_scan<false><<<gr, kThreads, smem, st>>>(spk, Pk);
         s.kernels++;
+        CK(cudaGetLastError(), "launch scan");
       }
-      s.kernels--;  // counted once more below
-    } else if (P.needs_rows)
-      k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
-    else if (groups)
-      k_scan<false, false, true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
-    else
-      k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
-    s.kernels++;
-    CK(cudaGetLastError(), "launch scan");
+    } else {
+      const unsigned vgrid = P.needs_rows ? c->grid_rows : groups ? c->grid_group : c->grid_agg;
+      const unsigned grid = (unsigned)std::min<unsigned long long>(vgrid, n_tiles);
+      if (P.needs_rows)
+        k_scan<true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
+      else if (groups)
+        k_scan<false, true><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
+      else
+        k_scan<false><<<grid, kThreads, c->scan_smem, st>>>(sp, c->plan);
+      s.kernels++;
+      CK(cudaGetLastError(), "launch scan");
+    }
     if (s.timed) CK(cudaEventRecord(s.scan_t1, st), "event record");
     if (rows) {
       const uint32_t tpb = rows_tiles_per_block(n_tiles);

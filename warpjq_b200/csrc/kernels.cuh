@@ -205,12 +205,8 @@ struct ScanParams {
   const unsigned long long *in_end;
   const unsigned long long *in_tile0;
   RunCounters *in_ctr;
-  // Mixed batches (k_scan<false, true>): input i runs plans[in_plan[i]];
-  // any_grouped when one of them groups.
-  const DevPlan *plans;
-  const uint32_t *in_plan;
-  uint32_t any_grouped;
-  uint32_t any_rows;    // a mixed batch: one of the plans prints rows
+  uint32_t any_rows;    // a mixed batch one of whose plans prints rows (its
+                        // aggregate launches write empty row tiles)
   uint32_t rec_stride;  // bytes per row record (a mixed batch: the largest of its plans')
   // A mixed batch runs as one launch per distinct plan: this launch takes
   // its tiles from tile_list[0, n_list) (null: every tile) by tickets from
@@ -677,11 +673,9 @@ __device__ __noinline__ void flush_counts(RunCounters *dst, RunCounters *also, c
 
 // The plan is a kernel parameter (constant bank): fields at fixed offsets
 // are instruction operands, and no plan read goes through global memory.
-// kMulti (aggregates only): a mixed batch, each input with its own plan,
-// taken per tile from sp.plans in device memory instead of `plan`.
-// kGroups: the group-by path is compiled in (grouped aggregates, mixed
-// batches); without it the kernel is lighter for every other query.
-template <bool kRows, bool kMulti = false, bool kGroups = kMulti>
+// kGroups: the group-by path is compiled in (grouped aggregates); without
+// it the kernel is lighter for every other query.
+template <bool kRows, bool kGroups = false>
 __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : (kRows ? kScanBlocksPerSMRows : kScanBlocksPerSM))
     k_scan(const __grid_constant__ ScanParams sp, const __grid_constant__ DevPlan plan) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -711,7 +705,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
 
   if (lane < kFixDigits) cta_fix[lane] = 0;
   if (lane == 0) acc->clear();
-  const bool grouped = kGroups && !kRows && (kMulti ? sp.any_grouped != 0 : P.group_slot >= 0);
+  const bool grouped = kGroups && !kRows && P.group_slot >= 0;
   if (grouped) {
     for (int k = lane; k < kGroupCache; k += 32) {
       gcache->tag[k] = 0xFFFFFFFFu;
@@ -746,10 +740,6 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
       ts = data_start + (tile - sp.in_tile0[input]) * T;
       ctr_in = sp.in_ctr + input;
     }
-    // The tile's plan (a mixed batch: its input's own).
-    const DevPlan &P = kMulti ? sp.plans[sp.in_plan[input]] : plan;
-    // Whether the tile's query prints rows (a mixed batch holds both kinds).
-    const bool rowsT = kMulti ? P.needs_rows != 0 : kRows;
     const uint32_t nf = P.output_kind == 2 ? P.n_fields : (P.output_kind == 1 ? 1u : 0u);
     const unsigned long long te = min(ts + T, data_end);
     const uint32_t tlen = (uint32_t)(te - ts);
@@ -951,7 +941,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         } else if (status == LS_TYPE_ERROR) {
           tile_first_type = min(tile_first_type, ordinal);
         } else if (status == 101) {
-          if (rowsT) {
+          if (kRows) {
             has_row = 1;
             row_len = row_length(P, lp, out_len, slots);
           } else {
@@ -987,7 +977,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         }
 
         // Aggregate contribution of this line.
-        bool contrib = !rowsT && status == 101;
+        bool contrib = !kRows && status == 101;
         long long iv = 0;
         double fv = 0.0;
         bool is_int = false, is_num = false;
@@ -1041,7 +1031,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
             }
           }
         }
-        if (kGroups && !rowsT && P.group_slot >= 0) {
+        if (kGroups && !kRows && P.group_slot >= 0) {
           // Lanes whose keys hash alike compare their key bytes with the
           // lowest such lane; only lanes that differ from it look up the
           // table themselves.
@@ -1108,7 +1098,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
             sp.g.keys[kid].saw_non_numeric = 1;
         }
 
-        if (rowsT) {
+        if (kRows) {
           uint32_t er, tr;
           unsigned long long eb, tb;
           warp_scan2(has_row, (unsigned long long)row_len, er, eb, tr, tb);
@@ -1156,7 +1146,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
         if (sp.tile_input) atomicMin(&ctr_in->first_type_tile, tile);
       }
     }
-    if (rowsT || sp.any_rows) {  // an aggregate tile of a batch with rows has none
+    if (kRows || sp.any_rows) {  // an aggregate tile of a batch with rows has none
       if (lane == 0) {
         RowTile rt;
         rt.rec_begin = (unsigned long long)blockIdx.x * sp.rec_cap_per_cta + tile_rec0;
@@ -1168,7 +1158,7 @@ __global__ void __launch_bounds__(kThreads, kGroups ? kScanBlocksPerSMGrouped : 
     }
     // A batch input's counts and aggregate go to its own record, tile by tile.
     if (sp.tile_input)
-      flush_counts(ctr_in, sp.ctr, P, rowsT, lane, acc, cta_fix);
+      flush_counts(ctr_in, sp.ctr, P, kRows, lane, acc, cta_fix);
   }
 
   // Merge this CTA's cached group accumulators into the global records.
