@@ -163,14 +163,14 @@ warpjq_status warpjq_batch_launch(warpjq_ctx *ctx, const uint8_t *d_data, const 
                                   char *err, size_t err_len);
 
 /* A mixed batch: like warpjq_batch_launch, but input i runs the query of
- * input_ctx[i], so inputs with different queries share one launch of the
- * persistent scan kernel (each tile takes its input's plan from device
- * memory).  Aggregate queries only (count, sum, min, max, avg, group_by,
- * with or without select): every input_ctx[i], and `ctx`, must hold one;
- * WARPJQ_ERR_INVALID_ARG otherwise.  `ctx` supplies the buffers, tiling and
- * stream order, and is collected with warpjq_batch_collect; each item's
- * aggregate and groups are then rendered by its own query (its host
- * formatter knows the aggregate kind).  The input contexts are only read
+ * input_ctx[i], so inputs with different queries share one launch sequence:
+ * one launch of the persistent scan per distinct query, each over the tiles
+ * of that query's inputs with its plan as a kernel parameter, then one set
+ * of row, reduce and finalize passes.  Aggregate and row queries alike; each
+ * input's rows are a contiguous range of the batch's output, in input
+ * order.  `ctx` supplies the buffers, tiling and stream order, and is
+ * collected with warpjq_batch_collect; each item is then rendered by its own
+ * query (warpjq_query_render_batch).  The input contexts are only read
  * during this call.  No reference counterpart. */
 warpjq_status warpjq_batch_launch_mixed(warpjq_ctx *ctx, warpjq_ctx *const *input_ctx,
                                         const uint8_t *d_data, const uint64_t *offsets,
