@@ -417,7 +417,8 @@ class Query:
     def batch_launch_mixed(self, queries, d_ptr: int, offsets, lengths, stream: int = 0):
         """Enqueues one mixed batch on this query's context: input i is
         d_ptr[offsets[i], + lengths[i]) and runs queries[i] (aggregate or row
-        queries; each tile takes its input's plan).  Collect with
+        queries; one scan launch per distinct query over its inputs' tiles,
+        each specialised for that query).  Collect with
         batch_collect() and render with batch_outputs_mixed()."""
         k, _ = _load()
         n = len(offsets)
