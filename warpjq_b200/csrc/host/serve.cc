@@ -286,6 +286,10 @@ void complete_batch(warpjq_server *S, Slot &s, warpjq_ctx *ctx, warpjq_query *q,
 
 void complete_slot(warpjq_server *S, Slot &s) {
   std::vector<warpjq_serve_result> out;
+  // the requests this slot launched (those that failed at admission were
+  // completed and counted off then, though they stay in s.reqs)
+  size_t launched = s.mixed.size();
+  for (auto &v : s.by_q) launched += v.size();
   if (!s.mixed.empty()) complete_batch(S, s, warpjq_query_ctx(s.driver), s.driver, s.mixed, true, out);
   for (size_t qi = 0; qi < s.by_q.size(); qi++)
     if (!s.by_q[qi].empty()) complete_batch(S, s, warpjq_query_ctx(s.qs[qi]), s.qs[qi], s.by_q[qi], false, out);
@@ -295,7 +299,7 @@ void complete_slot(warpjq_server *S, Slot &s) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
     for (auto &x : out) S->done.push_back(x);
-    S->on_device -= s.reqs.size();
+    S->on_device -= launched;
   }
   S->cv_done.notify_all();
   s.reqs.clear();
@@ -309,6 +313,7 @@ void complete_slot(warpjq_server *S, Slot &s) {
 // launches the slot's batches.  Requests that fail here complete at once.
 void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
   const auto now = Clock::now();
+  const size_t n_take = take.size();  // counted on the device by the caller
   std::vector<warpjq_serve_result> failed;
   s.reqs.clear();
   // arena room for host inputs, unaligned device inputs and converted CSV
@@ -319,7 +324,10 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
     if (!r.owned && (!dev || (uintptr_t)r.data % 16)) room += r.len + 16;
   }
   if (!s.arena.reserve(room, 0, s.st)) {
-    for (auto &r : take) failed.push_back(fail_result(r, "out of device memory for the request's input"));
+    for (auto &r : take) {
+      failed.push_back(fail_result(r, "out of device memory for the request's input"));
+      if (r.owned) cudaFreeAsync(r.owned, s.st);
+    }
     take.clear();
   }
   uint64_t pos = 0;
@@ -411,7 +419,7 @@ void admit(warpjq_server *S, Slot &s, std::vector<Req> take) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
     for (auto &x : failed) S->done.push_back(x);
-    S->on_device -= take.size() - launched;
+    S->on_device -= n_take - launched;
   }
   if (!failed.empty()) S->cv_done.notify_all();
 }
