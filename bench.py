@@ -268,8 +268,7 @@ def measure_batch(wjq, dev, offs, lens, qidx):
     def batched():
         for k, g in enumerate(groups):
             batch_q[k].batch_launch(ptr, [offs[i] for i in g], [lens[i] for i in g], stream)
-        for k in range(len(groups)):
-            batch_q[k].batch_collect()
+        return [batch_q[k].batch_collect() for k in range(len(groups))]
 
     graph_q = [wjq.Query(q, chunk_bytes=1 << 20) for q in BATCH_QUERIES]
     for k, q in enumerate(BATCH_QUERIES):
@@ -279,8 +278,7 @@ def measure_batch(wjq, dev, offs, lens, qidx):
 
     def replay():
         graph.launch(stream)
-        for k in range(len(groups)):
-            graph_q[k].batch_collect()
+        return [graph_q[k].batch_collect() for k in range(len(groups))]
 
     # mixed: every input in one launch sequence, each with its own plan
     # (aggregate and row queries alike)
@@ -290,17 +288,33 @@ def measure_batch(wjq, dev, offs, lens, qidx):
 
     def mixed():
         driver.batch_launch_mixed([batch_q[qidx[i]] for i in every], ptr, offs, lens, stream)
-        driver.batch_collect()
+        return driver.batch_collect()
 
-    out = {}
+    out, got = {}, {}
     for name, fn in (("plain", plain), ("batched", batched), ("graph", replay), ("mixed", mixed)):
         fn()  # warm: buffers reach their sizes
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        fn()
+        got[name] = fn()
         torch.cuda.synchronize()
         out[name] = time.perf_counter() - t0
     graph.close()
+
+    # every input's counts, exact sums and group count, arm against arm
+    def key(it):
+        return (it.n_lines, it.n_blank, it.n_invalid, it.n_selected, it.count, it.isum_lo, it.isum_hi,
+                it.n_groups, it.fsum)
+
+    def per_query_arm(res):
+        per = {}
+        for k, g in enumerate(groups):
+            items = res[k][0]
+            for j, i in enumerate(g):
+                per[i] = key(items[j])
+        return [per[i] for i in every]
+
+    mixed_keys = [key(it) for it in got["mixed"][0]]
+    arms_agree = per_query_arm(got["batched"]) == per_query_arm(got["graph"]) == mixed_keys
     return {"inputs": len(offs), "bytes": total,
             "sizes": "log-uniform 4 KB - 64 MB (the configuration's sizes; 4096 of them total "
                      "about 28 GB, not the configuration's approximate 8 GB)",
@@ -311,6 +325,7 @@ def measure_batch(wjq, dev, offs, lens, qidx):
             "plain_s": round(out["plain"], 4), "batched_s": round(out["batched"], 4),
             "graph_s": round(out["graph"], 4),
             "mixed_gbs": round(total / out["mixed"] / 1e9, 3),
+            "arms_agree": arms_agree,
             "mixed": "all 4096 inputs in one launch sequence, each with its own plan (8 queries: "
                      "aggregates, projection and passthrough)",
             "graph": "one CUDA graph: the 8 queries' batches captured on forked streams, one launch",
@@ -702,6 +717,8 @@ def main():
                     help="only the device-resident CSV leg, on BYTES of CSV (for profiling)")
     ap.add_argument("--nested-only", type=int, default=0, metavar="BYTES",
                     help="only the nested-schema leg, on BYTES of input (for profiling)")
+    ap.add_argument("--batch-only", type=int, default=0, metavar="BYTES",
+                    help="only the batching leg, its 4096 inputs cut from BYTES of nginx input")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -721,6 +738,16 @@ def main():
         return
     if args.nested_only:
         print(json.dumps({"nested": measure_nested(wjq, args.nested_only, reps=args.steps)}), flush=True)
+        return
+    if args.batch_only:
+        host = torch.empty(args.batch_only, dtype=torch.uint8).pin_memory()
+        hnp = host.numpy()
+        _, n, _ = wjq.gen_nginx(args.batch_only, seed=1, into=hnp)
+        dsrc = torch.empty(n + 16, dtype=torch.uint8, device="cuda")
+        dsrc[:n].copy_(host[:n])
+        bdev, boffs, blens, bq = batch_workload(dsrc, hnp, n)
+        del dsrc
+        print(json.dumps({"batch": measure_batch(wjq, bdev, boffs, blens, bq)}), flush=True)
         return
 
     torch.cuda.set_device(local)
